@@ -1,0 +1,552 @@
+// sbf_capi.cu -- C ABI of the Super Bloom engine (declared in include/sbf_b200.h).
+//
+// Host side of the drop-in boundary: it owns the filter's device words and
+// staging buffers, validates arguments with the reference's rules
+// (include/cusbf/filter.cuh:848-876, :1752-1782), stages host input through
+// pinned double buffers so copies overlap kernels, and launches the tile
+// kernels of sbf_kernels.cu.  There is no CPU fallback: every compute entry
+// point runs on the GPU or fails.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "../../include/sbf_b200.h"
+#include "sbf_internal.h"
+#include "sbf_host.h"
+
+using namespace sbf;
+
+// ---------------------------------------------------------------------------
+// Error state
+// ---------------------------------------------------------------------------
+
+namespace sbf {
+thread_local std::string g_last_error;
+thread_local int g_last_cuda = 0;
+
+int set_error(int status, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    g_last_cuda = static_cast<int>(e);
+    return set_error(SBF_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+}  // namespace sbf
+
+#define SBF_CUDA(expr)                                      \
+    do {                                                    \
+        cudaError_t _e = (expr);                            \
+        if (_e != cudaSuccess) return cuda_fail(_e, #expr); \
+    } while (0)
+
+#define SBF_TRY(expr)              \
+    do {                           \
+        int _s = (expr);           \
+        if (_s != SBF_OK) return _s; \
+    } while (0)
+
+extern "C" const char* sbf_last_error_message(void) { return g_last_error.c_str(); }
+extern "C" int sbf_last_cuda_error(void) { return g_last_cuda; }
+extern "C" const char* sbf_version(void) { return "sbf-b200 0.1.0 (sm_100a)"; }
+
+// ---------------------------------------------------------------------------
+// Filter object
+// ---------------------------------------------------------------------------
+
+namespace sbf {
+
+static uint64_t host_chunk_bytes() {
+    // Host-input chunk size; a chunk is copied while the previous one is
+    // hashed.  SBF_HOST_CHUNK_BYTES overrides it (minimum 4096).
+    if (const char* v = std::getenv("SBF_HOST_CHUNK_BYTES")) {
+        const long long b = std::strtoll(v, nullptr, 10);
+        if (b > 0) return std::max<uint64_t>(static_cast<uint64_t>(b), 4096);
+    }
+    return uint64_t{64} << 20;
+}
+
+int Staging::ensure_device(size_t bytes) {
+    if (bytes <= dev_cap) return SBF_OK;
+    for (int i = 0; i < 2; ++i) {
+        if (dev[i]) cudaFree(dev[i]);
+        dev[i] = nullptr;
+    }
+    dev_cap = 0;
+    for (int i = 0; i < 2; ++i) SBF_CUDA(cudaMalloc(&dev[i], bytes));
+    dev_cap = bytes;
+    return SBF_OK;
+}
+
+int Staging::ensure_pinned(size_t bytes) {
+    if (bytes <= pin_cap) return SBF_OK;
+    for (int i = 0; i < 2; ++i) {
+        if (pin[i]) cudaFreeHost(pin[i]);
+        pin[i] = nullptr;
+    }
+    pin_cap = 0;
+    for (int i = 0; i < 2; ++i) SBF_CUDA(cudaMallocHost(&pin[i], bytes));
+    pin_cap = bytes;
+    return SBF_OK;
+}
+
+void Staging::release() {
+    for (int i = 0; i < 2; ++i) {
+        if (dev[i]) cudaFree(dev[i]);
+        if (pin[i]) cudaFreeHost(pin[i]);
+        dev[i] = nullptr;
+        pin[i] = nullptr;
+    }
+    dev_cap = pin_cap = 0;
+}
+
+bool is_pinned(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace sbf
+
+uint64_t sbf_filter::kmers_of(uint64_t symbols) const {
+    return symbols < k ? 0 : symbols - k + 1;
+}
+
+int sbf_filter::launch(bool query, bool dense, const void* input, uint64_t input_bytes,
+                       uint64_t n_kmers, uint8_t* out, cudaStream_t st) const {
+    if (n_kmers == 0) return SBF_OK;
+    TileParams p{};
+    p.input = static_cast<const uint8_t*>(input);
+    p.input_bytes = input_bytes;
+    p.n_kmers = n_kmers;
+    // Grid phase: aligns query output strips (16 windows) to 16 bytes, or the
+    // staged input to 16 bytes for inserts.
+    int64_t phase = 0;
+    if (query)
+        phase = static_cast<int64_t>(reinterpret_cast<uintptr_t>(out) & 15u);
+    else if (!dense)
+        phase = static_cast<int64_t>(reinterpret_cast<uintptr_t>(input) & 15u);
+    p.sym_base = -phase;
+    p.words = d_words;
+    p.shard_mask = static_cast<uint32_t>(num_shards - 1);
+    p.out = out;
+    p.n_tiles = (n_kmers + static_cast<uint64_t>(phase) + kTileKmers - 1) / kTileKmers;
+    p.err = d_err;
+    const int which = (query ? 1 : 0) + (dense ? 2 : 0);
+    void (*fn)(TileParams) = which == 0   ? ks->insert_bytes
+                             : which == 1 ? ks->query_bytes
+                             : which == 2 ? ks->insert_dense
+                                          : ks->query_dense;
+    const uint64_t resident = static_cast<uint64_t>(sms) * static_cast<uint64_t>(occupancy[which]);
+    const uint64_t grid = std::min<uint64_t>(p.n_tiles, std::max<uint64_t>(resident, 1));
+    fn<<<static_cast<unsigned>(grid), kThreads, 0, st>>>(p);
+    SBF_CUDA(cudaGetLastError());
+    ++launches;
+    return SBF_OK;
+}
+
+int sbf_filter::check_device_error(cudaStream_t st) const {
+    int h_err = 0;
+    SBF_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SBF_CUDA(cudaStreamSynchronize(st));
+    if (h_err != kDevErrNone) {
+        cudaMemsetAsync(d_err, 0, sizeof(int), st);
+        cudaStreamSynchronize(st);
+        return set_error(SBF_ERR_CUDA, "device error %d (staging wait timed out)", h_err);
+    }
+    return SBF_OK;
+}
+
+// Host bytes -> device in chunks of whole windows with a (k-1)-symbol overlap,
+// double-buffered: the copy of chunk c+1 (on copy_stream) overlaps the kernel
+// of chunk c (on `st`).  `out_host`/`out_dev` receive query bytes.
+int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t in_bytes,
+                              uint64_t n_kmers, uint8_t* out_host, uint8_t* out_dev,
+                              cudaStream_t st) {
+    if (n_kmers == 0) return SBF_OK;
+    // Symbols <-> bytes: byte input has one byte per symbol; dense input has
+    // 32 symbols per 8-byte word, so chunks are cut at word boundaries.
+    const uint64_t chunk_target = host_chunk_bytes();
+    uint64_t chunk_kmers;
+    if (dense) {
+        chunk_kmers = std::max<uint64_t>((chunk_target * 4) / 32 * 32, 1024);
+    } else {
+        chunk_kmers = chunk_target;
+    }
+    const uint64_t n_chunks = (n_kmers + chunk_kmers - 1) / chunk_kmers;
+    auto chunk_span = [&](uint64_t c, uint64_t& first_byte, uint64_t& bytes, uint64_t& kmers,
+                          uint64_t& sym_offset) {
+        const uint64_t w0 = c * chunk_kmers;
+        kmers = std::min<uint64_t>(chunk_kmers, n_kmers - w0);
+        const uint64_t syms = kmers + k - 1;
+        if (dense) {
+            first_byte = (w0 / 32) * 8;
+            sym_offset = w0 % 32;  // always 0: chunk_kmers is a multiple of 32
+            bytes = std::min<uint64_t>(((sym_offset + syms + 31) / 32) * 8, in_bytes - first_byte);
+        } else {
+            first_byte = w0;
+            sym_offset = 0;
+            bytes = syms;
+        }
+    };
+    const uint64_t max_in = dense ? ((chunk_kmers + k - 1 + 31) / 32) * 8 + 8 : chunk_kmers + k;
+    const bool in_pinned = is_pinned(h_in);
+    const bool out_pinned = out_host != nullptr && is_pinned(out_host);
+    SBF_TRY(stage_in.ensure_device(max_in));
+    if (!in_pinned) SBF_TRY(stage_in.ensure_pinned(max_in));
+    if (query && out_dev == nullptr) SBF_TRY(stage_out.ensure_device(chunk_kmers));
+    if (query && out_host != nullptr && !out_pinned) SBF_TRY(stage_out.ensure_pinned(chunk_kmers));
+
+    for (uint64_t c = 0; c < n_chunks; ++c) {
+        const int slot = static_cast<int>(c & 1);
+        uint64_t first_byte, bytes, kmers, sym_offset;
+        chunk_span(c, first_byte, bytes, kmers, sym_offset);
+        // The slot's previous kernel (and output copy) must be finished
+        // before its buffers are reused.
+        SBF_CUDA(cudaEventSynchronize(ev_done[slot]));
+        if (query && out_host != nullptr && !out_pinned && c >= 2) {
+            // Drain the host output of chunk c-2 which used this slot.
+            uint64_t pf, pb, pk, po;
+            chunk_span(c - 2, pf, pb, pk, po);
+            std::memcpy(out_host + (c - 2) * chunk_kmers, stage_out.pin[slot], pk);
+        }
+        const char* src = static_cast<const char*>(h_in) + first_byte;
+        if (!in_pinned) {
+            std::memcpy(stage_in.pin[slot], src, bytes);
+            src = static_cast<const char*>(stage_in.pin[slot]);
+        }
+        SBF_CUDA(cudaMemcpyAsync(stage_in.dev[slot], src, bytes, cudaMemcpyHostToDevice,
+                                 copy_stream));
+        SBF_CUDA(cudaEventRecord(ev_copied[slot], copy_stream));
+        SBF_CUDA(cudaStreamWaitEvent(st, ev_copied[slot], 0));
+        uint8_t* dout = nullptr;
+        if (query) {
+            dout = out_dev ? out_dev + c * chunk_kmers
+                           : static_cast<uint8_t*>(stage_out.dev[slot]);
+        }
+        SBF_TRY(launch(query, dense, stage_in.dev[slot], bytes, kmers, dout, st));
+        if (query && out_host != nullptr) {
+            void* hdst = out_pinned ? static_cast<void*>(out_host + c * chunk_kmers)
+                                    : stage_out.pin[slot];
+            SBF_CUDA(cudaMemcpyAsync(hdst, dout, kmers, cudaMemcpyDeviceToHost, st));
+        }
+        // The host waits on this event before reusing the slot (top of the
+        // loop), so the copy of chunk c+2 never overwrites a buffer that a
+        // kernel is still reading, while chunk c+1's copy overlaps this kernel.
+        SBF_CUDA(cudaEventRecord(ev_done[slot], st));
+    }
+    SBF_CUDA(cudaStreamSynchronize(st));
+    if (query && out_host != nullptr && !out_pinned) {
+        for (uint64_t c = (n_chunks >= 2 ? n_chunks - 2 : 0); c < n_chunks; ++c) {
+            uint64_t pf, pb, pk, po;
+            chunk_span(c, pf, pb, pk, po);
+            std::memcpy(out_host + c * chunk_kmers, stage_out.pin[c & 1], pk);
+        }
+    }
+    return check_device_error(st);
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+static inline cudaStream_t S(sbf_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t hashes,
+                                 int alphabet, uint64_t requested_bits, sbf_filter_t** out) {
+    if (!out) return set_error(SBF_ERR_INVALID_ARGUMENT, "output handle pointer is null");
+    *out = nullptr;
+    if (alphabet != SBF_ALPHABET_DNA)
+        return set_error(SBF_ERR_INVALID_ARGUMENT,
+                         "alphabet %d is not implemented by the GPU engine (DNA only)", alphabet);
+    const KernelSet* ks = find_kernels(static_cast<int>(k), static_cast<int>(s),
+                                       static_cast<int>(m), static_cast<int>(hashes));
+    if (!ks)
+        return set_error(SBF_ERR_INVALID_ARGUMENT,
+                         "configuration k=%u s=%u m=%u hashes=%u is not compiled into this "
+                         "library",
+                         k, s, m, hashes);
+    uint64_t blocks = requested_bits / 256 + (requested_bits % 256 != 0);
+    if (blocks < 1) blocks = 1;
+    uint64_t shards = 1;
+    while (shards < blocks) shards <<= 1;
+    auto* f = new sbf_filter();
+    f->ks = ks;
+    f->k = k;
+    f->s = s;
+    f->m = m;
+    f->h = hashes;
+    f->num_shards = shards;
+    f->filter_bits = shards * 256;
+    int rc = SBF_OK;
+    do {
+        cudaError_t e = cudaGetDevice(&f->device);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "cudaGetDevice"); break; }
+        e = cudaDeviceGetAttribute(&f->sms, cudaDevAttrMultiProcessorCount, f->device);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "cudaDeviceGetAttribute"); break; }
+        void (*fns[4])(TileParams) = {ks->insert_bytes, ks->query_bytes, ks->insert_dense,
+                                      ks->query_dense};
+        for (int i = 0; i < 4 && rc == SBF_OK; ++i) {
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&f->occupancy[i],
+                                                              reinterpret_cast<const void*>(fns[i]),
+                                                              kThreads, 0);
+            if (e != cudaSuccess) rc = cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+            if (f->occupancy[i] < 1) f->occupancy[i] = 1;
+        }
+        if (rc != SBF_OK) break;
+        e = cudaMalloc(&f->d_words, shards * 32);
+        if (e != cudaSuccess) {
+            rc = e == cudaErrorMemoryAllocation
+                     ? (cudaGetLastError(),
+                        set_error(SBF_ERR_RESOURCE, "cannot allocate %llu bytes of filter words",
+                                  static_cast<unsigned long long>(shards * 32)))
+                     : cuda_fail(e, "cudaMalloc(words)");
+            break;
+        }
+        e = cudaMalloc(&f->d_err, 64);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "cudaMalloc(err)"); break; }
+        e = cudaMemset(f->d_err, 0, 64);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "cudaMemset(err)"); break; }
+        e = cudaStreamCreateWithFlags(&f->copy_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamCreate"); break; }
+        for (int i = 0; i < 2 && rc == SBF_OK; ++i) {
+            e = cudaEventCreateWithFlags(&f->ev_copied[i], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->ev_done[i], cudaEventDisableTiming);
+            if (e != cudaSuccess) rc = cuda_fail(e, "cudaEventCreate");
+        }
+        if (rc != SBF_OK) break;
+        e = cudaMemset(f->d_words, 0, shards * 32);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "cudaMemset(words)"); break; }
+        e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) { rc = cuda_fail(e, "cudaDeviceSynchronize"); break; }
+    } while (false);
+    if (rc != SBF_OK) {
+        sbf_filter_destroy(f);
+        return rc;
+    }
+    *out = f;
+    return SBF_OK;
+}
+
+extern "C" void sbf_filter_destroy(sbf_filter_t* f) {
+    if (!f) return;
+    f->stage_in.release();
+    f->stage_out.release();
+    if (f->d_words) cudaFree(f->d_words);
+    if (f->d_err) cudaFree(f->d_err);
+    for (int i = 0; i < 2; ++i) {
+        if (f->ev_copied[i]) cudaEventDestroy(f->ev_copied[i]);
+        if (f->ev_done[i]) cudaEventDestroy(f->ev_done[i]);
+    }
+    if (f->copy_stream) cudaStreamDestroy(f->copy_stream);
+    delete f;
+}
+
+extern "C" int sbf_filter_clear(sbf_filter_t* f, sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    SBF_CUDA(cudaMemsetAsync(f->d_words, 0, f->num_shards * 32, S(stream)));
+    SBF_CUDA(cudaStreamSynchronize(S(stream)));
+    return SBF_OK;
+}
+
+extern "C" uint64_t sbf_filter_bits(const sbf_filter_t* f) { return f ? f->filter_bits : 0; }
+extern "C" uint64_t sbf_filter_num_shards(const sbf_filter_t* f) { return f ? f->num_shards : 0; }
+
+extern "C" int sbf_filter_words(const sbf_filter_t* f, uint64_t** d_words, uint64_t* n_words) {
+    if (!f || !d_words || !n_words) return set_error(SBF_ERR_INVALID_ARGUMENT, "null argument");
+    *d_words = f->d_words;
+    *n_words = f->num_shards * 4;
+    return SBF_OK;
+}
+
+extern "C" uint64_t sbf_filter_kmer_count(const sbf_filter_t* f, uint64_t bytes) {
+    return f ? f->kmers_of(bytes) : 0;
+}
+
+extern "C" int sbf_filter_load_factor(sbf_filter_t* f, sbf_stream_t stream, double* out) {
+    if (!f || !out) return set_error(SBF_ERR_INVALID_ARGUMENT, "null argument");
+    unsigned long long* d_count = reinterpret_cast<unsigned long long*>(f->d_err + 8);
+    SBF_CUDA(launch_popcount(f->d_words, f->num_shards * 4, d_count, S(stream)));
+    unsigned long long bits = 0;
+    SBF_CUDA(cudaMemcpyAsync(&bits, d_count, sizeof bits, cudaMemcpyDeviceToHost, S(stream)));
+    SBF_CUDA(cudaStreamSynchronize(S(stream)));
+    *out = static_cast<double>(bits) / static_cast<double>(f->filter_bits);
+    return SBF_OK;
+}
+
+// ---- byte sequences ---------------------------------------------------------
+
+extern "C" int sbf_insert_sequence_async(sbf_filter_t* f, const char* d_seq, uint64_t bytes,
+                                         sbf_stream_t stream, uint64_t* kmers_out) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    const uint64_t n = f->kmers_of(bytes);
+    if (kmers_out) *kmers_out = n;
+    if (n == 0) return SBF_OK;
+    if (!d_seq) return set_error(SBF_ERR_INVALID_ARGUMENT, "sequence pointer is null");
+    return f->launch(false, false, d_seq, bytes, n, nullptr, S(stream));
+}
+
+extern "C" int sbf_insert_sequence(sbf_filter_t* f, const char* h_seq, uint64_t bytes,
+                                   sbf_stream_t stream, uint64_t* kmers_out) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    const uint64_t n = f->kmers_of(bytes);
+    if (kmers_out) *kmers_out = n;
+    if (n == 0) return SBF_OK;
+    if (!h_seq) return set_error(SBF_ERR_INVALID_ARGUMENT, "sequence pointer is null");
+    return f->host_pipeline(false, false, h_seq, bytes, n, nullptr, nullptr, S(stream));
+}
+
+extern "C" int sbf_contains_sequence_async(const sbf_filter_t* f, const char* d_seq,
+                                           uint64_t bytes, uint8_t* d_out, uint64_t out_len,
+                                           sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    const uint64_t n = f->kmers_of(bytes);
+    if (n == 0) return SBF_OK;
+    if (!d_seq || !d_out) return set_error(SBF_ERR_INVALID_ARGUMENT, "null device pointer");
+    if (out_len < n)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "query output span is too small (%llu < %llu)",
+                         static_cast<unsigned long long>(out_len),
+                         static_cast<unsigned long long>(n));
+    return f->launch(true, false, d_seq, bytes, n, d_out, S(stream));
+}
+
+extern "C" int sbf_contains_sequence_to_device(const sbf_filter_t* f, const char* h_seq,
+                                               uint64_t bytes, uint8_t* d_out, uint64_t out_len,
+                                               sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    const uint64_t n = f->kmers_of(bytes);
+    if (n == 0) return SBF_OK;
+    if (!h_seq || !d_out) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    if (out_len < n) return set_error(SBF_ERR_INVALID_ARGUMENT, "query output span is too small");
+    return const_cast<sbf_filter*>(f)->host_pipeline(true, false, h_seq, bytes, n, nullptr, d_out,
+                                                     S(stream));
+}
+
+extern "C" int sbf_contains_sequence(const sbf_filter_t* f, const char* h_seq, uint64_t bytes,
+                                     uint8_t* h_out, uint64_t out_len, sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    const uint64_t n = f->kmers_of(bytes);
+    if (n == 0) return SBF_OK;
+    if (!h_seq || !h_out) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    if (out_len < n) return set_error(SBF_ERR_INVALID_ARGUMENT, "query output span is too small");
+    return const_cast<sbf_filter*>(f)->host_pipeline(true, false, h_seq, bytes, n, h_out, nullptr,
+                                                     S(stream));
+}
+
+// ---- dense input --------------------------------------------------------------
+
+extern "C" uint64_t sbf_dense_packed_word_count(uint64_t num_symbols) {
+    return (num_symbols + 31) / 32;
+}
+
+extern "C" int sbf_pack_dense_device(const char* d_seq, uint64_t num_symbols, uint64_t* d_words,
+                                     sbf_stream_t stream) {
+    if (num_symbols == 0) return SBF_OK;
+    if (!d_seq || !d_words) return set_error(SBF_ERR_INVALID_ARGUMENT, "null device pointer");
+    SBF_CUDA(launch_pack_dense(reinterpret_cast<const uint8_t*>(d_seq), num_symbols, d_words,
+                               S(stream)));
+    return SBF_OK;
+}
+
+extern "C" int sbf_pack_dense_host(const char* h_seq, uint64_t num_symbols, uint64_t* h_words) {
+    if (num_symbols == 0) return SBF_OK;
+    if (!h_seq || !h_words) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    const uint64_t n_words = (num_symbols + 31) / 32;
+    std::memset(h_words, 0, n_words * 8);
+    for (uint64_t t = 0; t < num_symbols; ++t) {
+        const uint8_t b = static_cast<uint8_t>(h_seq[t]);
+        const uint8_t u = b & 0xDFu;
+        const bool valid = u == 'A' || u == 'C' || u == 'G' || u == 'T';
+        const uint64_t code = valid ? ((b >> 1) & 3u) : 3u;
+        h_words[t / 32] |= code << (2 * (t % 32));
+    }
+    return SBF_OK;
+}
+
+static int check_dense(const sbf_filter_t* f, const void* words, uint64_t n_words,
+                       uint64_t num_symbols) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (!words) return set_error(SBF_ERR_INVALID_ARGUMENT, "dense word pointer is null");
+    if (n_words < (num_symbols + 31) / 32)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "dense packed span is too small for num_symbols");
+    return SBF_OK;
+}
+
+extern "C" int sbf_insert_dense_packed_async(sbf_filter_t* f, const uint64_t* d_words,
+                                             uint64_t n_words, uint64_t num_symbols,
+                                             sbf_stream_t stream, uint64_t* kmers_out) {
+    const uint64_t n = f ? f->kmers_of(num_symbols) : 0;
+    if (kmers_out) *kmers_out = n;
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (n == 0) return SBF_OK;
+    SBF_TRY(check_dense(f, d_words, n_words, num_symbols));
+    return f->launch(false, true, d_words, ((num_symbols + 31) / 32) * 8, n, nullptr, S(stream));
+}
+
+extern "C" int sbf_insert_dense_packed(sbf_filter_t* f, const uint64_t* h_words,
+                                       uint64_t n_words, uint64_t num_symbols, sbf_stream_t stream,
+                                       uint64_t* kmers_out) {
+    const uint64_t n = f ? f->kmers_of(num_symbols) : 0;
+    if (kmers_out) *kmers_out = n;
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (n == 0) return SBF_OK;
+    SBF_TRY(check_dense(f, h_words, n_words, num_symbols));
+    return f->host_pipeline(false, true, h_words, ((num_symbols + 31) / 32) * 8, n, nullptr,
+                            nullptr, S(stream));
+}
+
+extern "C" int sbf_contains_dense_packed_async(const sbf_filter_t* f, const uint64_t* d_words,
+                                               uint64_t n_words, uint64_t num_symbols,
+                                               uint8_t* d_out, uint64_t out_len,
+                                               sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    const uint64_t n = f->kmers_of(num_symbols);
+    if (n == 0) return SBF_OK;
+    SBF_TRY(check_dense(f, d_words, n_words, num_symbols));
+    if (!d_out || out_len < n)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "dense packed query output span is too small");
+    return f->launch(true, true, d_words, ((num_symbols + 31) / 32) * 8, n, d_out, S(stream));
+}
+
+extern "C" int sbf_contains_dense_packed_to_device(const sbf_filter_t* f, const uint64_t* h_words,
+                                                   uint64_t n_words, uint64_t num_symbols,
+                                                   uint8_t* d_out, uint64_t out_len,
+                                                   sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    const uint64_t n = f->kmers_of(num_symbols);
+    if (n == 0) return SBF_OK;
+    SBF_TRY(check_dense(f, h_words, n_words, num_symbols));
+    if (!d_out || out_len < n)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "dense packed query output span is too small");
+    return const_cast<sbf_filter*>(f)->host_pipeline(true, true, h_words,
+                                                     ((num_symbols + 31) / 32) * 8, n, nullptr,
+                                                     d_out, S(stream));
+}
+
+extern "C" int sbf_contains_dense_packed(const sbf_filter_t* f, const uint64_t* h_words,
+                                         uint64_t n_words, uint64_t num_symbols, uint8_t* h_out,
+                                         uint64_t out_len, sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    const uint64_t n = f->kmers_of(num_symbols);
+    if (n == 0) return SBF_OK;
+    SBF_TRY(check_dense(f, h_words, n_words, num_symbols));
+    if (!h_out || out_len < n)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "dense packed query output span is too small");
+    return const_cast<sbf_filter*>(f)->host_pipeline(true, true, h_words,
+                                                     ((num_symbols + 31) / 32) * 8, n, h_out,
+                                                     nullptr, S(stream));
+}

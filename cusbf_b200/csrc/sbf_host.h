@@ -1,0 +1,55 @@
+// sbf_host.h -- host-side filter object behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "sbf_internal.h"
+
+namespace sbf {
+
+int set_error(int status, const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what);
+bool is_pinned(const void* p);
+
+// A pair of device buffers and a pair of pinned host buffers, grown on
+// demand and reused across calls.
+struct Staging {
+    void* dev[2] = {nullptr, nullptr};
+    void* pin[2] = {nullptr, nullptr};
+    size_t dev_cap = 0;
+    size_t pin_cap = 0;
+    int ensure_device(size_t bytes);
+    int ensure_pinned(size_t bytes);
+    void release();
+};
+
+}  // namespace sbf
+
+struct sbf_filter {
+    const sbf::KernelSet* ks = nullptr;
+    uint32_t k = 0, s = 0, m = 0, h = 0;
+    uint64_t num_shards = 0;
+    uint64_t filter_bits = 0;
+    uint64_t* d_words = nullptr;
+    int* d_err = nullptr;  // [0] device error word, [8..9] popcount scratch
+    int device = 0;
+    int sms = 0;
+    int occupancy[4] = {1, 1, 1, 1};  // insert/query x bytes/dense
+    mutable uint64_t launches = 0;
+
+    sbf::Staging stage_in;
+    sbf::Staging stage_out;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_copied[2] = {nullptr, nullptr};
+    cudaEvent_t ev_done[2] = {nullptr, nullptr};
+
+    uint64_t kmers_of(uint64_t symbols) const;
+    int launch(bool query, bool dense, const void* input, uint64_t input_bytes, uint64_t n_kmers,
+               uint8_t* out, cudaStream_t st) const;
+    int host_pipeline(bool query, bool dense, const void* h_in, uint64_t in_bytes,
+                      uint64_t n_kmers, uint8_t* out_host, uint8_t* out_dev, cudaStream_t st);
+    int check_device_error(cudaStream_t st) const;
+};

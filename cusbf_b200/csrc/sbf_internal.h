@@ -1,0 +1,57 @@
+// sbf_internal.h -- types shared by the kernels and the C-ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace sbf {
+
+// Launch geometry of the tile kernels.
+constexpr int kThreads = 256;                       // threads per CTA
+constexpr int kStrip = 16;                          // consecutive k-mers per thread
+constexpr int kTileKmers = kThreads * kStrip;       // k-mers per tile (4096)
+constexpr int kCodeWords = kThreads + 2;            // 16-base code words per tile
+constexpr int kStageBytes = kTileKmers + 64 + 32;   // staged input bytes per buffer
+
+// One launch of a tile kernel.  Grid position g of tile n is
+// g = n * kTileKmers + (0 .. kTileKmers-1); it holds window (k-mer)
+// i = g + sym_base, and symbol i is the first base of that window.
+struct TileParams {
+    const uint8_t* input;    // device bytes (ASCII) or dense words viewed as bytes
+    uint64_t input_bytes;    // readable bytes at `input`
+    uint64_t n_kmers;        // windows to process
+    int64_t sym_base;        // symbol index of grid position 0 (= -phase)
+    uint64_t* words;         // filter: num_shards * 4 words
+    uint32_t shard_mask;     // (uint32_t)(num_shards - 1)
+    uint8_t* out;            // query: one byte per window
+    uint64_t n_tiles;
+    int* err;                // device error word (non-zero = failure code)
+};
+
+// Device error codes written to TileParams::err.
+enum : int {
+    kDevErrNone = 0,
+    kDevErrStageTimeout = 1,  // a bulk-copy wait ran out of its time bound
+};
+
+// Function table for one compiled configuration <K,S,M,H>.
+struct KernelSet {
+    int k, s, m, h;
+    void (*insert_bytes)(TileParams);
+    void (*query_bytes)(TileParams);
+    void (*insert_dense)(TileParams);
+    void (*query_dense)(TileParams);
+};
+
+// Returns the kernel table for a configuration, or nullptr when it is not
+// compiled into this library.
+const KernelSet* find_kernels(int k, int s, int m, int h);
+
+// Auxiliary kernels (sbf_kernels.cu).
+cudaError_t launch_pack_dense(const uint8_t* seq, uint64_t num_symbols, uint64_t* words,
+                              cudaStream_t stream);
+cudaError_t launch_popcount(const uint64_t* words, uint64_t n_words, unsigned long long* out,
+                            cudaStream_t stream);
+
+}  // namespace sbf

@@ -1,0 +1,202 @@
+"""Seeded synthetic DNA workloads with the shapes of the benchmark configs.
+
+No public genome is used: the plain-method, genome-scale and ragged workloads
+are stood in for by seeded generators with their sizes and value
+distributions (GC content, tandem repeats, N runs, diverged interspersed
+repeat families, reads with substitution errors, log-normal lengths).
+
+All generators are deterministic functions of their seed (numpy PCG64 on the
+CPU).  ``reads_device`` samples reads on a CUDA device with a seeded torch
+generator, for the 10^7-10^8 read sets of the large workloads.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+SEPARATOR = ord("N")
+_BASES = np.frombuffer(b"ACGT", dtype=np.uint8)
+
+
+def _base_lut(gc: float) -> np.ndarray:
+    """256-entry byte -> base table with P(C)=P(G)=gc/2, P(A)=P(T)=(1-gc)/2."""
+    c = int(round(256 * gc / 2))
+    a = int(round(256 * (1 - gc) / 2))
+    t = 256 - 2 * c - a
+    lut = np.empty(256, dtype=np.uint8)
+    lut[:a] = ord("A")
+    lut[a:a + c] = ord("C")
+    lut[a + c:a + 2 * c] = ord("G")
+    lut[a + 2 * c:] = ord("T")
+    assert t >= 0
+    return lut
+
+
+def uniform_dna(n: int, seed: int, gc: float = 0.5, rng=None) -> np.ndarray:
+    """n i.i.d. bases (uint8 ASCII) with the given GC fraction."""
+    rng = rng if rng is not None else np.random.default_rng(seed)
+    lut = _base_lut(gc)
+    out = np.empty(n, dtype=np.uint8)
+    step = 1 << 26
+    for i in range(0, n, step):
+        m = min(step, n - i)
+        out[i:i + m] = lut[rng.integers(0, 256, size=m, dtype=np.uint8)]
+    return out
+
+
+def _mutate(seq: np.ndarray, rate: float, rng) -> np.ndarray:
+    """Substitutes each base with a different base with probability `rate`."""
+    if rate <= 0 or seq.size == 0:
+        return seq
+    n_sub = rng.binomial(seq.size, rate)
+    if n_sub == 0:
+        return seq
+    pos = rng.choice(seq.size, size=n_sub, replace=False) if n_sub < seq.size // 4 else \
+        np.flatnonzero(rng.random(seq.size) < rate)
+    out = seq.copy()
+    cur = out[pos]
+    code = (cur >> 1) & 3  # A0 C1 T2 G3
+    new = (code + rng.integers(1, 4, size=pos.size)) & 3
+    out[pos] = np.frombuffer(b"ACTG", dtype=np.uint8)[new]
+    return out
+
+
+def record_lengths(total_bp: int, n_records: int, lo: int, hi: int, seed: int) -> list[int]:
+    """n lengths drawn uniformly in [lo, hi], rescaled to sum to total_bp."""
+    rng = np.random.default_rng(seed)
+    raw = rng.uniform(lo, hi, size=n_records)
+    raw = raw / raw.sum() * total_bp
+    lens = np.floor(raw).astype(np.int64)
+    lens[-1] += total_bp - lens.sum()
+    return [int(x) for x in lens]
+
+
+def genome_records(total_bp: int, n_records: int, seed: int, gc: float = 0.41,
+                   tandem_frac: float = 0.0, n_run_frac: float = 0.0,
+                   interspersed_frac: float = 0.0, n_units: int = 2000,
+                   unit_len: tuple[int, int] = (300, 6000),
+                   divergence: tuple[float, float] = (0.05, 0.20),
+                   lengths: list[int] | None = None) -> list[np.ndarray]:
+    """Genome-like records.
+
+    * background: i.i.d. bases at GC fraction `gc`;
+    * interspersed repeats: copies of `n_units` seeded repeat units (lengths
+      uniform in `unit_len`), each copy substituted at a divergence drawn from
+      `divergence`, placed until `interspersed_frac` of the bases are covered;
+    * tandem repeats: regions of 100-2000 bp filled with a period-2..200 unit;
+    * N runs of 10-1000 bp covering `n_run_frac` of the bases.
+    """
+    rng = np.random.default_rng(seed)
+    if lengths is None:
+        lengths = [total_bp // n_records] * n_records
+        lengths[-1] += total_bp - sum(lengths)
+    recs = [uniform_dna(L, seed=0, gc=gc, rng=rng) for L in lengths]
+    total = sum(lengths)
+    cum = np.cumsum([0] + lengths)
+
+    def place(n_bases_target: int, make_piece):
+        covered = 0
+        while covered < n_bases_target:
+            piece = make_piece()
+            r = int(np.searchsorted(cum, rng.integers(0, total), side="right") - 1)
+            L = recs[r].size
+            if piece.size >= L:
+                continue
+            p = int(rng.integers(0, L - piece.size))
+            recs[r][p:p + piece.size] = piece
+            covered += piece.size
+
+    if interspersed_frac > 0:
+        units = [uniform_dna(int(rng.integers(unit_len[0], unit_len[1] + 1)), seed=0, gc=gc,
+                             rng=rng) for _ in range(n_units)]
+        place(int(interspersed_frac * total),
+              lambda: _mutate(units[int(rng.integers(0, n_units))],
+                              float(rng.uniform(*divergence)), rng))
+    if tandem_frac > 0:
+        def tandem():
+            period = int(rng.integers(2, 201))
+            unit = uniform_dna(period, seed=0, gc=gc, rng=rng)
+            length = int(rng.integers(100, 2001))
+            return np.resize(unit, length)
+        place(int(tandem_frac * total), tandem)
+    if n_run_frac > 0:
+        place(int(n_run_frac * total),
+              lambda: np.full(int(rng.integers(10, 1001)), SEPARATOR, dtype=np.uint8))
+    return recs
+
+
+def join_records(records: list[np.ndarray]) -> tuple[np.ndarray, np.ndarray]:
+    """Concatenates records with one 'N' separator between consecutive
+    records (include/cusbf/normalized_record_batch.hpp:113-121, DNA) and
+    returns (bytes, ranges[n, 2] of (offset, length))."""
+    n = len(records)
+    total = sum(r.size for r in records) + max(n - 1, 0)
+    out = np.empty(total, dtype=np.uint8)
+    ranges = np.zeros((n, 2), dtype=np.uint64)
+    pos = 0
+    for i, r in enumerate(records):
+        if i:
+            out[pos] = SEPARATOR
+            pos += 1
+        out[pos:pos + r.size] = r
+        ranges[i] = (pos, r.size)
+        pos += r.size
+    return out, ranges
+
+
+def reads_host(records: list[np.ndarray], n_reads: int, length: int, seed: int,
+               sub_rate: float = 0.01, positive_frac: float = 0.5, gc: float = 0.5) -> np.ndarray:
+    """(n_reads, length) uint8 reads: a `positive_frac` share sampled from the
+    records with substitutions at `sub_rate`, the rest i.i.d. random."""
+    rng = np.random.default_rng(seed)
+    out = uniform_dna(n_reads * length, seed=0, gc=gc, rng=rng).reshape(n_reads, length)
+    n_pos = int(round(n_reads * positive_frac))
+    lens = np.array([r.size for r in records], dtype=np.int64)
+    w = np.clip(lens - length, 0, None).astype(np.float64)
+    rec = rng.choice(len(records), size=n_pos, p=w / w.sum())
+    for i in range(n_pos):
+        r = records[rec[i]]
+        p = int(rng.integers(0, r.size - length + 1))
+        out[i] = _mutate(r[p:p + length], sub_rate, rng)
+    return out
+
+
+def lognormal_lengths(n: int, median: float, sigma: float, lo: int, hi: int, seed: int) -> np.ndarray:
+    """n integer lengths, log-normal with the given median, clipped to [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    x = rng.lognormal(mean=np.log(median), sigma=sigma, size=n)
+    return np.clip(np.round(x), lo, hi).astype(np.int64)
+
+
+def reads_device(source, n_reads: int, length: int, seed: int, sub_rate: float = 0.01,
+                 positive_frac: float = 0.5, device: str = "cuda"):
+    """(n_reads, length) uint8 CUDA tensor of reads: the first
+    `positive_frac` share sampled from `source` (a 1-D uint8 CUDA tensor of
+    joined records) with substitutions at `sub_rate`, the rest uniform random.
+    Deterministic for a given seed, torch version and device type."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    lut = torch.tensor(list(b"ACGT"), dtype=torch.uint8, device=device)
+    sub = torch.tensor(list(b"ACTG"), dtype=torch.uint8, device=device)
+    out = torch.empty((n_reads, length), dtype=torch.uint8, device=device)
+    n_pos = int(round(n_reads * positive_frac))
+    step = 1 << 20
+    span = source.numel() - length
+    offs = torch.arange(length, device=device, dtype=torch.int64)
+    for i in range(0, n_reads, step):
+        m = min(step, n_reads - i)
+        blk = out[i:i + m]
+        blk.copy_(lut[torch.randint(0, 4, (m, length), device=device, generator=g,
+                                    dtype=torch.int32).long()])
+        p_hi = min(i + m, n_pos)
+        if p_hi > i:
+            k = p_hi - i
+            starts = torch.randint(0, span, (k,), device=device, generator=g, dtype=torch.int64)
+            src = source[(starts[:, None] + offs[None, :])]
+            mask = torch.rand((k, length), device=device, generator=g) < sub_rate
+            shift = torch.randint(1, 4, (k, length), device=device, generator=g, dtype=torch.int32)
+            code = ((src >> 1) & 3).to(torch.int32)
+            mutated = sub[((code + shift) & 3).long()]
+            blk[:k] = torch.where(mask, mutated, src)
+    return out

@@ -1,0 +1,114 @@
+// ref_gpu.cu -- extern "C" handle over the UNMODIFIED reference cuSBF GPU
+// filter (include/cusbf/filter.cuh of tdortman/cuSBF), compiled for sm_100a.
+//
+// TEST INFRASTRUCTURE ONLY (built into oracle/_ref/, never shipped).  GPU
+// parity tests use it to check that the engine's filter words and query
+// bytes equal the reference GPU path's on the same input, and to time the
+// reference kernels beside the engine's.  It calls the reference's public
+// API exactly as its benchmark does (insert_sequence_async /
+// contains_sequence_async, benchmarks/benchmark_common.cuh:987-1035).
+#include <cstdint>
+#include <new>
+
+#include <cusbf/filter.cuh>
+
+namespace {
+using C31 = cusbf::Config<31, 28, 16, 4>;
+using C5 = cusbf::Config<5, 4, 3, 4>;
+
+struct Handle {
+    int cfg;
+    void* f;
+};
+
+// filter::ref() const does not instantiate in the reference (it converts a
+// const shard pointer to a non-const one), so the shard vector is reached
+// through the explicit-instantiation access rule instead.
+template <typename Tag, typename Tag::type Member>
+struct ShardAccess {
+    friend typename Tag::type shard_member(Tag) { return Member; }
+};
+struct Shards31 {
+    using type = thrust::device_vector<cusbf::filter_block<C31>> cusbf::filter<C31>::*;
+    friend type shard_member(Shards31);
+};
+struct Shards5 {
+    using type = thrust::device_vector<cusbf::filter_block<C5>> cusbf::filter<C5>::*;
+    friend type shard_member(Shards5);
+};
+template struct ShardAccess<Shards31, &cusbf::filter<C31>::d_shards_>;
+template struct ShardAccess<Shards5, &cusbf::filter<C5>::d_shards_>;
+
+const void* shard_ptr(cusbf::filter<C31>& f) {
+    return thrust::raw_pointer_cast((f.*shard_member(Shards31{})).data());
+}
+const void* shard_ptr(cusbf::filter<C5>& f) {
+    return thrust::raw_pointer_cast((f.*shard_member(Shards5{})).data());
+}
+
+template <typename Fn>
+int with(Handle* h, Fn&& fn) {
+    if (!h) return -1;
+    if (h->cfg == 0) return fn(*static_cast<cusbf::filter<C31>*>(h->f));
+    if (h->cfg == 1) return fn(*static_cast<cusbf::filter<C5>*>(h->f));
+    return -1;
+}
+}  // namespace
+
+extern "C" {
+
+void* sbf_refgpu_create(int cfg, uint64_t bits) {
+    try {
+        if (cfg == 0) return new Handle{0, new cusbf::filter<C31>(bits)};
+        if (cfg == 1) return new Handle{1, new cusbf::filter<C5>(bits)};
+    } catch (...) {
+    }
+    return nullptr;
+}
+
+void sbf_refgpu_destroy(void* p) {
+    auto* h = static_cast<Handle*>(p);
+    if (!h) return;
+    if (h->cfg == 0) delete static_cast<cusbf::filter<C31>*>(h->f);
+    if (h->cfg == 1) delete static_cast<cusbf::filter<C5>*>(h->f);
+    delete h;
+}
+
+int sbf_refgpu_clear(void* p, cudaStream_t stream) {
+    return with(static_cast<Handle*>(p), [&](auto& f) { return f.clear(stream) ? 0 : 1; });
+}
+
+int sbf_refgpu_insert_async(void* p, const char* d_seq, uint64_t len, cudaStream_t stream) {
+    return with(static_cast<Handle*>(p), [&](auto& f) {
+        auto r = f.insert_sequence_async(cusbf::device_span<const char>{d_seq, len}, stream);
+        return r ? 0 : 1;
+    });
+}
+
+int sbf_refgpu_contains_async(void* p, const char* d_seq, uint64_t len, uint8_t* d_out,
+                              uint64_t out_len, cudaStream_t stream) {
+    return with(static_cast<Handle*>(p), [&](auto& f) {
+        auto r = f.contains_sequence_async(cusbf::device_span<const char>{d_seq, len},
+                                           cusbf::device_span<uint8_t>{d_out, out_len}, stream);
+        return r ? 0 : 1;
+    });
+}
+
+const void* sbf_refgpu_words(void* p) {
+    const void* out = nullptr;
+    with(static_cast<Handle*>(p), [&](auto& f) {
+        out = shard_ptr(f);
+        return 0;
+    });
+    return out;
+}
+
+uint64_t sbf_refgpu_num_shards(void* p) {
+    uint64_t out = 0;
+    with(static_cast<Handle*>(p), [&](auto& f) {
+        out = f.num_shards();
+        return 0;
+    });
+    return out;
+}
+}
