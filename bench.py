@@ -1,0 +1,509 @@
+"""Benchmark of the Super Bloom engine: k-mers/s insert + query at k=31.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c3|c2|c1]
+                    [--impl ours|reference] [--scale S]
+
+Workload (default `c3`, the configuration the metric is quoted on): a seeded
+synthetic genome of 3.1 Gbp in 24 records of 46-248 Mbp at GC 41%, ~50%
+covered by diverged copies (5-20%) of 2000 repeat units of 300 bp-6 kbp and
+5% by tandem repeats, inserted into a filter of 21.4 bits per k-mer (2^36
+bits, 8 GiB); then 100M reads of 150 bp, half sampled from the genome with 1%
+substitutions and half uniform random, are queried.  k=31, s=28, m=16, 4
+hashes.  No public dataset is used; the inputs are seeded stand-ins with the
+configuration's shapes.
+
+One step = clear the filter, insert every genome record (one launch over the
+records joined with separator bases), query every read (one launch over the
+reads joined with separators; one result byte per window).  Inputs stay
+resident in HBM; they are far larger than the 126 MB L2, so no flush is
+needed between steps.  `value` = valid k-mers inserted + queried per second
+of device time (CUDA events on the launching stream), summed over ranks
+(weak scaling: every rank holds its own filter and workload, seeded by
+rank), over the max time across ranks.
+
+`e2e` times the same step through the public host API with pinned host
+buffers: sbf_insert_sequence (host genome) + sbf_contains_sequence (host
+reads -> host result bytes), so every host<->device copy is inside it.
+
+`--impl reference` times the reference cuSBF path's own arithmetic on the
+host cores (oracle/_ref, built from the reference headers; the C oracle
+port when that is absent) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "k-mers/s insert+query (3.1 Gbp, k=31); ragged-batch & served p50/p99 vs plain"
+K, S, M, H = 31, 28, 16, 4
+
+
+# ---------------------------------------------------------------------------
+# Workloads
+# ---------------------------------------------------------------------------
+
+def workload_spec(name: str, scale: float) -> dict:
+    if name == "c3":
+        return dict(name="plain-large", genome_bp=int(3.1e9 * scale), n_records=24,
+                    rec_lo=int(46e6 * scale), rec_hi=int(248e6 * scale), gc=0.41,
+                    features=dict(interspersed_frac=0.5, tandem_frac=0.05),
+                    bits_per_kmer=21.4, n_reads=int(100e6 * scale), read_len=150,
+                    positive_frac=0.5, sub_rate=0.01)
+    if name == "c2":
+        return dict(name="plain-genome-small", genome_bp=int(100e6 * scale), n_records=6,
+                    rec_lo=int(13e6 * scale), rec_hi=int(21e6 * scale), gc=0.36,
+                    features=dict(tandem_frac=0.03, n_run_frac=0.001),
+                    bits_per_kmer=21.4, n_reads=int(20e6 * scale), read_len=150,
+                    positive_frac=0.5, sub_rate=0.01)
+    if name == "c1":
+        return dict(name="plain-small", genome_bp=int(2e6 * scale), n_records=1,
+                    rec_lo=int(2e6 * scale), rec_hi=int(2e6 * scale), gc=0.5, features={},
+                    bits_per_kmer=85.7, n_reads=0, read_len=150, positive_frac=0.5,
+                    sub_rate=0.0, fresh_query_bp=int(2e6 * scale))
+    raise SystemExit(f"unknown config {name}")
+
+
+def build_host_genome(spec: dict, seed: int):
+    from cusbf_b200.synthetic import (genome_records, join_records, record_lengths,
+                                      uniform_dna)
+
+    if spec["n_records"] == 1 and not spec["features"]:
+        recs = [uniform_dna(spec["genome_bp"], seed=seed, gc=spec["gc"])]
+    else:
+        lens = record_lengths(spec["genome_bp"], spec["n_records"], spec["rec_lo"],
+                              spec["rec_hi"], seed=seed)
+        recs = genome_records(spec["genome_bp"], spec["n_records"], seed=seed, gc=spec["gc"],
+                              lengths=lens, processes=min(len(lens), os.cpu_count() or 1),
+                              **spec["features"])
+    joined, ranges = join_records(recs)
+    valid = int(sum(max(0, r.size - K + 1) for r in recs))
+    return joined, ranges, valid
+
+
+def valid_windows(seq: np.ndarray) -> int:
+    """Windows of `seq` whose K bases are all A/C/G/T (any case)."""
+    up = seq & 0xDF
+    ok = (up == ord("A")) | (up == ord("C")) | (up == ord("G")) | (up == ord("T"))
+    if seq.size < K:
+        return 0
+    c = np.concatenate([[0], np.cumsum(~ok, dtype=np.int64)])
+    return int(np.count_nonzero(c[K:] - c[:-K] == 0))
+
+
+def sample_runs(seq: np.ndarray, n_shards: int) -> tuple[int, int]:
+    """Super-k-mer runs and valid windows of `seq` (the R and N of the
+    algorithmic-bytes model), counted by the oracle."""
+    from oracle.oracle import Oracle
+
+    return Oracle(K, S, M, H).count_runs(seq, n_shards)
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=5)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# Reference arm: the reference's arithmetic on the host cores
+# ---------------------------------------------------------------------------
+
+def cpu_reference_run(joined: np.ndarray, reads_joined: np.ndarray | None, n_shards: int,
+                      steps: int, warmup: int, sample_bp: int, sample_reads_bytes: int,
+                      threads: int) -> dict:
+    from oracle import oracle as o
+
+    if o.RefCpu.available():
+        impl, kind = o.RefCpu(K, S, M, H, threads=threads), "reference"
+        desc = ("oracle/_ref: the reference cuSBF host-callable arithmetic (encode, "
+                "extractPackedSubwindow, minimizer_hash64, hash64, sectorizedBitAddress) "
+                "driven window by window, std::thread over all host cores")
+    else:
+        impl, kind = o.Oracle(K, S, M, H, threads=threads), "port"
+        desc = "oracle/sbf_oracle.c: C restatement of the reference semantics, pthreads"
+    ins = joined[:sample_bp]
+    qry = reads_joined[:sample_reads_bytes] if reads_joined is not None else joined[:sample_bp]
+    n_ins = valid_windows(ins)
+    n_q = valid_windows(qry)
+    words = np.zeros(n_shards * 4, dtype=np.uint64)
+    times = []
+    for i in range(warmup + steps):
+        words[:] = 0
+        t0 = time.perf_counter()
+        impl.insert(words, ins)
+        impl.contains(words, qry)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            times.append(dt)
+    per = float(np.mean(times))
+    return dict(value=(n_ins + n_q) / per, unit="k-mers/s", cores=threads, kind=kind,
+                sample=f"{ins.size / 1e6:.1f} Mbp of the genome inserted + "
+                       f"{qry.size / 1e6:.1f} MB of joined reads queried "
+                       f"({n_ins + n_q:,} valid k-mers) per step, filter {n_shards * 32 >> 20} MiB; "
+                       + desc,
+                ms_per_step=per * 1e3, kmers_per_step=n_ins + n_q)
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# Main
+# ---------------------------------------------------------------------------
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="size multiplier for small profiling runs (1.0 = the named config)")
+    ap.add_argument("--seed", type=int, default=42)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours" and args.scale == 1.0:
+        print("note: at least 3 warm-up steps are used for reported numbers", file=sys.stderr)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    spec = workload_spec(args.config, args.scale)
+
+    # Host data is generated before any CUDA call (the generator may fork a
+    # spawn pool).
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference_arm(args, spec, world)
+        return
+    joined, ranges, n_ins_valid = build_host_genome(spec, seed=args.seed + 1000 * rank)
+
+    import torch
+
+    import cusbf_b200 as sbf
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream(dev)
+
+    n_kmers_genome = max(0, joined.size - K + 1)
+    requested_bits = int(round(spec["bits_per_kmer"] * n_ins_valid))
+    f = sbf.Filter(requested_bits, k=K, s=S, m=M, hashes=H)
+    n_shards = f.num_shards()
+
+    d_genome = torch.from_numpy(joined).to(dev)
+    from cusbf_b200.synthetic import SEPARATOR, reads_device, uniform_dna
+
+    if spec["n_reads"] > 0:
+        reads = reads_device(d_genome, spec["n_reads"], spec["read_len"],
+                             seed=args.seed + 7 + 1000 * rank, sub_rate=spec["sub_rate"],
+                             positive_frac=spec["positive_frac"], device=str(dev))
+        rl = spec["read_len"]
+        d_query = torch.full((spec["n_reads"], rl + 1), SEPARATOR, dtype=torch.uint8, device=dev)
+        d_query[:, :rl] = reads
+        d_query = d_query.reshape(-1)[:-1].contiguous()
+        del reads
+        n_q_valid = spec["n_reads"] * (rl - K + 1)
+    else:
+        fresh = uniform_dna(spec["fresh_query_bp"], seed=1337, gc=spec["gc"])
+        q_host = np.concatenate([joined, np.frombuffer(b"N", np.uint8), fresh])
+        d_query = torch.from_numpy(q_host).to(dev)
+        n_q_valid = valid_windows(q_host)
+    n_q_windows = f.kmer_count(d_query.numel())
+    d_out = torch.empty(max(n_q_windows, 1), dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize(dev)
+
+    def step(ev):
+        f.clear(stream)  # synchronous, outside the insert/query events
+        ev[0].record(stream)
+        f.insert_sequence_async(d_genome, stream)
+        ev[1].record(stream)
+        f.contains_sequence_async(d_query, d_out, stream)
+        ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step([torch.cuda.Event(enable_timing=True) for _ in range(3)])
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    t_start.record(stream)
+    for i in range(args.steps):
+        step(evs[i])
+    t_end.record(stream)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    clock_info = clocks.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    ins_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
+    q_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
+    kmers_step = n_ins_valid + n_q_valid
+
+    # Max over ranks of the timed region; sum of the work.
+    if dist:
+        t = torch.tensor([total_ms, ins_ms, q_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, ins_ms, q_ms = (float(x) for x in t.tolist())
+    ms_per_step = total_ms / args.steps
+    value = world * kmers_step / (ms_per_step / 1e3)
+
+    # Parity spot check of this run against the oracle on a slice.
+    positives = int(d_out.sum(dtype=torch.int64).item())
+
+    # End-to-end through the host API with pinned buffers.
+    e2e = None
+    if not args.no_e2e:
+        h_genome = torch.from_numpy(joined).pin_memory()
+        h_query = torch.empty(d_query.numel(), dtype=torch.uint8).pin_memory()
+        h_query.copy_(d_query)
+        h_out = torch.empty(max(n_q_windows, 1), dtype=torch.uint8).pin_memory()
+        gnp, qnp, onp = h_genome.numpy(), h_query.numpy(), h_out.numpy()
+
+        def e2e_step():
+            f.clear(stream)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            w0 = time.perf_counter()
+            a.record(stream)
+            f.insert_sequence(gnp, stream)
+            sbf._check(sbf._lib.sbf_contains_sequence(f.handle, qnp.ctypes.data, qnp.size,
+                                                       onp.ctypes.data, n_q_windows,
+                                                       stream.cuda_stream))
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            return a.elapsed_time(b), (time.perf_counter() - w0) * 1e3
+
+        e2e_step()
+        if dist:
+            dist.barrier()
+        res = [e2e_step() for _ in range(max(1, args.e2e_steps))]
+        e_ms = float(np.mean([r[0] for r in res]))
+        e_wall = float(np.mean([r[1] for r in res]))
+        if dist:
+            t = torch.tensor([e_ms, e_wall], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms, e_wall = (float(x) for x in t.tolist())
+        assert int(h_out[:n_q_windows].sum(dtype=torch.int64)) == positives, \
+            "host-API query disagrees with the device-resident query"
+        e2e = {"value": world * kmers_step / (max(e_ms, e_wall) / 1e3), "unit": "k-mers/s",
+               "h2d_bytes_per_step": int(joined.size + qnp.size),
+               "d2h_bytes_per_step": int(n_q_windows), "ms_per_step": max(e_ms, e_wall),
+               "steps": len(res),
+               "api": "sbf_insert_sequence + sbf_contains_sequence (host buffers, pinned)"}
+
+    if rank != 0:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    # Roofline of the dominant kernel (query) and of insert: algorithmic bytes
+    # from runs counted by the oracle on samples of this workload.
+    q_sample = d_query[: min(d_query.numel(), 3_000_000)].cpu().numpy()
+    runs_q, valid_q = sample_runs(q_sample, n_shards)
+    r_per_q = runs_q / max(valid_q, 1)
+    g_sample = joined[: min(joined.size, 6_000_000)]
+    runs_i, valid_i = sample_runs(g_sample, n_shards)
+    r_per_i = runs_i / max(valid_i, 1)
+    q_bytes = d_query.numel() + n_q_windows + 32 * r_per_q * n_q_valid
+    i_bytes = joined.size + 64 * r_per_i * n_ins_valid
+    peaks = {}
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peaks = json.load(open(peaks_path))
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    traffic = None
+    tr_path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tr_path):
+        tr = json.load(open(tr_path))
+        if "query_bytes_per_window" in tr:
+            traffic = tr["query_bytes_per_window"] * n_q_windows
+    q_achieved = q_bytes / (q_ms / 1e3) / 1e9
+    i_achieved = i_bytes / (ins_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "query (tile_kernel<31,28,16,4> query, bytes)",
+                "achieved": round(q_achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(q_achieved / peak, 4), "peak_source": peak_src,
+                "traffic": traffic,
+                "algorithmic_bytes": int(q_bytes),
+                "model": "L + N + 32R (input bytes + one output byte per window + one 32-byte "
+                         f"sector per super-k-mer run; R/N={r_per_q:.4f} counted by the oracle "
+                         "on a 3 MB sample)",
+                "insert": {"achieved": round(i_achieved, 1), "frac": round(i_achieved / peak, 4),
+                           "algorithmic_bytes": int(i_bytes),
+                           "model": f"L + 64R (R/N={r_per_i:.4f} counted on a 6 Mbp sample)"}}
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = cpu_reference_run(joined, q_sample, n_shards, steps=2, warmup=1,
+                                sample_bp=min(joined.size, 8_000_000),
+                                sample_reads_bytes=min(q_sample.size, 3_000_000),
+                                threads=host_cores())
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "k-mers/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded stand-in with the configuration's shapes; no public genome)",
+        "config": {
+            "workload": f"{spec['name']}: {spec['genome_bp'] / 1e9:.3g} Gbp in "
+                        f"{spec['n_records']} records inserted, {spec['n_reads']:,} x "
+                        f"{spec['read_len']} bp reads queried",
+            "k": K, "s": S, "m": M, "hashes": H, "filter_bits": f.filter_bits(),
+            "bits_per_kmer_requested": spec["bits_per_kmer"],
+            "insert_kmers": n_ins_valid, "query_kmers": n_q_valid,
+            "query_windows": n_q_windows, "parallelism": f"replicas x{world} (weak)",
+            "l2": "inputs larger than L2 (no flush needed)",
+            "step": "clear (untimed memset inside the step) + insert launch + query launch",
+        },
+        "insert": {"ms": ins_ms, "kmers_per_s": n_ins_valid / (ins_ms / 1e3)},
+        "query": {"ms": q_ms, "kmers_per_s": n_q_valid / (q_ms / 1e3),
+                  "positives": positives},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": 2 * args.steps,
+        "clocks": clock_info,
+    }
+    print(json.dumps(line), flush=True)
+    f.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference_arm(args, spec, world) -> None:
+    """The reference's own CPU implementation of the path (rank 0 only), on
+    a bounded sample: the start of the workload's first genome record and
+    20,000 reads sampled from it, with the full workload's filter size."""
+    from cusbf_b200.synthetic import (SEPARATOR, genome_record, reads_host, record_lengths,
+                                      uniform_dna)
+    from oracle.oracle import num_shards
+
+    if spec["n_records"] == 1 and not spec["features"]:
+        joined = uniform_dna(spec["genome_bp"], seed=args.seed, gc=spec["gc"])
+    else:
+        lens = record_lengths(spec["genome_bp"], spec["n_records"], spec["rec_lo"],
+                              spec["rec_hi"], seed=args.seed)
+        joined = genome_record(0, min(lens[0], 8_000_000), args.seed, gc=spec["gc"],
+                               **spec["features"])
+    n_valid_full = spec["genome_bp"] - spec["n_records"] * (K - 1)
+    shards = num_shards(int(round(spec["bits_per_kmer"] * n_valid_full)))
+    reads_joined = None
+    if spec["n_reads"] > 0:
+        n = min(spec["n_reads"], 20_000)
+        rd = reads_host([joined], n, spec["read_len"], seed=args.seed + 7,
+                        sub_rate=spec["sub_rate"], positive_frac=spec["positive_frac"])
+        q = np.full((n, spec["read_len"] + 1), SEPARATOR, dtype=np.uint8)
+        q[:, :-1] = rd
+        reads_joined = q.reshape(-1)[:-1]
+    res = cpu_reference_run(joined, reads_joined, shards, steps=args.steps,
+                            warmup=args.warmup, sample_bp=min(joined.size, 4_000_000),
+                            sample_reads_bytes=reads_joined.size if reads_joined is not None else 0,
+                            threads=host_cores())
+    line = {
+        "metric": METRIC, "value": res["value"], "unit": "k-mers/s", "impl": "reference",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded stand-in with the configuration's shapes; no public genome)",
+        "config": {"workload": f"{spec['name']}: bounded sample per step (see cpu_baseline)",
+                   "k": K, "s": S, "m": M, "hashes": H, "filter_shards": shards},
+        "cpu_baseline": {"value": res["value"], "unit": "k-mers/s", "cores": res["cores"],
+                         "kind": res["kind"], "sample": res["sample"]},
+        "e2e": {"value": res["value"], "unit": "k-mers/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -8,11 +8,14 @@
 namespace sbf {
 
 // Launch geometry of the tile kernels.
-constexpr int kThreads = 256;                       // threads per CTA
-constexpr int kStrip = 16;                          // consecutive k-mers per thread
-constexpr int kTileKmers = kThreads * kStrip;       // k-mers per tile (4096)
-constexpr int kCodeWords = kThreads + 2;            // 16-base code words per tile
-constexpr int kStageBytes = kTileKmers + 64 + 32;   // staged input bytes per buffer
+constexpr int kThreads = 256;                          // threads per CTA
+constexpr int kStrip = 32;                             // consecutive k-mers per thread
+constexpr int kTileKmers = kThreads * kStrip;          // k-mers per tile (8192)
+constexpr int kStripWords = kStrip / 16 + 2;           // code words one strip reads
+constexpr int kCodeWords = (kThreads - 1) * (kStrip / 16) + kStripWords;  // per tile
+constexpr int kStageBytes = kCodeWords * 16 + 64;      // staged input bytes per buffer
+constexpr int kSlots = 10;                             // query shard slots per thread
+constexpr int kQuerySlotBytes = kSlots * kThreads * 32;  // dynamic smem of query kernels
 
 // One launch of a tile kernel.  Grid position g of tile n is
 // g = n * kTileKmers + (0 .. kTileKmers-1); it holds window (k-mer)

@@ -162,78 +162,85 @@ __device__ __forceinline__ void encode_word(const TileGeom& g, const uint8_t* bu
     }
 }
 
+// Expands the four low bits of `nib` into four 0/1 bytes (bit r -> byte r).
+__device__ __forceinline__ uint32_t spread4(uint32_t nib) {
+    return (nib * 0x00204081u) & 0x01010101u;
+}
+
 // ---------------------------------------------------------------------------
-// Strip computation: 16 windows per thread
+// Strip computation: kStrip consecutive windows per thread
 // ---------------------------------------------------------------------------
 
-template <class C>
-struct Strip {
-    uint32_t shard[kStrip];
-    uint32_t vmask;  // bit j: window j is in range and holds only valid bases
-};
-
-// A[r]: the 16 bases starting at strip position r, earliest base in bits 31:30.
-__device__ __forceinline__ uint32_t win16(uint32_t c0, uint32_t c1, uint32_t c2, int r) {
-    return r < 16 ? __funnelshift_l(c1, c0, 2 * r) : __funnelshift_l(c2, c1, 2 * (r - 16));
+// The 16 bases starting at strip position r, earliest base in bits 31:30.
+// `c` holds the strip's code words; r is a compile-time constant after
+// unrolling, so every access is a register.
+__device__ __forceinline__ uint32_t win16(const uint32_t* c, int r) {
+    const int q = r >> 4, s = r & 15;
+    return s == 0 ? c[q] : __funnelshift_l(c[q + 1], c[q], 2 * s);
 }
 
 template <class C>
-__device__ __forceinline__ uint64_t smer_at(uint32_t c0, uint32_t c1, uint32_t c2, int r) {
+__device__ __forceinline__ uint64_t mh_at(const uint32_t* c, int r) {
+    return mmer_hash(win16(c, r) >> (2 * (16 - C::M)));
+}
+
+template <class C>
+__device__ __forceinline__ uint64_t smer_at(const uint32_t* c, int r) {
     if constexpr (C::S > 16) {
-        const uint64_t hi = win16(c0, c1, c2, r) >> (2 * (32 - C::S));
-        return (hi << 32) | win16(c0, c1, c2, r + C::S - 16);
+        const uint64_t hi = win16(c, r) >> (2 * (32 - C::S));
+        return (hi << 32) | win16(c, r + C::S - 16);
     } else {
-        return win16(c0, c1, c2, r) >> (2 * (16 - C::S));
+        return win16(c, r) >> (2 * (16 - C::S));
     }
 }
 
-template <class C>
-__device__ __forceinline__ void strip_shards(uint32_t c0, uint32_t c1, uint32_t c2,
-                                             uint32_t shard_mask, uint32_t* shard) {
+// Calls fn(j, shard) for the strip's windows j = 0..kStrip-1 in order.
+// For 16 m-mers per window the minimum is a Gil-Werman sliding minimum over
+// blocks of 16 positions: window j of block b is min(suffix_b[j],
+// prefix_{b+1}[j-1]), about three 64-bit comparisons per window.
+template <class C, class Fn>
+__device__ __forceinline__ void for_each_shard(const uint32_t* c, uint32_t shard_mask, Fn&& fn) {
     constexpr int W = C::W;
-    constexpr int NP = kStrip + W - 1;  // m-mer positions used by the strip
     if constexpr (W == 16) {
-        // Gil-Werman: suffix minima of block [0,16), running prefix minima
-        // of block [16, 31); window j = min(suffix[j], prefix[j-1]).
-        uint64_t suf[16];
-        suf[15] = mmer_hash(win16(c0, c1, c2, 15) >> (2 * (16 - C::M)));
 #pragma unroll
-        for (int r = 14; r >= 0; --r)
-            suf[r] = min64(mmer_hash(win16(c0, c1, c2, r) >> (2 * (16 - C::M))), suf[r + 1]);
-        shard[0] = static_cast<uint32_t>(suf[0]) & shard_mask;
-        uint64_t pre = ~uint64_t{0};
+        for (int b = 0; b < kStrip / 16; ++b) {
+            uint64_t suf[16];
+            suf[15] = mh_at<C>(c, 16 * b + 15);
 #pragma unroll
-        for (int j = 1; j < kStrip; ++j) {
-            pre = min64(pre, mmer_hash(win16(c0, c1, c2, 15 + j) >> (2 * (16 - C::M))));
-            shard[j] = static_cast<uint32_t>(min64(suf[j], pre)) & shard_mask;
+            for (int r = 14; r >= 0; --r) suf[r] = min64(mh_at<C>(c, 16 * b + r), suf[r + 1]);
+            fn(16 * b, static_cast<uint32_t>(suf[0]) & shard_mask);
+            uint64_t pre = ~uint64_t{0};
+#pragma unroll
+            for (int j = 1; j < 16; ++j) {
+                pre = min64(pre, mh_at<C>(c, 16 * b + 15 + j));
+                fn(16 * b + j, static_cast<uint32_t>(min64(suf[j], pre)) & shard_mask);
+            }
         }
     } else {
-        uint64_t mh[NP];
-#pragma unroll
-        for (int r = 0; r < NP; ++r) mh[r] = mmer_hash(win16(c0, c1, c2, r) >> (2 * (16 - C::M)));
 #pragma unroll
         for (int j = 0; j < kStrip; ++j) {
-            uint64_t v = mh[j];
+            uint64_t v = mh_at<C>(c, j);
 #pragma unroll
-            for (int o = 1; o < W; ++o) v = min64(v, mh[j + o]);
-            shard[j] = static_cast<uint32_t>(v) & shard_mask;
+            for (int o = 1; o < W; ++o) v = min64(v, mh_at<C>(c, j + o));
+            fn(j, static_cast<uint32_t>(v) & shard_mask);
         }
     }
 }
 
-// Valid-window mask of the strip: window j holds K valid bases and lies in
-// [0, n_kmers).
+// Valid-window mask: window j holds K valid bases and lies in [0, n_kmers).
+// inv[q] holds the invalid bits of code word q (bit r = base 16q + r).
 template <class C>
-__device__ __forceinline__ uint32_t strip_valid(uint32_t i0, uint32_t i1, uint32_t i2,
-                                                int64_t first_kmer, uint64_t n_kmers) {
-    uint32_t vmask = 0xFFFFu;
-    const uint64_t inv = static_cast<uint64_t>(i0) | (static_cast<uint64_t>(i1) << 16) |
-                         (static_cast<uint64_t>(i2) << 32);
-    constexpr uint64_t kWin = (C::K >= 64) ? ~uint64_t{0} : ((uint64_t{1} << C::K) - 1);
-    if (inv & ((uint64_t{1} << (15 + C::K)) - 1)) {
+__device__ __forceinline__ uint32_t strip_valid(const uint32_t* inv, int64_t first_kmer,
+                                                uint64_t n_kmers) {
+    uint32_t vmask = 0xFFFFFFFFu;
+    const uint64_t bits = static_cast<uint64_t>(inv[0]) | (static_cast<uint64_t>(inv[1]) << 16) |
+                          (static_cast<uint64_t>(inv[2]) << 32) |
+                          (static_cast<uint64_t>(inv[3]) << 48);
+    constexpr uint64_t kWin = (uint64_t{1} << C::K) - 1;
+    if (bits) {
 #pragma unroll
         for (int j = 0; j < kStrip; ++j)
-            if ((inv >> j) & kWin) vmask &= ~(1u << j);
+            if ((bits >> j) & kWin) vmask &= ~(1u << j);
     }
     if (first_kmer < 0 || first_kmer + kStrip > static_cast<int64_t>(n_kmers)) {
 #pragma unroll
@@ -245,99 +252,280 @@ __device__ __forceinline__ uint32_t strip_valid(uint32_t i0, uint32_t i1, uint32
     return vmask;
 }
 
-// Four word masks of the s-mer at strip position r.
+// One-hot word masks of the s-mer at strip position r.
 template <class C>
-__device__ __forceinline__ void smer_masks(uint32_t c0, uint32_t c1, uint32_t c2, int r,
-                                           uint64_t m[4]) {
-    const uint64_t h = smer_hash(smer_at<C>(c0, c1, c2, r));
+__device__ __forceinline__ void smer_masks(const uint32_t* c, int r, uint64_t m[4]) {
+    const uint64_t h = smer_hash(smer_at<C>(c, r));
     m[0] = m[1] = m[2] = m[3] = 0;
 #pragma unroll
     for (int j = 0; j < C::H; ++j) m[j & 3] |= uint64_t{1} << bit_address<C::H>(h, j);
 }
 
-// True when every bit of the s-mer at strip position r is set in w0..w3.
+__device__ __forceinline__ void flush_run(uint64_t* words, uint32_t shard, const uint64_t a[4]) {
+    uint64_t* dst = words + static_cast<uint64_t>(shard) * 4;
+    red_or(dst + 0, a[0]);
+    red_or(dst + 1, a[1]);
+    red_or(dst + 2, a[2]);
+    red_or(dst + 3, a[3]);
+}
+
+// Insert: the mask of window j is T_j = OR of the one-hot masks of its F
+// s-mers; a super-k-mer run (consecutive valid windows with equal shard)
+// accumulates acc = OR T_j and is flushed with one red.or per shard word when
+// the next window leaves the run.
 template <class C>
-__device__ __forceinline__ uint32_t smer_present(uint64_t h, uint64_t w0, uint64_t w1,
-                                                 uint64_t w2, uint64_t w3) {
-    uint64_t acc = ~uint64_t{0};
+__device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
+                                             uint32_t shard_mask, uint64_t* words) {
+    constexpr int F = C::F;
+    uint64_t acc[4] = {0, 0, 0, 0};
+    uint32_t prev_shard = 0;
+    bool prev_valid = false;
+    if constexpr (F == 4) {
+        // T_j = P_j | P_{j+2} with pair masks P_x = m_x | m_{x+1}.
+        uint64_t m0[4], m1[4], m2[4];
+        smer_masks<C>(c, 0, m0);
+        smer_masks<C>(c, 1, m1);
+        smer_masks<C>(c, 2, m2);
+        uint64_t pa[4], pb[4];
 #pragma unroll
-    for (int j = 0; j < C::H; ++j) {
-        const uint64_t w = (j & 3) == 0 ? w0 : (j & 3) == 1 ? w1 : (j & 3) == 2 ? w2 : w3;
-        acc &= w >> bit_address<C::H>(h, j);
+        for (int w = 0; w < 4; ++w) {
+            pa[w] = m0[w] | m1[w];
+            pb[w] = m1[w] | m2[w];
+        }
+        for_each_shard<C>(c, shard_mask, [&](int j, uint32_t shard) {
+            uint64_t m3[4];
+            smer_masks<C>(c, j + 3, m3);
+            const bool valid = (vmask >> j) & 1u;
+            const bool cont = valid && prev_valid && shard == prev_shard;
+            if (prev_valid && !cont) flush_run(words, prev_shard, acc);
+            const uint64_t keep = cont ? ~uint64_t{0} : uint64_t{0};
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                const uint64_t pc = m2[w] | m3[w];
+                acc[w] = (acc[w] & keep) | pa[w] | pc;
+                pa[w] = pb[w];
+                pb[w] = pc;
+                m2[w] = m3[w];
+            }
+            prev_shard = shard;
+            prev_valid = valid;
+        });
+    } else {
+        uint64_t ring[F][4];
+#pragma unroll
+        for (int o = 0; o < F - 1; ++o) smer_masks<C>(c, o, ring[o]);
+        for_each_shard<C>(c, shard_mask, [&](int j, uint32_t shard) {
+            smer_masks<C>(c, j + F - 1, ring[(j + F - 1) % F]);
+            const bool valid = (vmask >> j) & 1u;
+            const bool cont = valid && prev_valid && shard == prev_shard;
+            if (prev_valid && !cont) flush_run(words, prev_shard, acc);
+            const uint64_t keep = cont ? ~uint64_t{0} : uint64_t{0};
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                uint64_t t = ring[j % F][w];
+#pragma unroll
+                for (int o = 1; o < F; ++o) t |= ring[(j + o) % F][w];
+                acc[w] = (acc[w] & keep) | t;
+            }
+            prev_shard = shard;
+            prev_valid = valid;
+        });
     }
-    return static_cast<uint32_t>(acc) & 1u;
+    if (prev_valid) flush_run(words, prev_shard, acc);
+}
+
+// Query shard slots: the run heads of a strip fetch their 32-byte shards into
+// per-thread shared-memory slots with cp.async, all at once, so a thread has
+// every shard load of its strip in flight while it hashes the strip's s-mers.
+static_assert(kSlots * kThreads * 32 == kQuerySlotBytes, "slot geometry");
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(smem_dst)),
+                 "l"(gmem_src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+__device__ __forceinline__ void load_shard_now(const uint64_t* p, uint64_t w[4]) {
+    asm volatile("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];"
+                 : "=l"(w[0]), "=l"(w[1]), "=l"(w[2]), "=l"(w[3])
+                 : "l"(p));
+}
+
+// The H = 4 bit addresses of the s-mer at strip position r, one per byte:
+// byte j is the bit of shard word j.
+template <class C>
+__device__ __forceinline__ uint32_t smer_bytes4(const uint32_t* c, int r) {
+    const uint64_t h = smer_hash(smer_at<C>(c, r));
+    const uint32_t lo = static_cast<uint32_t>(h), hi = static_cast<uint32_t>(h >> 32);
+    // lo bits 0-5 -> word 0, lo bits 16-21 -> word 1, hi bits 0-5 -> word 2,
+    // hi bits 16-21 -> word 3.
+    const uint32_t a = lo & 0x003F003Fu;           // b0 in byte 0, b1 in byte 2
+    const uint32_t b = (hi & 0x003F003Fu) << 8;    // b2 in byte 1, b3 in byte 3
+    return __byte_perm(a | b, 0u, 0x3120u);        // bytes b0 b1 b2 b3
 }
 
 template <class C>
-__device__ __forceinline__ void insert_strip(uint32_t c0, uint32_t c1, uint32_t c2,
-                                             const uint32_t* shard, uint32_t vmask,
-                                             uint64_t* words) {
-    constexpr int F = C::F;
-    constexpr int NP = kStrip + F - 1;
-    uint64_t pm[NP][4];
+__device__ __forceinline__ uint32_t smer_present_h(uint64_t h, const uint64_t* w) {
+    uint32_t acc = 0xFFFFFFFFu;
 #pragma unroll
-    for (int r = 0; r < NP; ++r) smer_masks<C>(c0, c1, c2, r, pm[r]);
-    uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    for (int j = 0; j < C::H; ++j) acc &= static_cast<uint32_t>(w[j & 3] >> bit_address<C::H>(h, j));
+    return acc;
+}
+
+__device__ __forceinline__ void store_strip_bytes(uint32_t result, uint8_t* out, int64_t first_kmer,
+                                                  uint64_t n_kmers) {
+    if (first_kmer >= 0 && first_kmer + kStrip <= static_cast<int64_t>(n_kmers)) {
+        uint4 v0, v1;
+        v0.x = spread4(result & 0xFu);
+        v0.y = spread4((result >> 4) & 0xFu);
+        v0.z = spread4((result >> 8) & 0xFu);
+        v0.w = spread4((result >> 12) & 0xFu);
+        v1.x = spread4((result >> 16) & 0xFu);
+        v1.y = spread4((result >> 20) & 0xFu);
+        v1.z = spread4((result >> 24) & 0xFu);
+        v1.w = spread4(result >> 28);
+        uint4* dst = reinterpret_cast<uint4*>(out + first_kmer);
+        dst[0] = v0;
+        dst[1] = v1;
+    } else {
 #pragma unroll
-    for (int j = 0; j < kStrip; ++j) {
-        uint64_t t0 = pm[j][0], t1 = pm[j][1], t2 = pm[j][2], t3 = pm[j][3];
-#pragma unroll
-        for (int o = 1; o < F; ++o) {
-            t0 |= pm[j + o][0];
-            t1 |= pm[j + o][1];
-            t2 |= pm[j + o][2];
-            t3 |= pm[j + o][3];
-        }
-        const bool valid = (vmask >> j) & 1u;
-        const bool cont = j > 0 && ((vmask >> (j - 1)) & 1u) && shard[j] == shard[j - 1];
-        a0 = cont ? (a0 | t0) : t0;
-        a1 = cont ? (a1 | t1) : t1;
-        a2 = cont ? (a2 | t2) : t2;
-        a3 = cont ? (a3 | t3) : t3;
-        const bool next_cont =
-            j + 1 < kStrip && ((vmask >> (j + 1)) & 1u) && shard[j + 1] == shard[j];
-        if (valid && !next_cont) {
-            uint64_t* dst = words + static_cast<uint64_t>(shard[j]) * 4;
-            red_or(dst + 0, a0);
-            red_or(dst + 1, a1);
-            red_or(dst + 2, a2);
-            red_or(dst + 3, a3);
+        for (int j = 0; j < kStrip; ++j) {
+            const int64_t i = first_kmer + j;
+            if (i >= 0 && i < static_cast<int64_t>(n_kmers))
+                out[i] = static_cast<uint8_t>((result >> j) & 1u);
         }
     }
 }
 
+// Query of one strip without slots: each run head loads its shard when it is
+// reached.  Used for strips with more run heads than slots.
 template <class C>
-__device__ __forceinline__ uint32_t query_strip(uint32_t c0, uint32_t c1, uint32_t c2,
-                                                const uint32_t* shard, uint32_t vmask,
-                                                const uint64_t* words) {
+__device__ __noinline__ uint32_t query_strip_direct(const uint32_t* c, uint32_t vmask,
+                                                    uint32_t shard_mask, const uint64_t* words) {
     constexpr int F = C::F;
-    constexpr int NP = kStrip + F - 1;
-    uint64_t h[NP];
+    uint64_t ring[F];
 #pragma unroll
-    for (int r = 0; r < NP; ++r) h[r] = smer_hash(smer_at<C>(c0, c1, c2, r));
-    uint32_t result = 0;
-    uint64_t w0 = 0, w1 = 0, w2 = 0, w3 = 0;
+    for (int o = 0; o < F - 1; ++o) ring[o] = smer_hash(smer_at<C>(c, o));
+    uint64_t w[4] = {0, 0, 0, 0};
     bool have = false;
-    uint32_t cur = 0;
-#pragma unroll
-    for (int j = 0; j < kStrip; ++j) {
+    uint32_t cur = 0, result = 0;
+    for_each_shard<C>(c, shard_mask, [&](int j, uint32_t sh) {
+        ring[(j + F - 1) % F] = smer_hash(smer_at<C>(c, j + F - 1));
         const bool valid = (vmask >> j) & 1u;
-        const bool head = valid && (!have || shard[j] != cur);
-        if (head) {
-            load_shard(words + static_cast<uint64_t>(shard[j]) * 4, w0, w1, w2, w3);
-            cur = shard[j];
+        if (valid && (!have || sh != cur)) {
+            load_shard_now(words + static_cast<uint64_t>(sh) * 4, w);
+            cur = sh;
             have = true;
         }
         uint32_t present = valid ? 1u : 0u;
 #pragma unroll
-        for (int o = 0; o < F; ++o) present &= smer_present<C>(h[j + o], w0, w1, w2, w3);
-        result |= present << j;
-    }
+        for (int o = 0; o < F; ++o) present &= smer_present_h<C>(ring[(j + o) % F], w);
+        result |= (present & 1u) << j;
+    });
     return result;
 }
 
-__device__ __forceinline__ uint32_t spread4(uint32_t nib) {
-    return (nib * 0x00204081u) & 0x01010101u;
+// Query of one strip: minimizers -> cp.async of every run head's shard into
+// the thread's slots (issued as the heads are found) -> s-mer hashing while
+// the copies are in flight -> wait -> findere tests -> output bytes.
+template <class C>
+__device__ __forceinline__ void query_strip(const uint32_t* c, uint32_t vmask, uint32_t shard_mask,
+                                            const uint64_t* words, uint64_t* slot0,
+                                            uint8_t* out, int64_t first_kmer, uint64_t n_kmers) {
+    // Slot n of this thread lives at slot0 + n * kThreads * 4 ([slot][thread]
+    // layout: neighbouring threads touch neighbouring 32-byte slots).
+    constexpr int kSlotStride = kThreads * 4;
+    constexpr int F = C::F;
+    uint32_t heads = 0;
+    int n = 0;
+    {
+        bool have = false;
+        uint32_t cur = 0;
+        for_each_shard<C>(c, shard_mask, [&](int j, uint32_t sh) {
+            const bool valid = (vmask >> j) & 1u;
+            if (valid && (!have || sh != cur)) {
+                heads |= 1u << j;
+                if (n < kSlots) {
+                    const uint64_t* src = words + static_cast<uint64_t>(sh) * 4;
+                    uint64_t* dst = slot0 + n * kSlotStride;
+                    cp_async16(dst, src);
+                    cp_async16(dst + 2, src + 2);
+                }
+                ++n;
+                cur = sh;
+                have = true;
+            }
+        });
+    }
+    cp_async_commit();
+    if (n > kSlots) {
+        cp_async_wait_all();
+        store_strip_bytes(query_strip_direct<C>(c, vmask, shard_mask, words), out, first_kmer,
+                          n_kmers);
+        return;
+    }
+    // Hash the strip's s-mers while the shard copies are in flight.
+    constexpr int NP = kStrip + F - 1;
+    uint32_t bytes[C::H == 4 ? NP : 1];
+    uint64_t hs[C::H == 4 ? 1 : NP];
+#pragma unroll
+    for (int r = 0; r < NP; ++r) {
+        if constexpr (C::H == 4)
+            bytes[r] = smer_bytes4<C>(c, r);
+        else
+            hs[r] = smer_hash(smer_at<C>(c, r));
+    }
+    cp_async_wait_all();
+    uint64_t w[4] = {0, 0, 0, 0};
+    uint32_t result = 0;
+    n = 0;
+    // Bit addresses of the F positions of the current window, extracted once
+    // per position as it enters the window.
+    uint32_t ring[C::H == 4 ? F : 1][4];
+    if constexpr (C::H == 4) {
+#pragma unroll
+        for (int o = 0; o < F - 1; ++o) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) ring[o][q] = __byte_perm(bytes[o], 0u, 0x4440u + q);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kStrip; ++j) {
+        if constexpr (C::H == 4) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                ring[(j + F - 1) % F][q] = __byte_perm(bytes[j + F - 1], 0u, 0x4440u + q);
+        }
+        if ((heads >> j) & 1u) {
+            const uint64_t* sn = slot0 + n * kSlotStride;
+            const uint4 lo = *reinterpret_cast<const uint4*>(sn);
+            const uint4 hi = *reinterpret_cast<const uint4*>(sn + 2);
+            w[0] = (static_cast<uint64_t>(lo.y) << 32) | lo.x;
+            w[1] = (static_cast<uint64_t>(lo.w) << 32) | lo.z;
+            w[2] = (static_cast<uint64_t>(hi.y) << 32) | hi.x;
+            w[3] = (static_cast<uint64_t>(hi.w) << 32) | hi.z;
+            ++n;
+        }
+        uint32_t present = (vmask >> j) & 1u;
+#pragma unroll
+        for (int o = 0; o < F; ++o) {
+            if constexpr (C::H == 4) {
+                const uint32_t* b = ring[(j + o) % F];
+                present &= static_cast<uint32_t>(w[0] >> b[0]) & static_cast<uint32_t>(w[1] >> b[1]) &
+                           static_cast<uint32_t>(w[2] >> b[2]) & static_cast<uint32_t>(w[3] >> b[3]);
+            } else {
+                present &= smer_present_h<C>(hs[j + o], w);
+            }
+        }
+        result |= (present & 1u) << j;
+    }
+    store_strip_bytes(result, out, first_kmer, n_kmers);
 }
 
 // ---------------------------------------------------------------------------
@@ -345,10 +533,10 @@ __device__ __forceinline__ uint32_t spread4(uint32_t nib) {
 // ---------------------------------------------------------------------------
 
 template <class C, bool kQuery, bool kDense>
-__global__ void __launch_bounds__(kThreads) tile_kernel(TileParams p) {
+__global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
     __shared__ alignas(128) uint8_t stage[2][kStageBytes];
-    __shared__ uint32_t code[kCodeWords + 2];
-    __shared__ uint32_t inval[kCodeWords + 2];
+    __shared__ uint32_t code[kCodeWords + 4];
+    __shared__ uint32_t inval[kCodeWords + 4];
     __shared__ alignas(8) uint64_t bars[2];
 
     const int tid = threadIdx.x;
@@ -365,6 +553,9 @@ __global__ void __launch_bounds__(kThreads) tile_kernel(TileParams p) {
         if (tile < p.n_tiles) issue_stage<kDense>(p, tile, stage[0], &bars[0]);
         if (tile + stride < p.n_tiles) issue_stage<kDense>(p, tile + stride, stage[1], &bars[1]);
     }
+    // Per-thread shard slots of the query kernel, [slot][thread] layout, in
+    // dynamic shared memory (kQuerySlotBytes per CTA).
+    extern __shared__ __align__(16) uint64_t slots[];
     uint32_t it = 0;
     for (; tile < p.n_tiles; tile += stride, ++it) {
         const int b = it & 1;
@@ -390,32 +581,19 @@ __global__ void __launch_bounds__(kThreads) tile_kernel(TileParams p) {
         if (tid == 0 && tile + 2 * stride < p.n_tiles)
             issue_stage<kDense>(p, tile + 2 * stride, stage[b], &bars[b]);
 
-        const uint32_t c0 = code[tid], c1 = code[tid + 1], c2 = code[tid + 2];
-        const int64_t first_kmer = g.s0 + static_cast<int64_t>(tid) * kStrip;
-        const uint32_t vmask =
-            strip_valid<C>(inval[tid], inval[tid + 1], inval[tid + 2], first_kmer, p.n_kmers);
-        uint32_t shard[kStrip];
-        strip_shards<C>(c0, c1, c2, p.shard_mask, shard);
-        if constexpr (kQuery) {
-            const uint32_t res = query_strip<C>(c0, c1, c2, shard, vmask, p.words);
-            // Windows outside [0, n_kmers) are not written; the rest get 0/1.
-            if (first_kmer >= 0 && first_kmer + kStrip <= static_cast<int64_t>(p.n_kmers)) {
-                uint4 v;
-                v.x = spread4(res & 0xFu);
-                v.y = spread4((res >> 4) & 0xFu);
-                v.z = spread4((res >> 8) & 0xFu);
-                v.w = spread4((res >> 12) & 0xFu);
-                *reinterpret_cast<uint4*>(p.out + first_kmer) = v;
-            } else {
+        uint32_t c[kStripWords], iv[kStripWords];
 #pragma unroll
-                for (int j = 0; j < kStrip; ++j) {
-                    const int64_t i = first_kmer + j;
-                    if (i >= 0 && i < static_cast<int64_t>(p.n_kmers))
-                        p.out[i] = static_cast<uint8_t>((res >> j) & 1u);
-                }
-            }
+        for (int q = 0; q < kStripWords; ++q) {
+            c[q] = code[tid * (kStrip / 16) + q];
+            iv[q] = inval[tid * (kStrip / 16) + q];
+        }
+        const int64_t first_kmer = g.s0 + static_cast<int64_t>(tid) * kStrip;
+        const uint32_t vmask = strip_valid<C>(iv, first_kmer, p.n_kmers);
+        if constexpr (kQuery) {
+            query_strip<C>(c, vmask, p.shard_mask, p.words, slots + 4 * tid, p.out, first_kmer,
+                           p.n_kmers);
         } else {
-            if (vmask) insert_strip<C>(c0, c1, c2, shard, vmask, p.words);
+            if (vmask) insert_strip<C>(c, vmask, p.shard_mask, p.words);
         }
     }
 }

@@ -70,58 +70,76 @@ def record_lengths(total_bp: int, n_records: int, lo: int, hi: int, seed: int) -
     return [int(x) for x in lens]
 
 
-def genome_records(total_bp: int, n_records: int, seed: int, gc: float = 0.41,
-                   tandem_frac: float = 0.0, n_run_frac: float = 0.0,
-                   interspersed_frac: float = 0.0, n_units: int = 2000,
-                   unit_len: tuple[int, int] = (300, 6000),
-                   divergence: tuple[float, float] = (0.05, 0.20),
-                   lengths: list[int] | None = None) -> list[np.ndarray]:
-    """Genome-like records.
+def _repeat_units(seed: int, n_units: int, unit_len: tuple[int, int], gc: float) -> list[np.ndarray]:
+    rng = np.random.default_rng([seed, 0xFA11])
+    return [uniform_dna(int(rng.integers(unit_len[0], unit_len[1] + 1)), seed=0, gc=gc, rng=rng)
+            for _ in range(n_units)]
+
+
+def genome_record(index: int, length: int, seed: int, gc: float = 0.41,
+                  tandem_frac: float = 0.0, n_run_frac: float = 0.0,
+                  interspersed_frac: float = 0.0, n_units: int = 2000,
+                  unit_len: tuple[int, int] = (300, 6000),
+                  divergence: tuple[float, float] = (0.05, 0.20)) -> np.ndarray:
+    """Record `index` of a genome-like workload (seeded by (seed, index)).
 
     * background: i.i.d. bases at GC fraction `gc`;
-    * interspersed repeats: copies of `n_units` seeded repeat units (lengths
-      uniform in `unit_len`), each copy substituted at a divergence drawn from
-      `divergence`, placed until `interspersed_frac` of the bases are covered;
+    * interspersed repeats: copies of `n_units` repeat units shared by all
+      records (seeded by `seed`, lengths uniform in `unit_len`), each copy
+      substituted at a divergence drawn from `divergence`, placed until
+      `interspersed_frac` of the record is covered;
     * tandem repeats: regions of 100-2000 bp filled with a period-2..200 unit;
-    * N runs of 10-1000 bp covering `n_run_frac` of the bases.
+    * N runs of 10-1000 bp covering `n_run_frac` of the record.
     """
-    rng = np.random.default_rng(seed)
-    if lengths is None:
-        lengths = [total_bp // n_records] * n_records
-        lengths[-1] += total_bp - sum(lengths)
-    recs = [uniform_dna(L, seed=0, gc=gc, rng=rng) for L in lengths]
-    total = sum(lengths)
-    cum = np.cumsum([0] + lengths)
+    rng = np.random.default_rng([seed, index])
+    rec = uniform_dna(length, seed=0, gc=gc, rng=rng)
 
     def place(n_bases_target: int, make_piece):
         covered = 0
         while covered < n_bases_target:
             piece = make_piece()
-            r = int(np.searchsorted(cum, rng.integers(0, total), side="right") - 1)
-            L = recs[r].size
-            if piece.size >= L:
-                continue
-            p = int(rng.integers(0, L - piece.size))
-            recs[r][p:p + piece.size] = piece
+            if piece.size >= length:
+                break
+            p = int(rng.integers(0, length - piece.size))
+            rec[p:p + piece.size] = piece
             covered += piece.size
 
     if interspersed_frac > 0:
-        units = [uniform_dna(int(rng.integers(unit_len[0], unit_len[1] + 1)), seed=0, gc=gc,
-                             rng=rng) for _ in range(n_units)]
-        place(int(interspersed_frac * total),
+        units = _repeat_units(seed, n_units, unit_len, gc)
+        place(int(interspersed_frac * length),
               lambda: _mutate(units[int(rng.integers(0, n_units))],
                               float(rng.uniform(*divergence)), rng))
     if tandem_frac > 0:
         def tandem():
             period = int(rng.integers(2, 201))
             unit = uniform_dna(period, seed=0, gc=gc, rng=rng)
-            length = int(rng.integers(100, 2001))
-            return np.resize(unit, length)
-        place(int(tandem_frac * total), tandem)
+            return np.resize(unit, int(rng.integers(100, 2001)))
+        place(int(tandem_frac * length), tandem)
     if n_run_frac > 0:
-        place(int(n_run_frac * total),
+        place(int(n_run_frac * length),
               lambda: np.full(int(rng.integers(10, 1001)), SEPARATOR, dtype=np.uint8))
-    return recs
+    return rec
+
+
+def _record_job(args):
+    return genome_record(*args[0], **args[1])
+
+
+def genome_records(total_bp: int, n_records: int, seed: int, gc: float = 0.41,
+                   lengths: list[int] | None = None, processes: int = 1,
+                   **features) -> list[np.ndarray]:
+    """Genome-like records (see genome_record); `processes` > 1 builds them in
+    a spawn-context process pool (start it before any CUDA call)."""
+    if lengths is None:
+        lengths = [total_bp // n_records] * n_records
+        lengths[-1] += total_bp - sum(lengths)
+    jobs = [((i, L, seed, gc), features) for i, L in enumerate(lengths)]
+    if processes > 1 and len(jobs) > 1:
+        import multiprocessing as mp
+
+        with mp.get_context("spawn").Pool(min(processes, len(jobs))) as pool:
+            return pool.map(_record_job, jobs)
+    return [_record_job(j) for j in jobs]
 
 
 def join_records(records: list[np.ndarray]) -> tuple[np.ndarray, np.ndarray]:
