@@ -153,7 +153,7 @@ int sbf_filter::launch(bool query, bool dense, const void* input, uint64_t input
                                           : ks->query_dense;
     const uint64_t resident = static_cast<uint64_t>(sms) * static_cast<uint64_t>(occupancy[which]);
     const uint64_t grid = std::min<uint64_t>(p.n_tiles, std::max<uint64_t>(resident, 1));
-    fn<<<static_cast<unsigned>(grid), kThreads, query ? kQuerySlotBytes : 0, st>>>(p);
+    fn<<<static_cast<unsigned>(grid), kThreads, query ? kQuerySlotBytes : kInsertSlotBytes, st>>>(p);
     SBF_CUDA(cudaGetLastError());
     ++launches;
     return SBF_OK;
@@ -301,7 +301,8 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
         void (*fns[4])(TileParams) = {ks->insert_bytes, ks->query_bytes, ks->insert_dense,
                                       ks->query_dense};
         for (int i = 0; i < 4 && rc == SBF_OK; ++i) {
-            const int dyn = (i & 1) ? kQuerySlotBytes : 0;  // query kernels: shard slots
+            // Query kernels: shard slots; insert kernels: flush staging ring.
+            const int dyn = (i & 1) ? kQuerySlotBytes : kInsertSlotBytes;
             if (dyn) {
                 e = cudaFuncSetAttribute(reinterpret_cast<const void*>(fns[i]),
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);

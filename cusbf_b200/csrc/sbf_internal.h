@@ -15,7 +15,10 @@ constexpr int kStripWords = kStrip / 16 + 2;           // code words one strip r
 constexpr int kCodeWords = (kThreads - 1) * (kStrip / 16) + kStripWords;  // per tile
 constexpr int kStageBytes = kCodeWords * 16 + 64;      // staged input bytes per buffer
 constexpr int kSlots = 10;                             // query shard slots per thread
-constexpr int kQuerySlotBytes = kSlots * kThreads * 32;  // dynamic smem of query kernels
+constexpr int kOverflow = 6;                           // deferred shard loads per thread
+constexpr int kQuerySlotBytes = kSlots * kThreads * 32 + kOverflow * kThreads * 4;
+constexpr int kFlushSlots = 8;                         // insert bulk-reduce staging slots
+constexpr int kInsertSlotBytes = kFlushSlots * kThreads * 32;  // dynamic smem of inserts
 
 // One launch of a tile kernel.  Grid position g of tile n is
 // g = n * kTileKmers + (0 .. kTileKmers-1); it holds window (k-mer)

@@ -112,8 +112,7 @@ __device__ __forceinline__ void issue_stage(const TileParams& p, uint64_t tile, 
 // Plain loads of the readable bytes of the stage window that the bulk copy
 // did not cover (at most 15 at each end of the input).
 template <bool kDense>
-__device__ __forceinline__ void fill_ragged(const TileParams& p, uint64_t tile, uint8_t* buf) {
-    const TileGeom g = tile_geom<kDense>(p, tile);
+__device__ __forceinline__ void fill_ragged(const TileParams& p, const TileGeom& g, uint8_t* buf) {
     const int64_t base = static_cast<int64_t>(g.r0);
     const int64_t w0 = static_cast<int64_t>(g.a - g.r0);  // window start rel. to input
     const int64_t w1 = w0 + g.span;
@@ -194,6 +193,11 @@ __device__ __forceinline__ uint64_t smer_at(const uint32_t* c, int r) {
     }
 }
 
+// Low word of min(a, b): the shard only needs the minimum's low 32 bits.
+__device__ __forceinline__ uint32_t min64_lo(uint64_t a, uint64_t b) {
+    return static_cast<uint32_t>(a < b ? a : b);
+}
+
 // Calls fn(j, shard) for the strip's windows j = 0..kStrip-1 in order.
 // For 16 m-mers per window the minimum is a Gil-Werman sliding minimum over
 // blocks of 16 positions: window j of block b is min(suffix_b[j],
@@ -213,7 +217,7 @@ __device__ __forceinline__ void for_each_shard(const uint32_t* c, uint32_t shard
 #pragma unroll
             for (int j = 1; j < 16; ++j) {
                 pre = min64(pre, mh_at<C>(c, 16 * b + 15 + j));
-                fn(16 * b + j, static_cast<uint32_t>(min64(suf[j], pre)) & shard_mask);
+                fn(16 * b + j, min64_lo(suf[j], pre) & shard_mask);
             }
         }
     } else {
@@ -261,12 +265,37 @@ __device__ __forceinline__ void smer_masks(const uint32_t* c, int r, uint64_t m[
     for (int j = 0; j < C::H; ++j) m[j & 3] |= uint64_t{1} << bit_address<C::H>(h, j);
 }
 
-__device__ __forceinline__ void flush_run(uint64_t* words, uint32_t shard, const uint64_t a[4]) {
-    uint64_t* dst = words + static_cast<uint64_t>(shard) * 4;
-    red_or(dst + 0, a[0]);
-    red_or(dst + 1, a[1]);
-    red_or(dst + 2, a[2]);
-    red_or(dst + 3, a[3]);
+// A run's four word masks are merged into its shard with one 32-byte TMA
+// bulk reduction (cp.reduce.async.bulk .or.b64) from a shared-memory staging
+// slot: one L2 sector operation instead of four 8-byte atomics.  Each thread
+// cycles through kFlushSlots slots; before reusing a slot it waits until the
+// bulk operation issued kFlushSlots flushes earlier has read it.
+struct FlushRing {
+    uint64_t* slot0;  // this thread's slot 0; slot k at slot0 + k * kThreads * 4
+    uint32_t count;
+};
+
+__device__ __forceinline__ void flush_run(uint64_t* words, uint32_t shard, const uint64_t a[4],
+                                          FlushRing& ring) {
+    static_assert(kFlushSlots == 8, "wait_group.read immediate below assumes 8 slots");
+    uint64_t* slot = ring.slot0 + (ring.count & (kFlushSlots - 1)) * (kThreads * 4);
+    asm volatile("cp.async.bulk.wait_group.read 7;" ::: "memory");
+    *reinterpret_cast<ulonglong2*>(slot) = make_ulonglong2(a[0], a[1]);
+    *reinterpret_cast<ulonglong2*>(slot + 2) = make_ulonglong2(a[2], a[3]);
+    fence_proxy_async_smem();
+    asm volatile(
+        "cp.reduce.async.bulk.global.shared::cta.bulk_group.or.b64 [%0], [%1], 32;" ::"l"(
+            words + static_cast<uint64_t>(shard) * 4),
+        "r"(smem_addr(slot))
+        : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    ++ring.count;
+}
+
+__device__ __forceinline__ void flush_ring_drain() {
+    // Every bulk reduction issued by this thread has completed (its global
+    // writes performed and its shared-memory slot read).
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
 // Insert: the mask of window j is T_j = OR of the one-hot masks of its F
@@ -275,7 +304,8 @@ __device__ __forceinline__ void flush_run(uint64_t* words, uint32_t shard, const
 // the next window leaves the run.
 template <class C>
 __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
-                                             uint32_t shard_mask, uint64_t* words) {
+                                             uint32_t shard_mask, uint64_t* words,
+                                             FlushRing& ring) {
     constexpr int F = C::F;
     uint64_t acc[4] = {0, 0, 0, 0};
     uint32_t prev_shard = 0;
@@ -297,7 +327,7 @@ __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
             smer_masks<C>(c, j + 3, m3);
             const bool valid = (vmask >> j) & 1u;
             const bool cont = valid && prev_valid && shard == prev_shard;
-            if (prev_valid && !cont) flush_run(words, prev_shard, acc);
+            if (prev_valid && !cont) flush_run(words, prev_shard, acc, ring);
             const uint64_t keep = cont ? ~uint64_t{0} : uint64_t{0};
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
@@ -311,33 +341,34 @@ __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
             prev_valid = valid;
         });
     } else {
-        uint64_t ring[F][4];
+        uint64_t mring[F][4];
 #pragma unroll
-        for (int o = 0; o < F - 1; ++o) smer_masks<C>(c, o, ring[o]);
+        for (int o = 0; o < F - 1; ++o) smer_masks<C>(c, o, mring[o]);
         for_each_shard<C>(c, shard_mask, [&](int j, uint32_t shard) {
-            smer_masks<C>(c, j + F - 1, ring[(j + F - 1) % F]);
+            smer_masks<C>(c, j + F - 1, mring[(j + F - 1) % F]);
             const bool valid = (vmask >> j) & 1u;
             const bool cont = valid && prev_valid && shard == prev_shard;
-            if (prev_valid && !cont) flush_run(words, prev_shard, acc);
+            if (prev_valid && !cont) flush_run(words, prev_shard, acc, ring);
             const uint64_t keep = cont ? ~uint64_t{0} : uint64_t{0};
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
-                uint64_t t = ring[j % F][w];
+                uint64_t t = mring[j % F][w];
 #pragma unroll
-                for (int o = 1; o < F; ++o) t |= ring[(j + o) % F][w];
+                for (int o = 1; o < F; ++o) t |= mring[(j + o) % F][w];
                 acc[w] = (acc[w] & keep) | t;
             }
             prev_shard = shard;
             prev_valid = valid;
         });
     }
-    if (prev_valid) flush_run(words, prev_shard, acc);
+    if (prev_valid) flush_run(words, prev_shard, acc, ring);
 }
 
 // Query shard slots: the run heads of a strip fetch their 32-byte shards into
 // per-thread shared-memory slots with cp.async, all at once, so a thread has
 // every shard load of its strip in flight while it hashes the strip's s-mers.
-static_assert(kSlots * kThreads * 32 == kQuerySlotBytes, "slot geometry");
+static_assert(kSlots * kThreads * 32 + kOverflow * kThreads * 4 == kQuerySlotBytes,
+              "slot geometry");
 
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(smem_dst)),
@@ -437,35 +468,64 @@ __device__ __noinline__ uint32_t query_strip_direct(const uint32_t* c, uint32_t 
 template <class C>
 __device__ __forceinline__ void query_strip(const uint32_t* c, uint32_t vmask, uint32_t shard_mask,
                                             const uint64_t* words, uint64_t* slot0,
-                                            uint8_t* out, int64_t first_kmer, uint64_t n_kmers) {
-    // Slot n of this thread lives at slot0 + n * kThreads * 4 ([slot][thread]
-    // layout: neighbouring threads touch neighbouring 32-byte slots).
+                                            uint32_t* ovf0, uint8_t* out, int64_t first_kmer,
+                                            uint64_t n_kmers) {
+    // Slot n of this thread lives at slot0 + n * kThreads * 4 and overflow
+    // entry e at ovf0 + e * kThreads ([entry][thread] layouts: neighbouring
+    // threads touch neighbouring addresses).
     constexpr int kSlotStride = kThreads * 4;
     constexpr int F = C::F;
+    // Run heads: a valid window whose predecessor is invalid or selects
+    // another shard.  The first kSlots heads copy their shard into slots; the
+    // next kOverflow only record their shard id (loaded when reached).  The
+    // copy for window 0 is decided after the loop: when the left neighbour's
+    // last run continues into this strip (same shard, both ends valid), its
+    // staged slot is read instead of loading the sector again.
     uint32_t heads = 0;
     int n = 0;
+    uint32_t first_sh = 0, last_sh = 0;
     {
-        bool have = false;
-        uint32_t cur = 0;
+        uint32_t prev = 0;
         for_each_shard<C>(c, shard_mask, [&](int j, uint32_t sh) {
             const bool valid = (vmask >> j) & 1u;
-            if (valid && (!have || sh != cur)) {
+            const bool prev_valid = j > 0 && ((vmask >> (j - 1)) & 1u);
+            if (j == 0) first_sh = sh;
+            if (j == kStrip - 1) last_sh = sh;
+            if (valid && (!prev_valid || sh != prev)) {
                 heads |= 1u << j;
-                if (n < kSlots) {
-                    const uint64_t* src = words + static_cast<uint64_t>(sh) * 4;
-                    uint64_t* dst = slot0 + n * kSlotStride;
-                    cp_async16(dst, src);
-                    cp_async16(dst + 2, src + 2);
+                if (j > 0) {
+                    if (n < kSlots) {
+                        const uint64_t* src = words + static_cast<uint64_t>(sh) * 4;
+                        uint64_t* dst = slot0 + n * kSlotStride;
+                        cp_async16(dst, src);
+                        cp_async16(dst + 2, src + 2);
+                    } else if (n < kSlots + kOverflow) {
+                        ovf0[(n - kSlots) * kThreads] = sh;
+                    }
                 }
                 ++n;
-                cur = sh;
-                have = true;
             }
+            prev = sh;
         });
     }
+    const int lane = threadIdx.x & 31;
+    const bool last_open = (vmask >> (kStrip - 1)) & 1u;
+    // Lend the last run's slot only when its head is not window 0: window 0's
+    // slot may itself be borrowed (never loaded), so lending it would chain.
+    const bool last_is_w0 = n == 1 && (vmask & 1u);
+    const int my_last_slot = last_open && n >= 1 && n <= kSlots && !last_is_w0 ? n - 1 : -1;
+    const uint32_t left_sh = __shfl_up_sync(0xFFFFFFFFu, last_sh, 1);
+    const int left_slot = __shfl_up_sync(0xFFFFFFFFu, my_last_slot, 1);
+    const bool borrow = lane > 0 && (vmask & 1u) && left_slot >= 0 && left_sh == first_sh;
+    if ((vmask & 1u) && !borrow) {
+        const uint64_t* src = words + static_cast<uint64_t>(first_sh) * 4;
+        cp_async16(slot0, src);
+        cp_async16(slot0 + 2, src + 2);
+    }
     cp_async_commit();
-    if (n > kSlots) {
+    if (n > kSlots + kOverflow) {
         cp_async_wait_all();
+        __syncwarp();
         store_strip_bytes(query_strip_direct<C>(c, vmask, shard_mask, words), out, first_kmer,
                           n_kmers);
         return;
@@ -482,6 +542,7 @@ __device__ __forceinline__ void query_strip(const uint32_t* c, uint32_t vmask, u
             hs[r] = smer_hash(smer_at<C>(c, r));
     }
     cp_async_wait_all();
+    __syncwarp();  // neighbours' slots are complete before any is borrowed
     uint64_t w[4] = {0, 0, 0, 0};
     uint32_t result = 0;
     n = 0;
@@ -503,13 +564,20 @@ __device__ __forceinline__ void query_strip(const uint32_t* c, uint32_t vmask, u
                 ring[(j + F - 1) % F][q] = __byte_perm(bytes[j + F - 1], 0u, 0x4440u + q);
         }
         if ((heads >> j) & 1u) {
-            const uint64_t* sn = slot0 + n * kSlotStride;
-            const uint4 lo = *reinterpret_cast<const uint4*>(sn);
-            const uint4 hi = *reinterpret_cast<const uint4*>(sn + 2);
-            w[0] = (static_cast<uint64_t>(lo.y) << 32) | lo.x;
-            w[1] = (static_cast<uint64_t>(lo.w) << 32) | lo.z;
-            w[2] = (static_cast<uint64_t>(hi.y) << 32) | hi.x;
-            w[3] = (static_cast<uint64_t>(hi.w) << 32) | hi.z;
+            if (n < kSlots) {
+                // Slot 0 may be the left neighbour's last slot (its thread's
+                // slots sit 4 words below this thread's).
+                const uint64_t* sn = (n == 0 && borrow) ? slot0 + left_slot * kSlotStride - 4
+                                                        : slot0 + n * kSlotStride;
+                const uint4 lo = *reinterpret_cast<const uint4*>(sn);
+                const uint4 hi = *reinterpret_cast<const uint4*>(sn + 2);
+                w[0] = (static_cast<uint64_t>(lo.y) << 32) | lo.x;
+                w[1] = (static_cast<uint64_t>(lo.w) << 32) | lo.z;
+                w[2] = (static_cast<uint64_t>(hi.y) << 32) | hi.x;
+                w[3] = (static_cast<uint64_t>(hi.w) << 32) | hi.z;
+            } else {
+                load_shard_now(words + static_cast<uint64_t>(ovf0[(n - kSlots) * kThreads]) * 4, w);
+            }
             ++n;
         }
         uint32_t present = (vmask >> j) & 1u;
@@ -553,9 +621,12 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
         if (tile < p.n_tiles) issue_stage<kDense>(p, tile, stage[0], &bars[0]);
         if (tile + stride < p.n_tiles) issue_stage<kDense>(p, tile + stride, stage[1], &bars[1]);
     }
-    // Per-thread shard slots of the query kernel, [slot][thread] layout, in
-    // dynamic shared memory (kQuerySlotBytes per CTA).
+    // Dynamic shared memory, [slot][thread] layout: the query kernel's shard
+    // slots (kQuerySlotBytes per CTA) or the insert kernel's flush staging
+    // ring (kInsertSlotBytes per CTA).
     extern __shared__ __align__(16) uint64_t slots[];
+    FlushRing ring{slots + 4 * tid, 0u};
+    (void)ring;
     uint32_t it = 0;
     for (; tile < p.n_tiles; tile += stride, ++it) {
         const int b = it & 1;
@@ -566,11 +637,12 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
             // Give the other buffer's copy (if any) a bounded chance to land
             // before the CTA's shared memory is released.
             if (tile + stride < p.n_tiles) (void)mbar_wait_bounded(&bars[b ^ 1], parity);
+            if constexpr (!kQuery) flush_ring_drain();
             return;
         }
-        fill_ragged<kDense>(p, tile, stage[b]);
-        __syncthreads();
         const TileGeom g = tile_geom<kDense>(p, tile);
+        fill_ragged<kDense>(p, g, stage[b]);
+        __syncthreads();
         for (int q = tid; q < kCodeWords; q += kThreads) {
             uint32_t cw, iv;
             encode_word<kDense>(g, stage[b], q, cw, iv);
@@ -590,12 +662,14 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
         const int64_t first_kmer = g.s0 + static_cast<int64_t>(tid) * kStrip;
         const uint32_t vmask = strip_valid<C>(iv, first_kmer, p.n_kmers);
         if constexpr (kQuery) {
-            query_strip<C>(c, vmask, p.shard_mask, p.words, slots + 4 * tid, p.out, first_kmer,
-                           p.n_kmers);
+            query_strip<C>(c, vmask, p.shard_mask, p.words, slots + 4 * tid,
+                           reinterpret_cast<uint32_t*>(slots + kSlots * kThreads * 4) + tid, p.out,
+                           first_kmer, p.n_kmers);
         } else {
-            if (vmask) insert_strip<C>(c, vmask, p.shard_mask, p.words);
+            if (vmask) insert_strip<C>(c, vmask, p.shard_mask, p.words, ring);
         }
     }
+    if constexpr (!kQuery) flush_ring_drain();
 }
 
 // ---------------------------------------------------------------------------
