@@ -37,7 +37,9 @@ ERR_IO = 2
 ERR_FASTX_PARSE = 3
 ERR_INVALID_ARGUMENT = 4
 ERR_RESOURCE = 5
-_CATEGORY = {1: "cuda", 2: "io", 3: "fastx_parse", 4: "invalid_argument", 5: "resource"}
+ERR_ABORTED = 6
+_CATEGORY = {1: "cuda", 2: "io", 3: "fastx_parse", 4: "invalid_argument", 5: "resource",
+             6: "aborted"}
 
 ALPHABET_DNA = 0
 ALPHABET_DNA_TRIPLET = 1
@@ -45,11 +47,14 @@ ALPHABET_PROTEIN = 2
 
 
 class SbfError(RuntimeError):
-    """A failed library call; ``category`` is the reference ErrorCategory name."""
+    """A failed library call; ``category`` is the reference ErrorCategory name
+    and ``location`` the (file, line, column) of a FASTX parse error."""
 
-    def __init__(self, status: int, message: str):
+    def __init__(self, status: int, message: str, location=None):
         self.status = status
         self.category = _CATEGORY.get(status, "unknown")
+        self.message = message
+        self.location = location
         super().__init__(f"[{self.category}] {message}")
 
 
@@ -98,6 +103,48 @@ class QueryReport(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class NormalizedRecord(C.Structure):
+    """NormalizedRecord (include/cusbf/normalized_record_batch.hpp:20-29)."""
+
+    _fields_ = [("record_index", C.c_uint64), ("input_offset", C.c_uint64),
+                ("size", C.c_uint64), ("valid_kmers", C.c_uint64)]
+
+
+class QueryLayoutRecord(C.Structure):
+    """QueryLayoutRecord (include/cusbf/detail/query_layout.cuh:13-20)."""
+
+    _fields_ = [("record_index", C.c_uint64), ("input_offset", C.c_uint64),
+                ("size", C.c_uint64), ("valid_kmers", C.c_uint64),
+                ("hit_offset", C.c_uint64), ("hit_count", C.c_uint64)]
+
+
+class RecordView(C.Structure):
+    """RecordQueryView (include/cusbf/Fastx.hpp:135-148), valid during a callback."""
+
+    _fields_ = [("record_index", C.c_uint64), ("sequence", C.c_void_p),
+                ("sequence_bytes", C.c_uint64), ("queried_bases", C.c_uint64),
+                ("queried_kmers", C.c_uint64), ("positive_kmers", C.c_uint64),
+                ("hits", C.c_void_p), ("n_hits", C.c_uint64)]
+
+
+RECORD_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(RecordView))
+
+
+class FastxRecordView(C.Structure):
+    """FastxRecordView (include/cusbf/Fastx.hpp:173-188), valid during a callback."""
+
+    _fields_ = [("record_index", C.c_uint64), ("header", C.c_void_p),
+                ("header_bytes", C.c_uint64), ("sequence", C.c_void_p),
+                ("sequence_bytes", C.c_uint64), ("queried_bases", C.c_uint64),
+                ("queried_kmers", C.c_uint64), ("positive_kmers", C.c_uint64),
+                ("hits", C.c_void_p), ("n_hits", C.c_uint64)]
+
+
+FASTX_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(FastxRecordView))
+SCAN_CB = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p,
+                      C.c_uint64)
+READ_FN = C.CFUNCTYPE(C.c_int64, C.c_void_p, C.c_void_p, C.c_uint64)
+
 _vp = C.c_void_p
 _u64 = C.c_uint64
 _u32 = C.c_uint32
@@ -112,6 +159,8 @@ def _sig(name, res, *args):
 
 _lib_last_error = _sig("sbf_last_error_message", C.c_char_p)
 _sig("sbf_last_cuda_error", C.c_int)
+_sig("sbf_last_error_location", C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_uint32),
+     C.POINTER(C.c_uint32))
 _sig("sbf_version", C.c_char_p)
 _sig("sbf_filter_create", C.c_int, _u32, _u32, _u32, _u32, C.c_int, _u64, C.POINTER(_vp))
 _sig("sbf_filter_destroy", None, _vp)
@@ -134,6 +183,25 @@ _sig("sbf_insert_dense_packed", C.c_int, _vp, _vp, _u64, _u64, _vp, C.POINTER(_u
 _sig("sbf_contains_dense_packed_async", C.c_int, _vp, _vp, _u64, _u64, _vp, _u64, _vp)
 _sig("sbf_contains_dense_packed_to_device", C.c_int, _vp, _vp, _u64, _u64, _vp, _u64, _vp)
 _sig("sbf_contains_dense_packed", C.c_int, _vp, _vp, _u64, _u64, _vp, _u64, _vp)
+_sig("sbf_validate_record_batch", C.c_int, _u64, _vp, _u64)
+_sig("sbf_normalized_batch_bytes", _u64, _vp, _u64)
+_sig("sbf_normalize_record_batch", C.c_int, _u32, _vp, _u64, _vp, _u64, _vp, _u64,
+     C.POINTER(_u64), _vp)
+_sig("sbf_query_layout", C.c_int, _u32, _vp, _u64, _vp, C.POINTER(_u64))
+_sig("sbf_insert_record_batch", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, C.POINTER(InsertReport))
+_sig("sbf_insert_record_batch_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, C.POINTER(_u64))
+_sig("sbf_query_record_batch", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, C.POINTER(QueryReport),
+     RECORD_CB, _vp)
+_sig("sbf_contains_record_batch_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _vp)
+_sig("sbf_fastx_scan", C.c_int, READ_FN, _vp, C.c_char_p, SCAN_CB, _vp, C.POINTER(_u64))
+_sig("sbf_fastx_scan_file", C.c_int, C.c_char_p, SCAN_CB, _vp, C.POINTER(_u64))
+_sig("sbf_insert_fastx", C.c_int, _vp, READ_FN, _vp, C.c_char_p, C.c_double, _vp,
+     C.POINTER(InsertReport))
+_sig("sbf_insert_fastx_file", C.c_int, _vp, C.c_char_p, C.c_double, _vp, C.POINTER(InsertReport))
+_sig("sbf_query_fastx", C.c_int, _vp, READ_FN, _vp, C.c_char_p, C.c_double, _vp,
+     C.POINTER(QueryReport), FASTX_CB, _vp)
+_sig("sbf_query_fastx_file", C.c_int, _vp, C.c_char_p, C.c_double, _vp, C.POINTER(QueryReport),
+     FASTX_CB, _vp)
 
 
 def lib() -> C.CDLL:
@@ -147,7 +215,12 @@ def version() -> str:
 
 def _check(status: int) -> None:
     if status != OK:
-        raise SbfError(status, _lib.sbf_last_error_message().decode(errors="replace"))
+        loc = None
+        if status == ERR_FASTX_PARSE:
+            f, ln, col = C.c_char_p(), _u32(), _u32()
+            _lib.sbf_last_error_location(C.byref(f), C.byref(ln), C.byref(col))
+            loc = ((f.value or b"").decode(errors="replace"), ln.value, col.value)
+        raise SbfError(status, _lib.sbf_last_error_message().decode(errors="replace"), loc)
 
 
 def _stream(stream) -> int:
@@ -183,6 +256,54 @@ def _host_bytes(seq) -> np.ndarray:
 
 def _np_ptr(a: np.ndarray) -> int:
     return a.ctypes.data
+
+
+def _ranges(ranges) -> np.ndarray:
+    """(n, 2) uint64 array of (sequence_offset, sequence_bytes) pairs."""
+    r = np.ascontiguousarray(np.asarray(ranges, dtype=np.uint64).reshape(-1, 2))
+    return r
+
+
+def records_from_ranges(seq, ranges):
+    """RecordBatchView-style helper: the records a (sequence, ranges) pair names."""
+    b = _host_bytes(seq)
+    return [b[int(o):int(o) + int(n)] for o, n in _ranges(ranges)]
+
+
+def validate_record_batch(nbytes: int, ranges) -> None:
+    r = _ranges(ranges)
+    _check(_lib.sbf_validate_record_batch(nbytes, _np_ptr(r), r.shape[0]))
+
+
+def normalized_batch_bytes(ranges) -> int:
+    r = _ranges(ranges)
+    return _lib.sbf_normalized_batch_bytes(_np_ptr(r), r.shape[0])
+
+
+def normalize_record_batch(k: int, seq, ranges):
+    """normalize_record_batch (normalized_record_batch.hpp:289-316): the
+    separator-joined sequence and one NormalizedRecord per record."""
+    b = _host_bytes(seq)
+    r = _ranges(ranges)
+    n = r.shape[0]
+    total = _u64()
+    recs = (NormalizedRecord * max(n, 1))()
+    _check(_lib.sbf_normalize_record_batch(k, _np_ptr(b), b.size, _np_ptr(r), n, None, 0,
+                                           C.byref(total), None))
+    out = np.zeros(max(total.value, 1), dtype=np.uint8)
+    _check(_lib.sbf_normalize_record_batch(k, _np_ptr(b), b.size, _np_ptr(r), n, _np_ptr(out),
+                                           out.size, C.byref(total), recs))
+    return out[:total.value], list(recs)[:n]
+
+
+def query_layout(k: int, records):
+    """QueryLayout::build (query_layout.cuh:42-72): (layout records, total hits)."""
+    n = len(records)
+    arr = (NormalizedRecord * max(n, 1))(*records)
+    out = (QueryLayoutRecord * max(n, 1))()
+    total = _u64()
+    _check(_lib.sbf_query_layout(k, arr, n, out, C.byref(total)))
+    return list(out)[:n], total.value
 
 
 class Filter:
@@ -333,6 +454,220 @@ class Filter:
         return out[:n]
 
 
+def _record_methods():
+    def insert_record_batch(self, seq, ranges, stream=None) -> InsertReport:
+        """insert_record_batch (filter.cuh:338-364): host records."""
+        b = _host_bytes(seq)
+        r = _ranges(ranges)
+        rep = InsertReport()
+        _check(_lib.sbf_insert_record_batch(self._h, _np_ptr(b), b.size, _np_ptr(r), r.shape[0],
+                                            _stream(stream), C.byref(rep)))
+        return rep
+
+    def insert_record_batch_async(self, d_seq, ranges, stream=None) -> int:
+        """insert_record_batch_async (filter.cuh:385-400): separators in place."""
+        p, n = _dev_ptr(d_seq)
+        r = _ranges(ranges)
+        out = _u64()
+        _check(_lib.sbf_insert_record_batch_async(self._h, p, n, _np_ptr(r), r.shape[0],
+                                                  _stream(stream), C.byref(out)))
+        return out.value
+
+    def query_record_batch(self, seq, ranges, consume=None, stream=None) -> QueryReport:
+        """query_record_batch (filter.cuh:549-582).  `consume(view)` receives a
+        dict per record: record_index, sequence (bytes), queried_bases,
+        queried_kmers, positive_kmers, hits (numpy copy)."""
+        b = _host_bytes(seq)
+        r = _ranges(ranges)
+        rep = QueryReport()
+        cb = RECORD_CB()
+        box = []
+        if consume is not None:
+            def _cb(_user, view_p):
+                v = view_p.contents
+                hits = (np.ctypeslib.as_array(C.cast(v.hits, C.POINTER(C.c_uint8)), (v.n_hits,)).copy()
+                        if v.n_hits else np.zeros(0, np.uint8))
+                seqb = C.string_at(v.sequence, v.sequence_bytes) if v.sequence_bytes else b""
+                try:
+                    consume({"record_index": v.record_index, "sequence": seqb,
+                             "queried_bases": v.queried_bases, "queried_kmers": v.queried_kmers,
+                             "positive_kmers": v.positive_kmers, "hits": hits})
+                    return 0
+                except BaseException as e:  # noqa: BLE001 - re-raised after the call
+                    box.append(e)
+                    return 1
+            cb = RECORD_CB(_cb)
+        st = _lib.sbf_query_record_batch(self._h, _np_ptr(b), b.size, _np_ptr(r), r.shape[0],
+                                         _stream(stream), C.byref(rep), cb, None)
+        if box:
+            raise box[0]
+        _check(st)
+        return rep
+
+    def contains_record_batch_async(self, d_seq, ranges, d_out, stream=None) -> None:
+        """contains_record_batch_async (filter.cuh:603-622)."""
+        p, n = _dev_ptr(d_seq)
+        o, on = _dev_ptr(d_out)
+        r = _ranges(ranges)
+        _check(_lib.sbf_contains_record_batch_async(self._h, p, n, _np_ptr(r), r.shape[0], o, on,
+                                                    _stream(stream)))
+
+    for f in (insert_record_batch, insert_record_batch_async, query_record_batch,
+              contains_record_batch_async):
+        setattr(Filter, f.__name__, f)
+
+
+_record_methods()
+
+
+class _Reader:
+    """Adapts bytes/str or a binary file-like object to the C read callback."""
+
+    def __init__(self, source):
+        import io
+
+        if isinstance(source, str):
+            source = source.encode()
+        if isinstance(source, (bytes, bytearray, memoryview)):
+            source = io.BytesIO(bytes(source))
+        self.f = source
+        self.error = None
+
+        def _read(_user, buf, cap):
+            try:
+                data = self.f.read(cap)
+            except Exception as e:  # surfaced as an io error
+                self.error = e
+                return -1
+            if not data:
+                return 0
+            C.memmove(buf, data, len(data))
+            return len(data)
+
+        self.fn = READ_FN(_read)
+
+
+def _fastx_view(v):
+    hits = (np.ctypeslib.as_array(C.cast(v.hits, C.POINTER(C.c_uint8)), (v.n_hits,)).copy()
+            if v.n_hits else np.zeros(0, np.uint8))
+    return {"record_index": v.record_index,
+            "header": C.string_at(v.header, v.header_bytes).decode(errors="replace")
+            if v.header_bytes else "",
+            "sequence": C.string_at(v.sequence, v.sequence_bytes) if v.sequence_bytes else b"",
+            "queried_bases": v.queried_bases, "queried_kmers": v.queried_kmers,
+            "positive_kmers": v.positive_kmers, "hits": hits}
+
+
+def _consumer(consume, box):
+    if consume is None:
+        return FASTX_CB()
+
+    def _cb(_user, vp):
+        try:
+            consume(_fastx_view(vp.contents))
+            return 0
+        except BaseException as e:  # noqa: BLE001 - re-raised after the call
+            box.append(e)
+            return 1
+    return FASTX_CB(_cb)
+
+
+def fastx_scan(source, source_name: str = "<stream>"):
+    """FastxReader over `source` (bytes/str content, a binary file object, or
+    a path via ``fastx_scan_file``): list of (header, sequence) pairs."""
+    out = []
+
+    def _cb(_u, _i, h, hn, s, sn):
+        out.append((C.string_at(h, hn).decode(errors="replace") if hn else "",
+                    C.string_at(s, sn) if sn else b""))
+        return 0
+    r = _Reader(source)
+    cb = SCAN_CB(_cb)
+    _check(_lib.sbf_fastx_scan(r.fn, None, source_name.encode(), cb, None, None))
+    return out
+
+
+def fastx_scan_file(path):
+    out = []
+
+    def _cb(_u, _i, h, hn, s, sn):
+        out.append((C.string_at(h, hn).decode(errors="replace") if hn else "",
+                    C.string_at(s, sn) if sn else b""))
+        return 0
+    cb = SCAN_CB(_cb)
+    _check(_lib.sbf_fastx_scan_file(os.fsencode(path), cb, None, None))
+    return out
+
+
+def _fastx_methods():
+    def insert_fastx(self, source, fill_fraction=0.7, stream=None, source_name="<stream>"):
+        """insert_fastx (filter.cuh:416-421) over bytes/str or a binary file object."""
+        r = _Reader(source)
+        rep = InsertReport()
+        _check(_lib.sbf_insert_fastx(self._h, r.fn, None, source_name.encode(), fill_fraction,
+                                     _stream(stream), C.byref(rep)))
+        return rep
+
+    def insert_fastx_file(self, path, fill_fraction=0.7, stream=None):
+        """insert_fastx_file (filter.cuh:437-452): plain or gzip file."""
+        rep = InsertReport()
+        _check(_lib.sbf_insert_fastx_file(self._h, os.fsencode(path), fill_fraction,
+                                          _stream(stream), C.byref(rep)))
+        return rep
+
+    def query_fastx(self, source, fill_fraction=0.7, stream=None, source_name="<stream>",
+                    consume=None):
+        """query_fastx (filter.cuh:632-638); with `consume`, query_fastx_records."""
+        r = _Reader(source)
+        rep = QueryReport()
+        box = []
+        cb = _consumer(consume, box)
+        st = _lib.sbf_query_fastx(self._h, r.fn, None, source_name.encode(), fill_fraction,
+                                  _stream(stream), C.byref(rep), cb, None)
+        if box:
+            raise box[0]
+        _check(st)
+        return rep
+
+    def query_fastx_file(self, path, fill_fraction=0.7, stream=None, consume=None):
+        """query_fastx_file (filter.cuh:654-668); with `consume`,
+        query_fastx_file_records (filter.cuh:713-735)."""
+        rep = QueryReport()
+        box = []
+        cb = _consumer(consume, box)
+        st = _lib.sbf_query_fastx_file(self._h, os.fsencode(path), fill_fraction, _stream(stream),
+                                       C.byref(rep), cb, None)
+        if box:
+            raise box[0]
+        _check(st)
+        return rep
+
+    def query_fastx_records(self, source, consume, fill_fraction=0.7, stream=None):
+        return self.query_fastx(source, fill_fraction, stream, consume=consume)
+
+    def query_fastx_file_records(self, path, consume, fill_fraction=0.7, stream=None):
+        return self.query_fastx_file(path, fill_fraction, stream, consume=consume)
+
+    def query_fastx_detailed(self, source, fill_fraction=0.7, stream=None):
+        """query_fastx_detailed (filter.cuh:750-760): (summary, records)."""
+        recs = []
+        summary = self.query_fastx(source, fill_fraction, stream, consume=recs.append)
+        return summary, recs
+
+    def query_fastx_file_detailed(self, path, fill_fraction=0.7, stream=None):
+        """query_fastx_file_detailed (filter.cuh:771-786)."""
+        recs = []
+        summary = self.query_fastx_file(path, fill_fraction, stream, consume=recs.append)
+        return summary, recs
+
+    for f in (insert_fastx, insert_fastx_file, query_fastx, query_fastx_file, query_fastx_records,
+              query_fastx_file_records, query_fastx_detailed, query_fastx_file_detailed):
+        setattr(Filter, f.__name__, f)
+
+
+_fastx_methods()
+
+
 def pack_dense_sequence(seq) -> np.ndarray:
     """Host dense packing (include/cusbf/dense_packed.hpp:36-50), DNA."""
     b = _host_bytes(seq)
@@ -351,5 +686,8 @@ def pack_dense_sequence_device(d_seq, num_symbols: int, d_words, stream=None) ->
 
 __all__ = [
     "Config", "Filter", "RecordRange", "InsertReport", "QueryReport", "SbfError",
+    "NormalizedRecord", "QueryLayoutRecord", "normalize_record_batch", "query_layout",
+    "normalized_batch_bytes", "validate_record_batch", "records_from_ranges",
+    "fastx_scan", "fastx_scan_file",
     "pack_dense_sequence", "pack_dense_sequence_device", "lib", "version", "LIBRARY_PATH",
 ]

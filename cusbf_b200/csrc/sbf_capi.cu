@@ -28,6 +28,14 @@ using namespace sbf;
 namespace sbf {
 thread_local std::string g_last_error;
 thread_local int g_last_cuda = 0;
+thread_local std::string g_err_file;
+thread_local uint32_t g_err_line = 0, g_err_col = 0;
+
+void set_error_location(const char* file, uint32_t line, uint32_t col) {
+    g_err_file = file ? file : "";
+    g_err_line = line;
+    g_err_col = col;
+}
 
 int set_error(int status, const char* fmt, ...) {
     char buf[512];
@@ -58,6 +66,12 @@ int cuda_fail(cudaError_t e, const char* what) {
     } while (0)
 
 extern "C" const char* sbf_last_error_message(void) { return g_last_error.c_str(); }
+extern "C" int sbf_last_error_location(const char** file, uint32_t* line, uint32_t* column) {
+    if (file) *file = g_err_file.c_str();
+    if (line) *line = g_err_line;
+    if (column) *column = g_err_col;
+    return SBF_OK;
+}
 extern "C" int sbf_last_cuda_error(void) { return g_last_cuda; }
 extern "C" const char* sbf_version(void) { return "sbf-b200 0.1.0 (sm_100a)"; }
 
@@ -356,6 +370,11 @@ extern "C" void sbf_filter_destroy(sbf_filter_t* f) {
     if (!f) return;
     f->stage_in.release();
     f->stage_out.release();
+    f->rb_dense.release();
+    f->rb_norm.release();
+    f->rb_meta.release();
+    f->rb_hits.release();
+    f->rb_stats.release();
     if (f->d_words) cudaFree(f->d_words);
     if (f->d_err) cudaFree(f->d_err);
     for (int i = 0; i < 2; ++i) {

@@ -1,0 +1,414 @@
+// sbf_fastx.cpp -- streaming FASTA/FASTQ parsing and the FASTX entry points.
+//
+// Parsing rules follow the reference reader (include/cusbf/Fastx.hpp:297-462
+// of tdortman/cuSBF):
+//   * blank lines before a header are skipped; a trailing '\r' is trimmed;
+//   * the first header fixes the format ('>' FASTA, '@' FASTQ); a header of
+//     the other kind is an error; anything else is an error;
+//   * FASTA sequence lines run until the next line starting with '>';
+//   * FASTQ sequence lines run until a line starting with '+', then quality
+//     lines are read until their total length reaches the sequence length
+//     (longer or shorter is an error; end of input before '+' is an error);
+//   * error locations are "source:line:column" (Fastx.hpp:268-289).
+// Chunking follows run_fastx_pipeline (detail/fastx_pipeline_core.cuh:33-122)
+// and fastx_chunk_reached_staging_budget (detail/fastx_chunk.cuh:97-127):
+// a chunk is flushed once its estimated device staging reaches
+// fill_fraction * (free memory - 64 MiB), or after every record when that
+// budget is 0.  Each flushed chunk is one record batch, so k-mers never span
+// records.  Unlike the reference reader, lines are scanned with memchr over a
+// large buffer instead of std::getline.
+#include <zlib.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/sbf_b200.h"
+#include "sbf_host.h"
+
+namespace sbf {
+
+namespace {
+
+class LineReader {
+   public:
+    LineReader(sbf_read_fn read, void* user) : read_(read), user_(user), buf_(1 << 22) {}
+
+    // Next line without its '\n' (and without a trailing '\r').  Returns 1
+    // with a line, 0 at end of input, -1 on a read error.
+    int next(std::string& line) {
+        line.clear();
+        for (;;) {
+            if (pos_ == end_) {
+                if (eof_) return line.empty() && !partial_ ? 0 : finish(line);
+                const int64_t n = read_(user_, buf_.data(), buf_.size());
+                if (n < 0) return -1;
+                if (n == 0) {
+                    eof_ = true;
+                    continue;
+                }
+                pos_ = 0;
+                end_ = static_cast<size_t>(n);
+            }
+            const char* p = buf_.data() + pos_;
+            const void* nl = std::memchr(p, '\n', end_ - pos_);
+            if (nl) {
+                const size_t len = static_cast<const char*>(nl) - p;
+                line.append(p, len);
+                pos_ += len + 1;
+                partial_ = false;
+                trim(line);
+                return 1;
+            }
+            line.append(p, end_ - pos_);
+            partial_ = true;
+            pos_ = end_;
+        }
+    }
+
+   private:
+    int finish(std::string& line) {
+        partial_ = false;
+        trim(line);
+        return 1;
+    }
+    static void trim(std::string& line) {
+        if (!line.empty() && line.back() == '\r') line.pop_back();
+    }
+
+    sbf_read_fn read_;
+    void* user_;
+    std::vector<char> buf_;
+    size_t pos_ = 0, end_ = 0;
+    bool eof_ = false;
+    bool partial_ = false;
+};
+
+enum class Format { unknown, fasta, fastq };
+
+class FastxParser {
+   public:
+    FastxParser(sbf_read_fn read, void* user, std::string source)
+        : lines_(read, user), source_(std::move(source)) {}
+
+    // 1 = record, 0 = end of input, or an sbf_status error (negated).
+    int next(std::string& header, std::string& seq) {
+        header.clear();
+        seq.clear();
+        std::string* hdr = nullptr;
+        if (!pending_.empty()) {
+            header.swap(pending_);
+            pending_.clear();
+            hdr = &header;
+        } else {
+            for (;;) {
+                const int r = lines_.next(line_);
+                if (r < 0) return -io_error();
+                if (r == 0) return 0;
+                ++line_no_;
+                if (!line_.empty()) break;
+            }
+            header.swap(line_);
+            hdr = &header;
+        }
+        const char tag = hdr->front();
+        if (format_ == Format::unknown) {
+            if (tag == '>')
+                format_ = Format::fasta;
+            else if (tag == '@')
+                format_ = Format::fastq;
+            else
+                return -parse_error("expected FASTA or FASTQ header", 1);
+        }
+        const char expect = format_ == Format::fasta ? '>' : '@';
+        if (tag != expect) return -parse_error("mixed FASTA and FASTQ records are not supported", 1);
+        hdr->erase(0, 1);
+        return format_ == Format::fasta ? read_fasta(seq) : read_fastq(seq);
+    }
+
+   private:
+    int read_fasta(std::string& seq) {
+        for (;;) {
+            const int r = lines_.next(line_);
+            if (r < 0) return -io_error();
+            if (r == 0) return 1;
+            ++line_no_;
+            if (!line_.empty() && line_.front() == '>') {
+                pending_.swap(line_);
+                return 1;
+            }
+            seq += line_;
+        }
+    }
+
+    int read_fastq(std::string& seq) {
+        for (;;) {
+            const int r = lines_.next(line_);
+            if (r < 0) return -io_error();
+            if (r == 0) {
+                const uint32_t col = line_.empty() ? 1 : static_cast<uint32_t>(line_.size());
+                return -parse_error("unterminated FASTQ record: missing '+' separator", col);
+            }
+            ++line_no_;
+            if (!line_.empty() && line_.front() == '+') break;
+            seq += line_;
+        }
+        // Qualities until their length reaches the sequence length.
+        const uint64_t expect = seq.size();
+        uint64_t qual = 0;
+        uint32_t short_col = 1;
+        while (qual < expect) {
+            const int r = lines_.next(line_);
+            if (r < 0) return -io_error();
+            if (r == 0) break;
+            ++line_no_;
+            short_col = line_.empty() ? 1 : static_cast<uint32_t>(line_.size() + 1);
+            qual += line_.size();
+            if (qual > expect) {
+                const uint64_t before = qual - line_.size();
+                const uint64_t idx = expect > before ? expect - before : line_.size();
+                const uint32_t col = line_.empty()
+                                         ? 1
+                                         : static_cast<uint32_t>(std::min<uint64_t>(idx, line_.size() - 1) + 1);
+                return -parse_error("FASTQ quality length exceeds sequence length", col);
+            }
+        }
+        if (qual == expect) return 1;
+        return -parse_error("FASTQ quality length does not match sequence length", short_col);
+    }
+
+    int parse_error(const char* what, uint32_t col) {
+        set_error_location(source_.c_str(), static_cast<uint32_t>(line_no_), col);
+        return set_error(SBF_ERR_FASTX_PARSE, "%s:%llu:%u: %s", source_.c_str(),
+                         static_cast<unsigned long long>(line_no_), col, what);
+    }
+    int io_error() {
+        return set_error(SBF_ERR_IO, "Failed to read FASTA/FASTQ input from %s", source_.c_str());
+    }
+
+    LineReader lines_;
+    std::string source_;
+    std::string line_, pending_;
+    Format format_ = Format::unknown;
+    uint64_t line_no_ = 0;
+};
+
+// Staging budget (detail/fastx_chunk.cuh:97-107).
+size_t staging_budget(double fill_fraction) {
+    if (fill_fraction <= 0.0) return 0;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    const size_t slack = size_t{64} << 20;
+    const size_t avail = free_b > slack ? free_b - slack : 0;
+    const double b = static_cast<double>(avail) * fill_fraction;
+    return b <= 0 ? 0 : static_cast<size_t>(b);
+}
+
+size_t host_chunk_limit() {
+    if (const char* v = std::getenv("SBF_FASTX_MAX_HOST_CHUNK_MB")) {
+        const long long mb = std::strtoll(v, nullptr, 10);
+        if (mb > 0) return static_cast<size_t>(mb) << 20;
+    }
+    return size_t{1} << 30;
+}
+
+// Whether the chunk's estimated staging reaches the budget
+// (fastx_chunk_reached_staging_budget, detail/fastx_chunk.cuh:110-127).
+bool should_flush(bool query, size_t budget, uint64_t raw, uint64_t records, uint32_t k) {
+    if (raw == 0) return false;
+    if (budget == 0) return true;
+    const uint64_t norm = raw + records * 2;
+    uint64_t staging = norm;
+    if (query) staging += norm < k ? 0 : norm - k + 1;
+    return staging >= budget || raw >= host_chunk_limit();
+}
+
+struct Chunk {
+    std::string seq;
+    std::vector<sbf_record_range> ranges;
+    std::vector<std::string> headers;
+    uint64_t first_index = 0;
+    void clear() {
+        seq.clear();
+        ranges.clear();
+        headers.clear();
+    }
+};
+
+struct QueryCtx {
+    const Chunk* chunk;
+    sbf_fastx_record_cb consume;
+    void* user;
+};
+
+int chunk_record_cb(void* u, const sbf_record_view* v) {
+    auto* ctx = static_cast<QueryCtx*>(u);
+    const std::string& h = ctx->chunk->headers[v->record_index];
+    sbf_fastx_record_view fv{ctx->chunk->first_index + v->record_index,
+                             h.data(),
+                             h.size(),
+                             v->sequence,
+                             v->sequence_bytes,
+                             v->queried_bases,
+                             v->queried_kmers,
+                             v->positive_kmers,
+                             v->hits,
+                             v->n_hits};
+    return ctx->consume(ctx->user, &fv);
+}
+
+int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const char* source,
+              double fill_fraction, sbf_stream_t stream, sbf_insert_report* irep,
+              sbf_query_report* qrep, sbf_fastx_record_cb consume, void* cuser) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (!read) return set_error(SBF_ERR_INVALID_ARGUMENT, "read callback is null");
+    FastxParser parser(read, ruser, source ? source : "<stream>");
+    const size_t budget = staging_budget(fill_fraction);
+    Chunk chunk;
+    sbf_insert_report it{0, 0, 0};
+    sbf_query_report qt{0, 0, 0, 0};
+    uint64_t next_index = 0;
+    std::string header, seq;
+    auto flush = [&]() -> int {
+        if (chunk.ranges.empty()) return SBF_OK;
+        if (query) {
+            sbf_query_report r{};
+            QueryCtx ctx{&chunk, consume, cuser};
+            const int s = sbf_query_record_batch(f, chunk.seq.data(), chunk.seq.size(),
+                                                 chunk.ranges.data(), chunk.ranges.size(), stream,
+                                                 &r, consume ? chunk_record_cb : nullptr, &ctx);
+            if (s != SBF_OK) return s;
+            qt.records_queried += r.records_queried;
+            qt.queried_bases += r.queried_bases;
+            qt.queried_kmers += r.queried_kmers;
+            qt.positive_kmers += r.positive_kmers;
+        } else {
+            sbf_insert_report r{};
+            const int s = sbf_insert_record_batch(f, chunk.seq.data(), chunk.seq.size(),
+                                                  chunk.ranges.data(), chunk.ranges.size(),
+                                                  stream, &r);
+            if (s != SBF_OK) return s;
+            it.records_indexed += r.records_indexed;
+            it.indexed_bases += r.indexed_bases;
+            it.inserted_kmers += r.inserted_kmers;
+        }
+        chunk.clear();
+        chunk.first_index = next_index;
+        return SBF_OK;
+    };
+    for (;;) {
+        const int r = parser.next(header, seq);
+        if (r < 0) return -r;
+        if (r == 0) break;
+        chunk.ranges.push_back(sbf_record_range{chunk.seq.size(), seq.size()});
+        chunk.seq += seq;
+        if (query && consume) chunk.headers.push_back(header);
+        ++next_index;
+        if (should_flush(query, budget, chunk.seq.size(), chunk.ranges.size(), f->k)) {
+            const int s = flush();
+            if (s != SBF_OK) return s;
+        }
+    }
+    const int s = flush();
+    if (s != SBF_OK) return s;
+    if (irep) *irep = it;
+    if (qrep) *qrep = qt;
+    return SBF_OK;
+}
+
+int64_t gz_read(void* user, char* buf, uint64_t cap) {
+    const unsigned chunk = static_cast<unsigned>(std::min<uint64_t>(cap, 1u << 30));
+    const int n = gzread(static_cast<gzFile>(user), buf, chunk);
+    return n < 0 ? -1 : n;
+}
+
+// Opens a plain or gzip file (zlib reads uncompressed files unchanged).
+int open_fastx(const char* path, gzFile* out) {
+    if (!path) return set_error(SBF_ERR_INVALID_ARGUMENT, "path is null");
+    gzFile g = gzopen(path, "rb");
+    if (!g) return set_error(SBF_ERR_IO, "Failed to open FASTA/FASTQ file: %s", path);
+    gzbuffer(g, 1 << 20);
+    *out = g;
+    return SBF_OK;
+}
+
+}  // namespace
+
+}  // namespace sbf
+
+using namespace sbf;
+
+extern "C" int sbf_fastx_scan(sbf_read_fn read, void* ruser, const char* source_name,
+                              sbf_fastx_scan_cb consume, void* user, uint64_t* records_out) {
+    if (!read || !consume) return set_error(SBF_ERR_INVALID_ARGUMENT, "null callback");
+    FastxParser parser(read, ruser, source_name ? source_name : "<stream>");
+    std::string header, seq;
+    uint64_t n = 0;
+    for (;;) {
+        const int r = parser.next(header, seq);
+        if (r < 0) return -r;
+        if (r == 0) break;
+        if (consume(user, n, header.data(), header.size(), seq.data(), seq.size()) != 0)
+            return set_error(SBF_ERR_ABORTED, "record consumer aborted the scan");
+        ++n;
+    }
+    if (records_out) *records_out = n;
+    return SBF_OK;
+}
+
+extern "C" int sbf_fastx_scan_file(const char* path, sbf_fastx_scan_cb consume, void* user,
+                                   uint64_t* records_out) {
+    gzFile g = nullptr;
+    const int o = open_fastx(path, &g);
+    if (o != SBF_OK) return o;
+    const int s = sbf_fastx_scan(gz_read, g, path, consume, user, records_out);
+    gzclose(g);
+    return s;
+}
+
+extern "C" int sbf_insert_fastx(sbf_filter_t* f, sbf_read_fn read, void* ruser,
+                                const char* source_name, double fill_fraction,
+                                sbf_stream_t stream, sbf_insert_report* report) {
+    return run_fastx(f, false, read, ruser, source_name, fill_fraction, stream, report, nullptr,
+                     nullptr, nullptr);
+}
+
+extern "C" int sbf_insert_fastx_file(sbf_filter_t* f, const char* path, double fill_fraction,
+                                     sbf_stream_t stream, sbf_insert_report* report) {
+    gzFile g = nullptr;
+    const int o = open_fastx(path, &g);
+    if (o != SBF_OK) return o;
+    const int s = run_fastx(f, false, gz_read, g, path, fill_fraction, stream, report, nullptr,
+                            nullptr, nullptr);
+    gzclose(g);
+    return s;
+}
+
+extern "C" int sbf_query_fastx(const sbf_filter_t* f, sbf_read_fn read, void* ruser,
+                               const char* source_name, double fill_fraction, sbf_stream_t stream,
+                               sbf_query_report* report, sbf_fastx_record_cb consume,
+                               void* user) {
+    return run_fastx(const_cast<sbf_filter*>(f), true, read, ruser, source_name, fill_fraction,
+                     stream, nullptr, report, consume, user);
+}
+
+extern "C" int sbf_query_fastx_file(const sbf_filter_t* f, const char* path, double fill_fraction,
+                                    sbf_stream_t stream, sbf_query_report* report,
+                                    sbf_fastx_record_cb consume, void* user) {
+    gzFile g = nullptr;
+    const int o = open_fastx(path, &g);
+    if (o != SBF_OK) return o;
+    const int s = run_fastx(const_cast<sbf_filter*>(f), true, gz_read, g, path, fill_fraction,
+                            stream, nullptr, report, consume, user);
+    gzclose(g);
+    return s;
+}

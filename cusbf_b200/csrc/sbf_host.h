@@ -5,12 +5,15 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
+#include "../../include/sbf_b200.h"
 #include "sbf_internal.h"
 
 namespace sbf {
 
 int set_error(int status, const char* fmt, ...);
+void set_error_location(const char* file, uint32_t line, uint32_t col);
 int cuda_fail(cudaError_t e, const char* what);
 bool is_pinned(const void* p);
 
@@ -23,6 +26,14 @@ struct Staging {
     size_t pin_cap = 0;
     int ensure_device(size_t bytes);
     int ensure_pinned(size_t bytes);
+    void release();
+};
+
+// A grow-only device buffer.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes);
     void release();
 };
 
@@ -46,7 +57,15 @@ struct sbf_filter {
     cudaEvent_t ev_copied[2] = {nullptr, nullptr};
     cudaEvent_t ev_done[2] = {nullptr, nullptr};
 
+    // Record-batch staging (sbf_records.cu).
+    sbf::DevBuf rb_dense, rb_norm, rb_meta, rb_hits, rb_stats;
+
     uint64_t kmers_of(uint64_t symbols) const;
+    int stage_record_batch(const char* h_seq, uint64_t len, const sbf_record_range* r, uint64_t n,
+                           cudaStream_t st, std::vector<uint64_t>& out_off, uint64_t& norm_len);
+    int record_stats(const sbf_record_range* r, uint64_t n, const uint8_t* d_hits,
+                     cudaStream_t st, std::vector<uint64_t>& valid,
+                     std::vector<uint64_t>& positive);
     int launch(bool query, bool dense, const void* input, uint64_t input_bytes, uint64_t n_kmers,
                uint8_t* out, cudaStream_t st) const;
     int host_pipeline(bool query, bool dense, const void* h_in, uint64_t in_bytes,

@@ -1,0 +1,443 @@
+// sbf_records.cu -- record batches: separator injection, query layout, per-record
+// counts, and the record-batch entry points of the C ABI.
+//
+// Semantics follow the reference (tdortman/cuSBF):
+//   * normalisation: records are joined with one separator symbol ('N' for
+//     DNA) between consecutive records once any content has been written;
+//     trailing partial symbols pad with separators first
+//     (include/cusbf/normalized_record_batch.hpp:113-121, :209-276);
+//   * range validation (normalized_record_batch.hpp:123-147, filter.cuh:848-876);
+//   * query layout: hit_offset = logical_offset / symbolWidth, hit_count =
+//     symbols - k + 1, total = windows of the whole normalised sequence
+//     (include/cusbf/detail/query_layout.cuh:42-72);
+//   * per-record valid k-mers (normalized_record_batch.hpp:88-110) and
+//     positive k-mers (include/cusbf/detail/count_positive_kmers.cuh:21-45).
+// The reference normalises on the host with memcpy; here the dense record
+// bytes are copied to the device once and a gather kernel injects the
+// separators, and per-record counts come from one segmented device pass.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "../../include/sbf_b200.h"
+#include "sbf_host.h"
+#include "sbf_internal.h"
+
+using namespace sbf;
+
+namespace sbf {
+
+constexpr uint8_t kSeparator = 'N';
+constexpr uint64_t kStatSegment = 1u << 16;  // bytes of a record per stats work item
+
+// ---------------------------------------------------------------------------
+// Host layout
+// ---------------------------------------------------------------------------
+
+int validate_ranges(uint64_t len, const sbf_record_range* r, uint64_t n) {
+    uint64_t next = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (r[i].sequence_offset < next)
+            return set_error(SBF_ERR_INVALID_ARGUMENT,
+                             "record batch ranges must be ordered and non-overlapping");
+        if (r[i].sequence_offset > len || r[i].sequence_bytes > len - r[i].sequence_offset)
+            return set_error(SBF_ERR_INVALID_ARGUMENT,
+                             "record batch range exceeds the source sequence");
+        next = r[i].sequence_offset + r[i].sequence_bytes;
+    }
+    return SBF_OK;
+}
+
+// Normalised offsets: out_off[i] = (bytes of records before i) + (separators
+// before i); a separator precedes record i exactly when some earlier record
+// is non-empty.  Returns the normalised length.
+uint64_t normalized_offsets(const sbf_record_range* r, uint64_t n, uint64_t* out_off) {
+    uint64_t pos = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (pos != 0) pos += 1;
+        out_off[i] = pos;
+        pos += r[i].sequence_bytes;
+    }
+    return pos;
+}
+
+// ---------------------------------------------------------------------------
+// Device kernels
+// ---------------------------------------------------------------------------
+
+// One warp per record (grid-strided): copies the record's bytes from the
+// dense source to its normalised offset and writes the separator before it.
+__global__ void normalize_gather_kernel(const uint8_t* dense, uint64_t dense_base,
+                                        const sbf_record_range* ranges, const uint64_t* out_off,
+                                        uint64_t n, uint8_t* out) {
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    for (uint64_t r = warp; r < n; r += warps) {
+        const uint64_t dst = out_off[r];
+        const uint64_t src = ranges[r].sequence_offset - dense_base;
+        const uint64_t len = ranges[r].sequence_bytes;
+        if (dst != 0 && lane == 0) out[dst - 1] = kSeparator;
+        for (uint64_t x = lane; x < len; x += 32) out[dst + x] = dense[src + x];
+    }
+}
+
+// Per-record statistics over segments of at most kStatSegment window starts:
+// valid windows (K consecutive A/C/G/T bytes) and, when `hits` is given,
+// positive windows.  One warp per segment; counters are accumulated with
+// atomics because long records span several segments.
+struct StatSegment {
+    uint64_t record;
+    uint64_t begin;  // first window start of the segment (record-relative)
+    uint64_t end;    // one past the last window start
+};
+
+__device__ __forceinline__ bool dna_valid(uint8_t b) {
+    const uint8_t u = b & 0xDFu;
+    return u == 'A' || u == 'C' || u == 'G' || u == 'T';
+}
+
+__global__ void record_stats_kernel(const uint8_t* norm, const uint64_t* out_off,
+                                    const sbf_record_range* ranges, const StatSegment* segs,
+                                    uint64_t n_segs, uint32_t k, const uint8_t* hits,
+                                    unsigned long long* valid_out,
+                                    unsigned long long* positive_out) {
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint64_t s = warp; s < n_segs; s += warps) {
+        const StatSegment sg = segs[s];
+        const uint8_t* rec = norm + out_off[sg.record];
+        const uint64_t size = ranges[sg.record].sequence_bytes;
+        // A window starting at p is valid iff bytes [p, p+k) are all valid.
+        // Scan window ends e in [begin+k-1, end+k-1) tracking the position of
+        // the last invalid byte, starting k-1 bytes early so the first window
+        // sees its whole span.
+        const uint64_t scan0 = sg.begin;
+        const uint64_t scan1 = sg.end + k - 1;  // <= size
+        int64_t last_inv = static_cast<int64_t>(scan0) - 1;  // nothing invalid before scan0 matters
+        unsigned long long valid = 0, pos = 0;
+        for (uint64_t base = scan0; base < scan1; base += 32) {
+            const uint64_t e = base + lane;
+            const bool in = e < scan1;
+            const bool inv = in && !dna_valid(rec[e]);
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, inv);
+            const uint32_t upto = m & (0xFFFFFFFFu >> (31 - lane));
+            const int64_t li = upto ? static_cast<int64_t>(base) + (31 - __clz(upto)) : last_inv;
+            const bool window_valid = in && e >= scan0 + k - 1 && (static_cast<int64_t>(e) - li) >= k;
+            valid += __popc(__ballot_sync(0xFFFFFFFFu, window_valid));
+            if (m) last_inv = static_cast<int64_t>(base) + (31 - __clz(m));
+        }
+        (void)size;
+        if (hits) {
+            const uint8_t* h = hits + out_off[sg.record];
+            unsigned long long local = 0;
+            for (uint64_t p = sg.begin + lane; p < sg.end; p += 32) local += h[p];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xFFFFFFFFu, local, o);
+            pos = local;
+        }
+        if (lane == 0) {
+            if (valid) atomicAdd(valid_out + sg.record, valid);
+            if (hits && pos) atomicAdd(positive_out + sg.record, pos);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Device staging of a host record batch
+// ---------------------------------------------------------------------------
+
+// Grow-only device buffer owned by a filter.
+int DevBuf::ensure(size_t bytes) {
+    if (bytes <= cap) return SBF_OK;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    const size_t want = std::max<size_t>(bytes, 4096);
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(SBF_ERR_RESOURCE, "cannot allocate %zu bytes of device staging", want);
+    }
+    cap = want;
+    return SBF_OK;
+}
+
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+}
+
+}  // namespace sbf
+
+#define SBF_CUDA(expr)                                      \
+    do {                                                    \
+        cudaError_t _e = (expr);                            \
+        if (_e != cudaSuccess) return cuda_fail(_e, #expr); \
+    } while (0)
+#define SBF_TRY(expr)                \
+    do {                             \
+        int _s = (expr);             \
+        if (_s != SBF_OK) return _s; \
+    } while (0)
+
+static inline cudaStream_t S(sbf_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Stages a host record batch on the device: dense bytes + ranges + offsets,
+// gathers the normalised sequence.  Fills `layout` (host) and returns the
+// normalised length in `norm_len`.
+int sbf_filter::stage_record_batch(const char* h_seq, uint64_t len, const sbf_record_range* r,
+                                   uint64_t n, cudaStream_t st, std::vector<uint64_t>& out_off,
+                                   uint64_t& norm_len) {
+    SBF_TRY(validate_ranges(len, r, n));
+    out_off.resize(n);
+    norm_len = normalized_offsets(r, n, out_off.data());
+    if (n == 0 || norm_len == 0) return SBF_OK;
+    // The dense span covering every record.
+    uint64_t lo = r[0].sequence_offset, hi = 0;
+    for (uint64_t i = 0; i < n; ++i) hi = std::max(hi, r[i].sequence_offset + r[i].sequence_bytes);
+    const uint64_t span = hi - lo;
+    SBF_TRY(rb_dense.ensure(span + 16));
+    SBF_TRY(rb_norm.ensure(norm_len + 16));
+    SBF_TRY(rb_meta.ensure(n * (sizeof(sbf_record_range) + sizeof(uint64_t)) + 64));
+    auto* d_ranges = static_cast<sbf_record_range*>(rb_meta.ptr);
+    auto* d_off = reinterpret_cast<uint64_t*>(d_ranges + n);
+    SBF_CUDA(cudaMemcpyAsync(rb_dense.ptr, h_seq + lo, span, cudaMemcpyHostToDevice, st));
+    SBF_CUDA(cudaMemcpyAsync(d_ranges, r, n * sizeof(sbf_record_range), cudaMemcpyHostToDevice, st));
+    SBF_CUDA(cudaMemcpyAsync(d_off, out_off.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    const uint64_t warps = std::min<uint64_t>(n, static_cast<uint64_t>(sms) * 64);
+    normalize_gather_kernel<<<static_cast<unsigned>((warps * 32 + 255) / 256), 256, 0, st>>>(
+        static_cast<const uint8_t*>(rb_dense.ptr), lo, d_ranges, d_off, n,
+        static_cast<uint8_t*>(rb_norm.ptr));
+    SBF_CUDA(cudaGetLastError());
+    // The host layout vector must stay alive until the copies complete.
+    SBF_CUDA(cudaStreamSynchronize(st));
+    return SBF_OK;
+}
+
+// Per-record valid (and, with hits, positive) counts into host vectors.
+int sbf_filter::record_stats(const sbf_record_range* r, uint64_t n, const uint8_t* d_hits,
+                             cudaStream_t st, std::vector<uint64_t>& valid,
+                             std::vector<uint64_t>& positive) {
+    valid.assign(n, 0);
+    positive.assign(n, 0);
+    std::vector<StatSegment> segs;
+    segs.reserve(n);
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint64_t size = r[i].sequence_bytes;
+        if (size < k) continue;
+        const uint64_t windows = size - k + 1;
+        for (uint64_t b = 0; b < windows; b += kStatSegment)
+            segs.push_back(StatSegment{i, b, std::min<uint64_t>(windows, b + kStatSegment)});
+    }
+    if (segs.empty()) return SBF_OK;
+    SBF_TRY(rb_stats.ensure(segs.size() * sizeof(StatSegment) + 2 * n * 8 + 64));
+    auto* d_segs = static_cast<StatSegment*>(rb_stats.ptr);
+    auto* d_valid = reinterpret_cast<unsigned long long*>(d_segs + segs.size());
+    auto* d_pos = d_valid + n;
+    SBF_CUDA(cudaMemcpyAsync(d_segs, segs.data(), segs.size() * sizeof(StatSegment),
+                             cudaMemcpyHostToDevice, st));
+    SBF_CUDA(cudaMemsetAsync(d_valid, 0, 2 * n * 8, st));
+    const auto* d_ranges = static_cast<const sbf_record_range*>(rb_meta.ptr);
+    const auto* d_off = reinterpret_cast<const uint64_t*>(d_ranges + n);
+    const uint64_t warps = std::min<uint64_t>(segs.size(), static_cast<uint64_t>(sms) * 64);
+    record_stats_kernel<<<static_cast<unsigned>((warps * 32 + 255) / 256), 256, 0, st>>>(
+        static_cast<const uint8_t*>(rb_norm.ptr), d_off, d_ranges, d_segs, segs.size(), k,
+        d_hits, d_valid, d_pos);
+    SBF_CUDA(cudaGetLastError());
+    SBF_CUDA(cudaMemcpyAsync(valid.data(), d_valid, n * 8, cudaMemcpyDeviceToHost, st));
+    if (d_hits)
+        SBF_CUDA(cudaMemcpyAsync(positive.data(), d_pos, n * 8, cudaMemcpyDeviceToHost, st));
+    SBF_CUDA(cudaStreamSynchronize(st));
+    return SBF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI: host helpers (no GPU)
+// ---------------------------------------------------------------------------
+
+extern "C" int sbf_validate_record_batch(uint64_t len, const sbf_record_range* ranges,
+                                         uint64_t n) {
+    if (n && !ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "ranges pointer is null");
+    return validate_ranges(len, ranges, n);
+}
+
+extern "C" uint64_t sbf_normalized_batch_bytes(const sbf_record_range* ranges, uint64_t n) {
+    uint64_t size = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (i != 0 || size != 0) size += 1;
+        size += ranges[i].sequence_bytes;
+    }
+    return size;
+}
+
+extern "C" int sbf_normalize_record_batch(uint32_t k, const char* h_seq, uint64_t len,
+                                          const sbf_record_range* ranges, uint64_t n, char* out,
+                                          uint64_t out_cap, uint64_t* out_len,
+                                          sbf_normalized_record* records_out) {
+    if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    SBF_TRY(validate_ranges(len, ranges, n));
+    std::vector<uint64_t> off(n);
+    const uint64_t total = normalized_offsets(ranges, n, off.data());
+    if (out_len) *out_len = total;
+    if (out && out_cap < total)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "normalised output buffer is too small");
+    for (uint64_t i = 0; i < n; ++i) {
+        const char* src = h_seq + ranges[i].sequence_offset;
+        const uint64_t size = ranges[i].sequence_bytes;
+        if (out) {
+            if (off[i] != 0) out[off[i] - 1] = static_cast<char>(kSeparator);
+            std::memcpy(out + off[i], src, size);
+        }
+        if (records_out) {
+            // valid_record_kmer_count (normalized_record_batch.hpp:88-110).
+            uint64_t valid = 0;
+            if (size >= k) {
+                uint64_t invalid = 0;
+                auto bad = [&](uint64_t p) {
+                    const uint8_t u = static_cast<uint8_t>(src[p]) & 0xDFu;
+                    return !(u == 'A' || u == 'C' || u == 'G' || u == 'T');
+                };
+                for (uint64_t p = 0; p < k; ++p) invalid += bad(p);
+                valid = invalid == 0;
+                for (uint64_t s = 1; s + k <= size; ++s) {
+                    invalid -= bad(s - 1);
+                    invalid += bad(s + k - 1);
+                    valid += invalid == 0;
+                }
+            }
+            records_out[i] = sbf_normalized_record{i, ranges[i].sequence_offset, size, valid};
+        }
+    }
+    return SBF_OK;
+}
+
+extern "C" int sbf_query_layout(uint32_t k, const sbf_normalized_record* records, uint64_t n,
+                                sbf_query_layout_record* out, uint64_t* total_hits) {
+    if (n && (!records || !out)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    uint64_t logical = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (logical != 0) logical += 1;
+        const uint64_t size = records[i].size;
+        out[i] = sbf_query_layout_record{records[i].record_index, records[i].input_offset, size,
+                                         records[i].valid_kmers, logical,
+                                         size < k ? 0 : size - k + 1};
+        logical += size;
+    }
+    if (total_hits) *total_hits = logical < k ? 0 : logical - k + 1;
+    return SBF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI: device record batches (separators already in place)
+// ---------------------------------------------------------------------------
+
+extern "C" int sbf_insert_record_batch_async(sbf_filter_t* f, const char* d_seq, uint64_t len,
+                                             const sbf_record_range* ranges, uint64_t n,
+                                             sbf_stream_t stream, uint64_t* kmers_out) {
+    if (kmers_out) *kmers_out = 0;
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (n && !ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "ranges pointer is null");
+    SBF_TRY(validate_ranges(len, ranges, n));
+    uint64_t total = 0;
+    for (uint64_t i = 0; i < n; ++i) total += f->kmers_of(ranges[i].sequence_bytes);
+    if (kmers_out) *kmers_out = total;
+    if (total == 0) return SBF_OK;
+    return f->launch(false, false, d_seq, len, f->kmers_of(len), nullptr, S(stream));
+}
+
+extern "C" int sbf_contains_record_batch_async(const sbf_filter_t* f, const char* d_seq,
+                                               uint64_t len, const sbf_record_range* ranges,
+                                               uint64_t n, uint8_t* d_out, uint64_t out_len,
+                                               sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (n && !ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "ranges pointer is null");
+    SBF_TRY(validate_ranges(len, ranges, n));
+    const uint64_t total = f->kmers_of(len);
+    if (total == 0) return SBF_OK;
+    if (!d_out || out_len < total)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "record batch query output span is too small");
+    return f->launch(true, false, d_seq, len, total, d_out, S(stream));
+}
+
+// ---------------------------------------------------------------------------
+// C ABI: host record batches
+// ---------------------------------------------------------------------------
+
+extern "C" int sbf_insert_record_batch(sbf_filter_t* f, const char* h_seq, uint64_t len,
+                                       const sbf_record_range* ranges, uint64_t n,
+                                       sbf_stream_t stream, sbf_insert_report* report) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    cudaStream_t st = S(stream);
+    std::vector<uint64_t> off;
+    uint64_t norm_len = 0;
+    SBF_TRY(f->stage_record_batch(h_seq, len, ranges, n, st, off, norm_len));
+    sbf_insert_report rep{n, 0, 0};
+    for (uint64_t i = 0; i < n; ++i) rep.indexed_bases += ranges[i].sequence_bytes;
+    const uint64_t windows = f->kmers_of(norm_len);
+    if (windows) {
+        SBF_TRY(f->launch(false, false, f->rb_norm.ptr, norm_len, windows, nullptr, st));
+        std::vector<uint64_t> valid, pos;
+        SBF_TRY(f->record_stats(ranges, n, nullptr, st, valid, pos));
+        for (uint64_t v : valid) rep.inserted_kmers += v;
+        SBF_TRY(f->check_device_error(st));
+    }
+    if (report) *report = rep;
+    return SBF_OK;
+}
+
+extern "C" int sbf_query_record_batch(const sbf_filter_t* cf, const char* h_seq, uint64_t len,
+                                      const sbf_record_range* ranges, uint64_t n,
+                                      sbf_stream_t stream, sbf_query_report* report,
+                                      sbf_record_query_cb consume, void* user) {
+    auto* f = const_cast<sbf_filter*>(cf);
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    cudaStream_t st = S(stream);
+    std::vector<uint64_t> off;
+    uint64_t norm_len = 0;
+    SBF_TRY(f->stage_record_batch(h_seq, len, ranges, n, st, off, norm_len));
+    sbf_query_report rep{n, 0, 0, 0};
+    for (uint64_t i = 0; i < n; ++i) rep.queried_bases += ranges[i].sequence_bytes;
+    const uint64_t windows = f->kmers_of(norm_len);
+    std::vector<uint64_t> valid(n, 0), pos(n, 0);
+    std::vector<uint8_t> hits;
+    if (windows) {
+        SBF_TRY(f->rb_hits.ensure(windows + 64));
+        auto* d_hits = static_cast<uint8_t*>(f->rb_hits.ptr);
+        SBF_TRY(f->launch(true, false, f->rb_norm.ptr, norm_len, windows, d_hits, st));
+        SBF_TRY(f->record_stats(ranges, n, d_hits, st, valid, pos));
+        if (consume) {
+            hits.resize(windows);
+            SBF_CUDA(cudaMemcpyAsync(hits.data(), d_hits, windows, cudaMemcpyDeviceToHost, st));
+        }
+        SBF_TRY(f->check_device_error(st));
+    }
+    for (uint64_t i = 0; i < n; ++i) {
+        rep.queried_kmers += valid[i];
+        rep.positive_kmers += pos[i];
+    }
+    if (consume) {
+        for (uint64_t i = 0; i < n; ++i) {
+            const uint64_t size = ranges[i].sequence_bytes;
+            const uint64_t hc = f->kmers_of(size);
+            sbf_record_view v{i,
+                              h_seq + ranges[i].sequence_offset,
+                              size,
+                              size,
+                              valid[i],
+                              pos[i],
+                              hc ? hits.data() + off[i] : nullptr,
+                              hc};
+            if (consume(user, &v) != 0)
+                return set_error(SBF_ERR_ABORTED, "record consumer aborted the query");
+        }
+    }
+    if (report) *report = rep;
+    return SBF_OK;
+}

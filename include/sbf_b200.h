@@ -39,6 +39,7 @@ typedef enum {
     SBF_ERR_FASTX_PARSE = 3,      /* ErrorCategory::fastx_parse      */
     SBF_ERR_INVALID_ARGUMENT = 4, /* ErrorCategory::invalid_argument */
     SBF_ERR_RESOURCE = 5,         /* ErrorCategory::resource         */
+    SBF_ERR_ABORTED = 6,          /* a consumer callback asked to stop */
 } sbf_status;
 
 /* Alphabet ids (include/cusbf/Alphabet.cuh:113-220).  The GPU engine
@@ -67,10 +68,72 @@ typedef struct {
     uint64_t positive_kmers;
 } sbf_query_report;
 
+/* NormalizedRecord (include/cusbf/normalized_record_batch.hpp:20-29). */
+typedef struct {
+    uint64_t record_index;
+    uint64_t input_offset;
+    uint64_t size;
+    uint64_t valid_kmers;
+} sbf_normalized_record;
+
+/* QueryLayoutRecord (include/cusbf/detail/query_layout.cuh:13-20). */
+typedef struct {
+    uint64_t record_index;
+    uint64_t input_offset;
+    uint64_t size;
+    uint64_t valid_kmers;
+    uint64_t hit_offset;
+    uint64_t hit_count;
+} sbf_query_layout_record;
+
+/* RecordQueryView (include/cusbf/Fastx.hpp:135-148): one record's result,
+ * valid only during the callback.  `hits` has `n_hits` bytes (1 = present). */
+typedef struct {
+    uint64_t record_index;
+    const char* sequence;
+    uint64_t sequence_bytes;
+    uint64_t queried_bases;
+    uint64_t queried_kmers;
+    uint64_t positive_kmers;
+    const uint8_t* hits;
+    uint64_t n_hits;
+} sbf_record_view;
+
+/* Per-record consumer of the record-batch query API (RecordQueryConsumer,
+ * Fastx.hpp:223-226).  Returning non-zero aborts the call, which then
+ * returns SBF_ERR_ABORTED (the C++ headers rethrow the consumer's exception,
+ * as the reference lets it propagate); the filter stays usable. */
+typedef int (*sbf_record_query_cb)(void* user, const sbf_record_view* record);
+
+/* FastxRecordView (include/cusbf/Fastx.hpp:173-188). */
+typedef struct {
+    uint64_t record_index;
+    const char* header;
+    uint64_t header_bytes;
+    const char* sequence;
+    uint64_t sequence_bytes;
+    uint64_t queried_bases;
+    uint64_t queried_kmers;
+    uint64_t positive_kmers;
+    const uint8_t* hits;
+    uint64_t n_hits;
+} sbf_fastx_record_view;
+
+/* Per-record consumer of the FASTX query APIs (FastxRecordConsumer,
+ * Fastx.hpp:235-238); non-zero aborts like sbf_record_query_cb. */
+typedef int (*sbf_fastx_record_cb)(void* user, const sbf_fastx_record_view* record);
+
+/* Pull-style input for the FASTX stream APIs: copies up to `cap` bytes into
+ * `buf` and returns the count, 0 at end of input, or -1 on a read error. */
+typedef int64_t (*sbf_read_fn)(void* user, char* buf, uint64_t cap);
+
 /* ---- errors --------------------------------------------------------- */
 
 /* Message of the calling thread's last failure ("" if none). */
 const char* sbf_last_error_message(void);
+/* Source location of the calling thread's last SBF_ERR_FASTX_PARSE failure
+ * (FastxParseError::location, error.hpp:53-56): file, 1-based line, column. */
+int sbf_last_error_location(const char** file, uint32_t* line, uint32_t* column);
 /* cudaError_t of the calling thread's last SBF_ERR_CUDA failure. */
 int sbf_last_cuda_error(void);
 /* Library version string. */
@@ -148,6 +211,81 @@ int sbf_contains_dense_packed_to_device(const sbf_filter_t* filter, const uint64
 int sbf_contains_dense_packed(const sbf_filter_t* filter, const uint64_t* h_words,
                               uint64_t n_words, uint64_t num_symbols, uint8_t* h_out,
                               uint64_t out_len, sbf_stream_t stream);
+
+/* ---- record batches (filter.cuh:338-400, :549-622) ----------------- */
+
+/* validateRecordBatch (normalized_record_batch.hpp:123-147): ranges must be
+ * ordered, non-overlapping and inside `len` bytes.  Host only. */
+int sbf_validate_record_batch(uint64_t len, const sbf_record_range* ranges, uint64_t n);
+/* estimate_normalized_batch_bytes (normalized_record_batch.hpp:179-194). */
+uint64_t sbf_normalized_batch_bytes(const sbf_record_range* ranges, uint64_t n);
+/* normalize_record_batch_into (normalized_record_batch.hpp:289-304), on the
+ * host: joins records with one 'N' and fills per-record metadata
+ * (`records_out` may be NULL; `out` may be NULL to size the output). */
+int sbf_normalize_record_batch(uint32_t k, const char* h_seq, uint64_t len,
+                               const sbf_record_range* ranges, uint64_t n, char* out,
+                               uint64_t out_cap, uint64_t* out_len,
+                               sbf_normalized_record* records_out);
+/* QueryLayout::build (include/cusbf/detail/query_layout.cuh:42-72). */
+int sbf_query_layout(uint32_t k, const sbf_normalized_record* records, uint64_t n,
+                     sbf_query_layout_record* out, uint64_t* total_hits);
+
+/* insert_record_batch (filter.cuh:338-364): host records, separators injected
+ * on the device; synchronises. */
+int sbf_insert_record_batch(sbf_filter_t* filter, const char* h_seq, uint64_t len,
+                            const sbf_record_range* ranges, uint64_t n, sbf_stream_t stream,
+                            sbf_insert_report* report);
+/* insert_record_batch_async (filter.cuh:385-400): device sequence with the
+ * separators already in place; `kmers_out` = attempted windows per record. */
+int sbf_insert_record_batch_async(sbf_filter_t* filter, const char* d_seq, uint64_t len,
+                                  const sbf_record_range* ranges, uint64_t n,
+                                  sbf_stream_t stream, uint64_t* kmers_out);
+/* query_record_batch (filter.cuh:549-582): aggregate report, and with a
+ * non-NULL `consume` one callback per record in order. */
+int sbf_query_record_batch(const sbf_filter_t* filter, const char* h_seq, uint64_t len,
+                           const sbf_record_range* ranges, uint64_t n, sbf_stream_t stream,
+                           sbf_query_report* report, sbf_record_query_cb consume, void* user);
+/* contains_record_batch_async (filter.cuh:603-622). */
+int sbf_contains_record_batch_async(const sbf_filter_t* filter, const char* d_seq, uint64_t len,
+                                    const sbf_record_range* ranges, uint64_t n, uint8_t* d_out,
+                                    uint64_t out_len, sbf_stream_t stream);
+
+/* ---- FASTA / FASTQ (filter.cuh:402-786, Fastx.hpp:297-481) ----------- */
+
+/* Record consumer of sbf_fastx_scan: header (without '>'/'@') and sequence
+ * of record `index`; non-zero stops the scan. */
+typedef int (*sbf_fastx_scan_cb)(void* user, uint64_t index, const char* header,
+                                 uint64_t header_bytes, const char* sequence,
+                                 uint64_t sequence_bytes);
+/* FastxReader::nextRecord (Fastx.hpp:314-354) over a whole input, host only:
+ * one callback per record; parse errors as SBF_ERR_FASTX_PARSE. */
+int sbf_fastx_scan(sbf_read_fn read, void* read_user, const char* source_name,
+                   sbf_fastx_scan_cb consume, void* user, uint64_t* records_out);
+/* The same over a plain or gzip file (openFastxFile, Fastx.hpp:470-481). */
+int sbf_fastx_scan_file(const char* path, sbf_fastx_scan_cb consume, void* user,
+                        uint64_t* records_out);
+
+/* insert_fastx (filter.cuh:416-421): FASTA or FASTQ (format from the first
+ * header; wrapped lines and CRLF accepted; FASTQ quality lengths checked)
+ * read through `read`; records are accumulated into chunks whose device
+ * staging stays within fill_fraction * (free memory - 64 MiB) (a fraction of
+ * 0 or less flushes every record) and inserted as record batches, so no
+ * k-mer spans two records.  `source_name` labels parse errors. */
+int sbf_insert_fastx(sbf_filter_t* filter, sbf_read_fn read, void* read_user,
+                     const char* source_name, double fill_fraction, sbf_stream_t stream,
+                     sbf_insert_report* report);
+/* insert_fastx_file (filter.cuh:437-452): plain or gzip-compressed file. */
+int sbf_insert_fastx_file(sbf_filter_t* filter, const char* path, double fill_fraction,
+                          sbf_stream_t stream, sbf_insert_report* report);
+/* query_fastx / query_fastx_records (filter.cuh:632-735): aggregate report;
+ * with a non-NULL `consume`, one FastxRecordView per record in source order. */
+int sbf_query_fastx(const sbf_filter_t* filter, sbf_read_fn read, void* read_user,
+                    const char* source_name, double fill_fraction, sbf_stream_t stream,
+                    sbf_query_report* report, sbf_fastx_record_cb consume, void* user);
+/* query_fastx_file / query_fastx_file_records (filter.cuh:654-735). */
+int sbf_query_fastx_file(const sbf_filter_t* filter, const char* path, double fill_fraction,
+                         sbf_stream_t stream, sbf_query_report* report,
+                         sbf_fastx_record_cb consume, void* user);
 
 #ifdef __cplusplus
 }
