@@ -193,6 +193,8 @@ _sig("sbf_insert_record_batch_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, C
 _sig("sbf_query_record_batch", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, C.POINTER(QueryReport),
      RECORD_CB, _vp)
 _sig("sbf_contains_record_batch_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _vp)
+_sig("sbf_record_batch_counts_noalloc", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _vp,
+     _vp, _vp)
 _sig("sbf_fastx_scan", C.c_int, READ_FN, _vp, C.c_char_p, SCAN_CB, _vp, C.POINTER(_u64))
 _sig("sbf_fastx_scan_file", C.c_int, C.c_char_p, SCAN_CB, _vp, C.POINTER(_u64))
 _sig("sbf_insert_fastx", C.c_int, _vp, READ_FN, _vp, C.c_char_p, C.c_double, _vp,
@@ -512,8 +514,22 @@ def _record_methods():
         _check(_lib.sbf_contains_record_batch_async(self._h, p, n, _np_ptr(r), r.shape[0], o, on,
                                                     _stream(stream)))
 
+    def record_batch_counts_noalloc(self, d_seq, ranges, d_hits=None, stream=None):
+        """Per-record (valid, positive) k-mer counts of a device record batch,
+        allocating nothing (sbf_record_batch_counts_noalloc; at most 262144
+        records; calls on one device must not overlap)."""
+        p, n = _dev_ptr(d_seq)
+        h, hn = _dev_ptr(d_hits) if d_hits is not None else (None, 0)
+        r = _ranges(ranges)
+        valid = np.zeros(r.shape[0], np.uint64)
+        pos = np.zeros(r.shape[0], np.uint64)
+        _check(_lib.sbf_record_batch_counts_noalloc(self._h, p, n, _np_ptr(r), r.shape[0], h, hn,
+                                                    _stream(stream), _np_ptr(valid),
+                                                    _np_ptr(pos)))
+        return valid, pos
+
     for f in (insert_record_batch, insert_record_batch_async, query_record_batch,
-              contains_record_batch_async):
+              contains_record_batch_async, record_batch_counts_noalloc):
         setattr(Filter, f.__name__, f)
 
 

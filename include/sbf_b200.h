@@ -250,6 +250,32 @@ int sbf_contains_record_batch_async(const sbf_filter_t* filter, const char* d_se
                                     const sbf_record_range* ranges, uint64_t n, uint8_t* d_out,
                                     uint64_t out_len, sbf_stream_t stream);
 
+/* Per-record counts of a device record batch (separators already in place,
+ * as for sbf_contains_record_batch_async) without allocating anything: no
+ * reference counterpart.  valid_out[i] = valid k-mer windows of record i
+ * (valid_record_kmer_count, normalized_record_batch.hpp:88-110) and, with a
+ * non-NULL d_hits (the batch's output of sbf_contains_record_batch_async,
+ * hits_len bytes), positive_out[i] = its set hits
+ * (count_positive_kmers_per_record, detail/count_positive_kmers.cuh:21-45);
+ * positive_out[i] = 0 without d_hits.  Both outputs are host arrays of n.
+ *
+ * For callers that may not allocate device memory at call time (a serving
+ * loop or a capture-replay caller whose memory is fixed up front, an
+ * allocator hook that must not re-enter the CUDA allocator): the other
+ * record-batch entry points may grow device buffers inside the filter, this
+ * one only uses an 8 MiB scratch area compiled into the library, and calls
+ * no cudaMalloc or cudaFree.  Limit: n <= 262144 records; larger batches
+ * return SBF_ERR_INVALID_ARGUMENT.  The first call on a device looks the
+ * scratch address up (cudaGetSymbolAddress, with that device made current),
+ * so make it before any stream capture.  Calls share the scratch: calls on
+ * one device must not overlap (serialise them on one stream or host thread),
+ * or they race.  Returns after the stream has reached the end of the call. */
+int sbf_record_batch_counts_noalloc(const sbf_filter_t* filter, const char* d_seq, uint64_t len,
+                                    const sbf_record_range* ranges, uint64_t n,
+                                    const uint8_t* d_hits, uint64_t hits_len,
+                                    sbf_stream_t stream, uint64_t* valid_out,
+                                    uint64_t* positive_out);
+
 /* ---- FASTA / FASTQ (filter.cuh:402-786, Fastx.hpp:297-481) ----------- */
 
 /* Record consumer of sbf_fastx_scan: header (without '>'/'@') and sequence
