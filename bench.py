@@ -400,12 +400,16 @@ def main() -> None:
         peaks = json.load(open(peaks_path))
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    traffic = None
+    traffic = i_traffic = None
     tr_path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tr_path):
+        # DRAM bytes per unit from one ncu capture of this workload, scaled
+        # to this run's units.
         tr = json.load(open(tr_path))
         if "query_bytes_per_window" in tr:
-            traffic = tr["query_bytes_per_window"] * n_q_windows
+            traffic = int(tr["query_bytes_per_window"] * n_q_windows)
+        if "insert_bytes_per_kmer" in tr:
+            i_traffic = int(tr["insert_bytes_per_kmer"] * n_ins_valid)
     q_achieved = q_bytes / (q_ms / 1e3) / 1e9
     i_achieved = i_bytes / (ins_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "kernel": "query (tile_kernel<31,28,16,4> query, bytes)",
@@ -417,7 +421,7 @@ def main() -> None:
                          f"sector per super-k-mer run; R/N={r_per_q:.4f} counted by the oracle "
                          "on a 3 MB sample)",
                 "insert": {"achieved": round(i_achieved, 1), "frac": round(i_achieved / peak, 4),
-                           "algorithmic_bytes": int(i_bytes),
+                           "algorithmic_bytes": int(i_bytes), "traffic": i_traffic,
                            "model": f"L + 64R (R/N={r_per_i:.4f} counted on a 6 Mbp sample)"}}
 
     cpu = None
