@@ -103,6 +103,16 @@ class QueryReport(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class RaggedTuning(C.Structure):
+    """sbf_ragged_tuning: host-pipeline knobs of ragged batches (0 = default)."""
+
+    _fields_ = [("chunk_bytes", C.c_uint64), ("stages", C.c_uint32),
+                ("ctas_per_sm", C.c_uint32), ("use_graph", C.c_uint32)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class NormalizedRecord(C.Structure):
     """NormalizedRecord (include/cusbf/normalized_record_batch.hpp:20-29)."""
 
@@ -193,6 +203,15 @@ _sig("sbf_insert_record_batch_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, C
 _sig("sbf_query_record_batch", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, C.POINTER(QueryReport),
      RECORD_CB, _vp)
 _sig("sbf_contains_record_batch_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _vp)
+_sig("sbf_ragged_insert_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _vp)
+_sig("sbf_ragged_contains_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _vp, _vp)
+_sig("sbf_ragged_insert", C.c_int, _vp, _vp, _u64, _vp, _u64, C.POINTER(RaggedTuning), _vp,
+     C.POINTER(InsertReport))
+_sig("sbf_ragged_query", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, C.POINTER(RaggedTuning),
+     _vp, C.POINTER(QueryReport))
+_sig("sbf_ragged_autotune", C.c_int, _vp, C.c_int, _vp, _u64, _vp, _u64, _u64, _vp,
+     C.POINTER(RaggedTuning))
+_sig("sbf_ragged_tuning_lookup", C.c_int, _vp, C.c_int, _u64, _u64, C.POINTER(RaggedTuning))
 _sig("sbf_record_batch_counts_noalloc", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _vp,
      _vp, _vp)
 _sig("sbf_fastx_scan", C.c_int, READ_FN, _vp, C.c_char_p, SCAN_CB, _vp, C.POINTER(_u64))
@@ -534,6 +553,80 @@ def _record_methods():
 
 
 _record_methods()
+
+
+def _tuning(t):
+    if t is None:
+        return None
+    if isinstance(t, RaggedTuning):
+        return C.byref(t)
+    return C.byref(RaggedTuning(**t))
+
+
+def _ragged_methods():
+    """Ragged batches: records processed in place by one persistent launch
+    (sbf_ragged_*; no reference counterpart).  Query output has one byte per
+    window of the whole buffer; record r's hits are
+    out[offset_r : offset_r + bytes_r - k + 1]."""
+
+    def ragged_insert_async(self, d_seq, d_ranges, d_counts=None, stream=None) -> None:
+        p, n = _dev_ptr(d_seq)
+        rp, rn = _dev_ptr(d_ranges)
+        cp = _dev_ptr(d_counts)[0] if d_counts is not None else None
+        _check(_lib.sbf_ragged_insert_async(self._h, p, n, rp, rn // 16, cp, _stream(stream)))
+
+    def ragged_contains_async(self, d_seq, d_ranges, d_out, d_counts=None, stream=None) -> None:
+        p, n = _dev_ptr(d_seq)
+        rp, rn = _dev_ptr(d_ranges)
+        o, on = _dev_ptr(d_out)
+        cp = _dev_ptr(d_counts)[0] if d_counts is not None else None
+        _check(_lib.sbf_ragged_contains_async(self._h, p, n, rp, rn // 16, o, on, cp,
+                                              _stream(stream)))
+
+    def ragged_insert(self, seq, ranges, tuning=None, stream=None) -> InsertReport:
+        b = _host_bytes(seq)
+        r = _ranges(ranges)
+        rep = InsertReport()
+        _check(_lib.sbf_ragged_insert(self._h, _np_ptr(b), b.size, _np_ptr(r), r.shape[0],
+                                      _tuning(tuning), _stream(stream), C.byref(rep)))
+        return rep
+
+    def ragged_query(self, seq, ranges, out=None, tuning=None, stream=None):
+        """Returns (hits, QueryReport); `out` may be a preallocated host array
+        (pinned for the fastest copies) of at least len - k + 1 bytes."""
+        b = _host_bytes(seq)
+        r = _ranges(ranges)
+        w = self.kmer_count(b.size)
+        if out is None:
+            out = np.zeros(max(w, 1), np.uint8)
+        o = out.numpy() if hasattr(out, "numpy") else out
+        rep = QueryReport()
+        _check(_lib.sbf_ragged_query(self._h, _np_ptr(b), b.size, _np_ptr(r), r.shape[0],
+                                     _np_ptr(o), o.size, _tuning(tuning), _stream(stream),
+                                     C.byref(rep)))
+        return o[:w], rep
+
+    def ragged_autotune(self, seq, ranges, query: bool, sample_bytes: int = 0,
+                        stream=None) -> RaggedTuning:
+        b = _host_bytes(seq)
+        r = _ranges(ranges)
+        t = RaggedTuning()
+        _check(_lib.sbf_ragged_autotune(self._h, int(query), _np_ptr(b), b.size, _np_ptr(r),
+                                        r.shape[0], sample_bytes, _stream(stream), C.byref(t)))
+        return t
+
+    def ragged_tuning_lookup(self, nbytes: int, n_records: int, query: bool):
+        """The tuning-table entry for a batch shape, or None."""
+        t = RaggedTuning()
+        st = _lib.sbf_ragged_tuning_lookup(self._h, int(query), nbytes, n_records, C.byref(t))
+        return t if st == OK else None
+
+    for f in (ragged_insert_async, ragged_contains_async, ragged_insert, ragged_query,
+              ragged_autotune, ragged_tuning_lookup):
+        setattr(Filter, f.__name__, f)
+
+
+_ragged_methods()
 
 
 class _Reader:

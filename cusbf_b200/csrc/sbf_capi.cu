@@ -312,9 +312,9 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
         if (e != cudaSuccess) { rc = cuda_fail(e, "cudaGetDevice"); break; }
         e = cudaDeviceGetAttribute(&f->sms, cudaDevAttrMultiProcessorCount, f->device);
         if (e != cudaSuccess) { rc = cuda_fail(e, "cudaDeviceGetAttribute"); break; }
-        void (*fns[4])(TileParams) = {ks->insert_bytes, ks->query_bytes, ks->insert_dense,
-                                      ks->query_dense};
-        for (int i = 0; i < 4 && rc == SBF_OK; ++i) {
+        void (*fns[6])(TileParams) = {ks->insert_bytes, ks->query_bytes, ks->insert_dense,
+                                      ks->query_dense, ks->insert_ragged, ks->query_ragged};
+        for (int i = 0; i < 6 && rc == SBF_OK; ++i) {
             // Query kernels: shard slots; insert kernels: flush staging ring.
             const int dyn = (i & 1) ? kQuerySlotBytes : kInsertSlotBytes;
             if (dyn) {
@@ -368,6 +368,7 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
 
 extern "C" void sbf_filter_destroy(sbf_filter_t* f) {
     if (!f) return;
+    ragged_release(f);
     f->stage_in.release();
     f->stage_out.release();
     f->rb_dense.release();

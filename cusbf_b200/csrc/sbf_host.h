@@ -37,6 +37,8 @@ struct DevBuf {
     void release();
 };
 
+struct RaggedState;
+
 }  // namespace sbf
 
 struct sbf_filter {
@@ -48,7 +50,7 @@ struct sbf_filter {
     int* d_err = nullptr;  // [0] device error word, [8..9] popcount scratch
     int device = 0;
     int sms = 0;
-    int occupancy[4] = {1, 1, 1, 1};  // insert/query x bytes/dense
+    int occupancy[6] = {1, 1, 1, 1, 1, 1};  // insert/query x bytes/dense/ragged
     mutable uint64_t launches = 0;
 
     sbf::Staging stage_in;
@@ -56,6 +58,9 @@ struct sbf_filter {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_copied[2] = {nullptr, nullptr};
     cudaEvent_t ev_done[2] = {nullptr, nullptr};
+
+    // Ragged-batch engine state (sbf_ragged.cu), created on first use.
+    sbf::RaggedState* ragged = nullptr;
 
     // Record-batch staging (sbf_records.cu).
     sbf::DevBuf rb_dense, rb_norm, rb_meta, rb_hits, rb_stats;
@@ -72,3 +77,7 @@ struct sbf_filter {
                       uint64_t n_kmers, uint8_t* out_host, uint8_t* out_dev, cudaStream_t st);
     int check_device_error(cudaStream_t st) const;
 };
+
+namespace sbf {
+void ragged_release(sbf_filter* f);
+}  // namespace sbf

@@ -20,6 +20,13 @@ constexpr int kQuerySlotBytes = kSlots * kThreads * 32 + kOverflow * kThreads * 
 constexpr int kFlushSlots = 8;                         // insert bulk-reduce staging slots
 constexpr int kInsertSlotBytes = kFlushSlots * kThreads * 32;  // dynamic smem of inserts
 
+// A record of a ragged launch: bytes [offset, offset + bytes) of the input.
+// Same layout as sbf_record_range of the C ABI.
+struct DevRange {
+    uint64_t offset;
+    uint64_t bytes;
+};
+
 // One launch of a tile kernel.  Grid position g of tile n is
 // g = n * kTileKmers + (0 .. kTileKmers-1); it holds window (k-mer)
 // i = g + sym_base, and symbol i is the first base of that window.
@@ -33,6 +40,13 @@ struct TileParams {
     uint8_t* out;            // query: one byte per window
     uint64_t n_tiles;
     int* err;                // device error word (non-zero = failure code)
+    // Ragged launches only.  Records sorted by offset and non-overlapping; a
+    // window is processed only when its K bytes lie inside one record.
+    const DevRange* ranges;
+    uint64_t n_ranges;
+    const uint32_t* tile_rec;      // per tile: first record whose end > tile start
+    unsigned int* queue;           // work-queue counter, zero before the launch
+    unsigned long long* counts;    // [0] valid windows, [1] positive windows
 };
 
 // Device error codes written to TileParams::err.
@@ -48,6 +62,8 @@ struct KernelSet {
     void (*query_bytes)(TileParams);
     void (*insert_dense)(TileParams);
     void (*query_dense)(TileParams);
+    void (*insert_ragged)(TileParams);
+    void (*query_ragged)(TileParams);
 };
 
 // Returns the kernel table for a configuration, or nullptr when it is not
@@ -57,6 +73,10 @@ const KernelSet* find_kernels(int k, int s, int m, int h);
 // Auxiliary kernels (sbf_kernels.cu).
 cudaError_t launch_pack_dense(const uint8_t* seq, uint64_t num_symbols, uint64_t* words,
                               cudaStream_t stream);
+// Ragged launches: tile_rec[t] = first record whose end exceeds the first
+// input byte of tile t (n_ranges when none).
+cudaError_t launch_tile_records(const DevRange* ranges, uint64_t n_ranges, int64_t sym_base,
+                                uint64_t n_tiles, uint32_t* tile_rec, cudaStream_t stream);
 cudaError_t launch_popcount(const uint64_t* words, uint64_t n_words, unsigned long long* out,
                             cudaStream_t stream);
 

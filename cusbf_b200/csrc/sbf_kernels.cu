@@ -466,7 +466,7 @@ __device__ __noinline__ uint32_t query_strip_direct(const uint32_t* c, uint32_t 
 // the thread's slots (issued as the heads are found) -> s-mer hashing while
 // the copies are in flight -> wait -> findere tests -> output bytes.
 template <class C>
-__device__ __forceinline__ void query_strip(const uint32_t* c, uint32_t vmask, uint32_t shard_mask,
+__device__ __forceinline__ uint32_t query_strip(const uint32_t* c, uint32_t vmask, uint32_t shard_mask,
                                             const uint64_t* words, uint64_t* slot0,
                                             uint32_t* ovf0, uint8_t* out, int64_t first_kmer,
                                             uint64_t n_kmers) {
@@ -526,9 +526,9 @@ __device__ __forceinline__ void query_strip(const uint32_t* c, uint32_t vmask, u
     if (n > kSlots + kOverflow) {
         cp_async_wait_all();
         __syncwarp();
-        store_strip_bytes(query_strip_direct<C>(c, vmask, shard_mask, words), out, first_kmer,
-                          n_kmers);
-        return;
+        const uint32_t direct = query_strip_direct<C>(c, vmask, shard_mask, words);
+        store_strip_bytes(direct, out, first_kmer, n_kmers);
+        return direct;
     }
     // Hash the strip's s-mers while the shard copies are in flight.
     constexpr int NP = kStrip + F - 1;
@@ -594,41 +594,122 @@ __device__ __forceinline__ void query_strip(const uint32_t* c, uint32_t vmask, u
         result |= (present & 1u) << j;
     }
     store_strip_bytes(result, out, first_kmer, n_kmers);
+    return result;
 }
 
 // ---------------------------------------------------------------------------
 // The tile kernel
 // ---------------------------------------------------------------------------
 
-template <class C, bool kQuery, bool kDense>
+// Ragged launches: marks the record structure of the staged tile.  brk bit
+// r of word q is set when tile position 16q + r starts a record (windows
+// that contain it and the byte before it span two records); bytes outside
+// every record are added to the invalid bits.  Each thread takes records
+// first, first + kThreads, ... of those overlapping the tile.
+template <class C>
+__device__ __forceinline__ void mark_records(const TileParams& p, int64_t s0, uint32_t first,
+                                             uint32_t* inval, uint32_t* brk) {
+    constexpr int64_t kSpan = kCodeWords * 16;
+    const int64_t len = static_cast<int64_t>(p.input_bytes);
+    const int64_t t_end = s0 + kSpan;
+    auto set_bits = [&](uint32_t* arr, int64_t a, int64_t b) {  // dense [a, b)
+        a = a > s0 ? a : s0;
+        b = b < t_end ? b : t_end;
+        for (int64_t x = a; x < b;) {
+            const int64_t pos = x - s0;
+            const int q = static_cast<int>(pos >> 4), r = static_cast<int>(pos & 15);
+            const int64_t n = (16 - r) < (b - x) ? (16 - r) : (b - x);
+            atomicOr(arr + q, ((1u << n) - 1u) << r);
+            x += n;
+        }
+    };
+    const uint64_t n = p.n_ranges;
+    if (threadIdx.x == 0) {
+        // Bytes before the first overlapping record.
+        const int64_t gap0 = first == 0 ? 0
+                                        : static_cast<int64_t>(p.ranges[first - 1].offset +
+                                                               p.ranges[first - 1].bytes);
+        const int64_t until = first < n ? static_cast<int64_t>(p.ranges[first].offset) : len;
+        set_bits(inval, gap0, until);
+    }
+    for (uint64_t r = first + threadIdx.x; r < n; r += kThreads) {
+        const DevRange rec = p.ranges[r];
+        const int64_t a = static_cast<int64_t>(rec.offset);
+        if (a >= t_end) break;
+        const int64_t b = a + static_cast<int64_t>(rec.bytes);
+        if (a > s0 && a < t_end) {
+            const int64_t pos = a - s0;
+            atomicOr(brk + (pos >> 4), 1u << (pos & 15));
+        }
+        const int64_t next = r + 1 < n ? static_cast<int64_t>(p.ranges[r + 1].offset) : len;
+        if (next > b) set_bits(inval, b, next);
+    }
+}
+
+// Ragged launches: clears windows j of the strip that contain a record start
+// other than their own first byte.
+template <class C>
+__device__ __forceinline__ uint32_t strip_in_record(const uint32_t* bk, uint32_t vmask) {
+    const uint64_t bits = static_cast<uint64_t>(bk[0]) | (static_cast<uint64_t>(bk[1]) << 16) |
+                          (static_cast<uint64_t>(bk[2]) << 32) |
+                          (static_cast<uint64_t>(bk[3]) << 48);
+    constexpr uint64_t kInner = ((uint64_t{1} << C::K) - 1) >> 1;  // positions j+1 .. j+K-1
+    if (bits) {
+#pragma unroll
+        for (int j = 0; j < kStrip; ++j)
+            if ((bits >> (j + 1)) & kInner) vmask &= ~(1u << j);
+    }
+    return vmask;
+}
+
+// Persistent tile kernel.  Plain launches walk tiles blockIdx.x + i * gridDim.x;
+// ragged launches take tiles from the device work-queue counter p.queue, so
+// tiles of uneven cost (records of any length, N runs) balance across CTAs.
+// Either way tile i+2 is known while tile i is processed, so its staging copy
+// is issued two tiles ahead.
+template <class C, bool kQuery, bool kDense, bool kRagged>
 __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
     __shared__ alignas(128) uint8_t stage[2][kStageBytes];
     __shared__ uint32_t code[kCodeWords + 4];
     __shared__ uint32_t inval[kCodeWords + 4];
+    __shared__ uint32_t brk[kRagged ? kCodeWords + 4 : 1];
+    __shared__ uint64_t tiles[3];
+    __shared__ uint32_t first_rec[3];
+    __shared__ unsigned long long tally[2];
     __shared__ alignas(8) uint64_t bars[2];
 
     const int tid = threadIdx.x;
+    auto take = [&](uint32_t i, int slot) {
+        uint64_t t;
+        if constexpr (kRagged) {
+            t = atomicAdd(p.queue, 1u);
+            first_rec[slot] = t < p.n_tiles ? p.tile_rec[t] : 0u;
+        } else {
+            t = blockIdx.x + static_cast<uint64_t>(i) * gridDim.x;
+        }
+        tiles[slot] = t;
+        return t;
+    };
     if (tid == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         mbar_fence_init();
+        tally[0] = tally[1] = 0;
+        const uint64_t t0 = take(0, 0), t1 = take(1, 1);
+        if (t0 < p.n_tiles) issue_stage<kDense>(p, t0, stage[0], &bars[0]);
+        if (t1 < p.n_tiles) issue_stage<kDense>(p, t1, stage[1], &bars[1]);
     }
     __syncthreads();
-
-    const uint64_t stride = gridDim.x;
-    uint64_t tile = blockIdx.x;
-    if (tid == 0) {
-        if (tile < p.n_tiles) issue_stage<kDense>(p, tile, stage[0], &bars[0]);
-        if (tile + stride < p.n_tiles) issue_stage<kDense>(p, tile + stride, stage[1], &bars[1]);
-    }
     // Dynamic shared memory, [slot][thread] layout: the query kernel's shard
     // slots (kQuerySlotBytes per CTA) or the insert kernel's flush staging
     // ring (kInsertSlotBytes per CTA).
     extern __shared__ __align__(16) uint64_t slots[];
     FlushRing ring{slots + 4 * tid, 0u};
     (void)ring;
-    uint32_t it = 0;
-    for (; tile < p.n_tiles; tile += stride, ++it) {
+    unsigned long long n_valid = 0, n_pos = 0;
+    for (uint32_t it = 0;; ++it) {
+        const uint64_t tile = tiles[it % 3];
+        if (tile >= p.n_tiles) break;
         const int b = it & 1;
         const uint32_t parity = (it >> 1) & 1u;
         const bool ok = mbar_wait_bounded(&bars[b], parity);
@@ -636,7 +717,8 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
             if (tid == 0) atomicExch(p.err, kDevErrStageTimeout);
             // Give the other buffer's copy (if any) a bounded chance to land
             // before the CTA's shared memory is released.
-            if (tile + stride < p.n_tiles) (void)mbar_wait_bounded(&bars[b ^ 1], parity);
+            if (tiles[(it + 1) % 3] < p.n_tiles)
+                (void)mbar_wait_bounded(&bars[b ^ 1], ((it + 1) >> 1) & 1u);
             if constexpr (!kQuery) flush_ring_drain();
             return;
         }
@@ -648,10 +730,17 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
             encode_word<kDense>(g, stage[b], q, cw, iv);
             code[q] = cw;
             inval[q] = iv;
+            if constexpr (kRagged) brk[q] = 0u;
+        }
+        if constexpr (kRagged) {
+            __syncthreads();
+            mark_records<C>(p, g.s0, first_rec[it % 3], inval, brk);
         }
         __syncthreads();
-        if (tid == 0 && tile + 2 * stride < p.n_tiles)
-            issue_stage<kDense>(p, tile + 2 * stride, stage[b], &bars[b]);
+        if (tid == 0) {
+            const uint64_t t2 = take(it + 2, (it + 2) % 3);
+            if (t2 < p.n_tiles) issue_stage<kDense>(p, t2, stage[b], &bars[b]);
+        }
 
         uint32_t c[kStripWords], iv[kStripWords];
 #pragma unroll
@@ -660,16 +749,59 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
             iv[q] = inval[tid * (kStrip / 16) + q];
         }
         const int64_t first_kmer = g.s0 + static_cast<int64_t>(tid) * kStrip;
-        const uint32_t vmask = strip_valid<C>(iv, first_kmer, p.n_kmers);
+        uint32_t vmask = strip_valid<C>(iv, first_kmer, p.n_kmers);
+        if constexpr (kRagged) {
+            uint32_t bk[kStripWords];
+#pragma unroll
+            for (int q = 0; q < kStripWords; ++q) bk[q] = brk[tid * (kStrip / 16) + q];
+            vmask = strip_in_record<C>(bk, vmask);
+            n_valid += __popc(vmask);
+        }
         if constexpr (kQuery) {
-            query_strip<C>(c, vmask, p.shard_mask, p.words, slots + 4 * tid,
-                           reinterpret_cast<uint32_t*>(slots + kSlots * kThreads * 4) + tid, p.out,
-                           first_kmer, p.n_kmers);
+            const uint32_t hits =
+                query_strip<C>(c, vmask, p.shard_mask, p.words, slots + 4 * tid,
+                               reinterpret_cast<uint32_t*>(slots + kSlots * kThreads * 4) + tid,
+                               p.out, first_kmer, p.n_kmers);
+            if constexpr (kRagged) n_pos += __popc(hits & vmask);
         } else {
             if (vmask) insert_strip<C>(c, vmask, p.shard_mask, p.words, ring);
         }
     }
     if constexpr (!kQuery) flush_ring_drain();
+    if constexpr (kRagged) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            n_valid += __shfl_down_sync(0xFFFFFFFFu, n_valid, o);
+            n_pos += __shfl_down_sync(0xFFFFFFFFu, n_pos, o);
+        }
+        if ((tid & 31) == 0) {
+            atomicAdd(&tally[0], n_valid);
+            atomicAdd(&tally[1], n_pos);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            atomicAdd(p.counts, tally[0]);
+            atomicAdd(p.counts + 1, tally[1]);
+        }
+    }
+}
+
+// tile_rec[t] = first record whose end exceeds the first byte tile t stages
+// (binary search; records sorted and non-overlapping).
+__global__ void tile_records_kernel(const DevRange* ranges, uint64_t n, int64_t sym_base,
+                                    uint64_t n_tiles, uint32_t* tile_rec) {
+    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n_tiles) return;
+    const int64_t s0 = static_cast<int64_t>(t) * kTileKmers + sym_base;
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (static_cast<int64_t>(ranges[mid].offset + ranges[mid].bytes) > s0)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    tile_rec[t] = static_cast<uint32_t>(lo);
 }
 
 // ---------------------------------------------------------------------------
@@ -715,6 +847,16 @@ cudaError_t launch_pack_dense(const uint8_t* seq, uint64_t num_symbols, uint64_t
     return cudaGetLastError();
 }
 
+const void* tile_records_kernel_ptr() { return reinterpret_cast<const void*>(&tile_records_kernel); }
+
+cudaError_t launch_tile_records(const DevRange* ranges, uint64_t n_ranges, int64_t sym_base,
+                                uint64_t n_tiles, uint32_t* tile_rec, cudaStream_t stream) {
+    if (n_tiles == 0) return cudaSuccess;
+    tile_records_kernel<<<static_cast<unsigned>((n_tiles + 255) / 256), 256, 0, stream>>>(
+        ranges, n_ranges, sym_base, n_tiles, tile_rec);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_popcount(const uint64_t* words, uint64_t n_words, unsigned long long* out,
                             cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned long long), stream);
@@ -737,10 +879,12 @@ constexpr KernelSet make_set() {
                      S,
                      M,
                      H,
-                     &tile_kernel<C, false, false>,
-                     &tile_kernel<C, true, false>,
-                     &tile_kernel<C, false, true>,
-                     &tile_kernel<C, true, true>};
+                     &tile_kernel<C, false, false, false>,
+                     &tile_kernel<C, true, false, false>,
+                     &tile_kernel<C, false, true, false>,
+                     &tile_kernel<C, true, true, false>,
+                     &tile_kernel<C, false, false, true>,
+                     &tile_kernel<C, true, false, true>};
 }
 
 static const KernelSet kSets[] = {

@@ -1,0 +1,611 @@
+// sbf_ragged.cu -- ragged batches: many records of uneven length through one
+// persistent tile-kernel launch with a device work queue, a multi-stage host
+// pipeline whose per-chunk device work can be replayed as a CUDA graph, and
+// an autotuner with a persisted table.  No reference counterpart: the
+// reference inserts a record batch by normalising it on the host (records
+// joined with one 'N', include/cusbf/normalized_record_batch.hpp:235-276)
+// and launching the plain kernel over the copy, or one launch per record
+// (filter.cuh:179, :464).
+//
+// Records stay where they are.  The kernel marks, per staged tile, the
+// first byte of every record and the bytes outside every record, and a
+// window is valid only when its K bytes lie inside one record: exactly the
+// windows of the reference's per-record insert/query.  Query output uses
+// the batch's own layout: the hit of the window that starts at byte p of
+// the batch is out[p], so record r's hits are out[offset_r, offset_r +
+// bytes_r - K + 1) and windows that cross records read 0.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <sys/stat.h>
+#include <string>
+#include <vector>
+
+#include "../../include/sbf_b200.h"
+#include "sbf_host.h"
+#include "sbf_internal.h"
+
+using namespace sbf;
+
+#define SBF_CUDA(expr)                                      \
+    do {                                                    \
+        cudaError_t _e = (expr);                            \
+        if (_e != cudaSuccess) return cuda_fail(_e, #expr); \
+    } while (0)
+#define SBF_TRY(expr)                \
+    do {                             \
+        int _s = (expr);             \
+        if (_s != SBF_OK) return _s; \
+    } while (0)
+
+static_assert(sizeof(DevRange) == sizeof(sbf_record_range), "record layout");
+
+namespace sbf {
+
+int validate_ranges(uint64_t len, const sbf_record_range* r, uint64_t n);
+const void* tile_records_kernel_ptr();
+
+constexpr int kMaxStages = 4;
+
+// One stage of the host pipeline: pinned and device buffers of one chunk.
+struct RaggedSlot {
+    uint8_t* pin_seq = nullptr;
+    size_t pin_seq_cap = 0;
+    DevRange* pin_rng = nullptr;
+    size_t pin_rng_cap = 0;
+    uint8_t* d_seq = nullptr;
+    size_t d_seq_cap = 0;
+    DevRange* d_rng = nullptr;
+    size_t d_rng_cap = 0;
+    uint32_t* d_tile_rec = nullptr;
+    size_t tile_cap = 0;
+    uint8_t* d_out = nullptr;
+    size_t out_cap = 0;
+    cudaEvent_t ev_copied = nullptr, ev_done = nullptr;
+    bool busy = false;
+    // Device work of one chunk as a graph: tile records -> queue reset ->
+    // tile kernel.  Built on first use per (slot, operation).
+    cudaGraph_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    cudaGraphNode_t n_rec[2] = {}, n_tile[2] = {};
+};
+
+struct RaggedState {
+    RaggedSlot slot[kMaxStages];
+    cudaStream_t copy_stream = nullptr;
+    // [0] work-queue counter; [2..3] (as u64) batch counts.
+    unsigned int* d_ctl = nullptr;
+    DevBuf direct_tile_rec;
+};
+
+template <class T>
+static int grow_device(T*& p, size_t& cap, size_t bytes) {
+    if (bytes <= cap) return SBF_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = std::max<size_t>(bytes, 4096);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(SBF_ERR_RESOURCE, "cannot allocate %zu bytes of ragged staging", want);
+    }
+    cap = want;
+    return SBF_OK;
+}
+
+template <class T>
+static int grow_pinned(T*& p, size_t& cap, size_t bytes) {
+    if (bytes <= cap) return SBF_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = std::max<size_t>(bytes, 4096);
+    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&p), want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(SBF_ERR_RESOURCE, "cannot allocate %zu bytes of pinned staging", want);
+    }
+    cap = want;
+    return SBF_OK;
+}
+
+static void release_slot(RaggedSlot& s) {
+    if (s.pin_seq) cudaFreeHost(s.pin_seq);
+    if (s.pin_rng) cudaFreeHost(s.pin_rng);
+    if (s.d_seq) cudaFree(s.d_seq);
+    if (s.d_rng) cudaFree(s.d_rng);
+    if (s.d_tile_rec) cudaFree(s.d_tile_rec);
+    if (s.d_out) cudaFree(s.d_out);
+    if (s.ev_copied) cudaEventDestroy(s.ev_copied);
+    if (s.ev_done) cudaEventDestroy(s.ev_done);
+    for (int i = 0; i < 2; ++i) {
+        if (s.exec[i]) cudaGraphExecDestroy(s.exec[i]);
+        if (s.graph[i]) cudaGraphDestroy(s.graph[i]);
+    }
+    s = RaggedSlot{};
+}
+
+void ragged_release(sbf_filter* f) {
+    if (!f->ragged) return;
+    RaggedState* r = f->ragged;
+    for (auto& s : r->slot) release_slot(s);
+    if (r->copy_stream) cudaStreamDestroy(r->copy_stream);
+    if (r->d_ctl) cudaFree(r->d_ctl);
+    r->direct_tile_rec.release();
+    delete r;
+    f->ragged = nullptr;
+}
+
+static int ragged_state(sbf_filter* f, RaggedState** out) {
+    if (!f->ragged) {
+        auto* r = new RaggedState();
+        f->ragged = r;
+        cudaError_t e = cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+        if ((e = cudaMalloc(&r->d_ctl, 64)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(ctl)");
+        if ((e = cudaMemset(r->d_ctl, 0, 64)) != cudaSuccess) return cuda_fail(e, "cudaMemset(ctl)");
+        for (auto& s : r->slot) {
+            if ((e = cudaEventCreateWithFlags(&s.ev_copied, cudaEventDisableTiming)) != cudaSuccess)
+                return cuda_fail(e, "cudaEventCreate");
+            if ((e = cudaEventCreateWithFlags(&s.ev_done, cudaEventDisableTiming)) != cudaSuccess)
+                return cuda_fail(e, "cudaEventCreate");
+        }
+    }
+    *out = f->ragged;
+    return SBF_OK;
+}
+
+static unsigned long long* ctl_counts(RaggedState* r) {
+    return reinterpret_cast<unsigned long long*>(r->d_ctl + 2);
+}
+
+// Kernel parameters of one ragged launch over `len` bytes at d_seq.
+static TileParams ragged_params(const sbf_filter* f, bool query, const uint8_t* d_seq,
+                                uint64_t len, const DevRange* d_rng, uint64_t n,
+                                const uint32_t* d_tile_rec, uint8_t* d_out, unsigned int* queue,
+                                unsigned long long* counts) {
+    TileParams p{};
+    p.input = d_seq;
+    p.input_bytes = len;
+    p.n_kmers = f->kmers_of(len);
+    int64_t phase = 0;
+    if (query)
+        phase = static_cast<int64_t>(reinterpret_cast<uintptr_t>(d_out) & 15u);
+    else
+        phase = static_cast<int64_t>(reinterpret_cast<uintptr_t>(d_seq) & 15u);
+    p.sym_base = -phase;
+    p.words = f->d_words;
+    p.shard_mask = static_cast<uint32_t>(f->num_shards - 1);
+    p.out = d_out;
+    p.n_tiles = (p.n_kmers + static_cast<uint64_t>(phase) + kTileKmers - 1) / kTileKmers;
+    p.err = f->d_err;
+    p.ranges = d_rng;
+    p.n_ranges = n;
+    p.tile_rec = d_tile_rec;
+    p.queue = queue;
+    p.counts = counts;
+    return p;
+}
+
+static unsigned ragged_grid(const sbf_filter* f, bool query, uint64_t n_tiles, uint32_t ctas) {
+    const int occ = f->occupancy[query ? 5 : 4];
+    const uint64_t per_sm = ctas == 0 ? static_cast<uint64_t>(occ)
+                                      : std::min<uint64_t>(ctas, static_cast<uint64_t>(occ));
+    const uint64_t resident = static_cast<uint64_t>(f->sms) * std::max<uint64_t>(per_sm, 1);
+    return static_cast<unsigned>(std::max<uint64_t>(std::min<uint64_t>(n_tiles, resident), 1));
+}
+
+// Stream launch of one ragged pass: tile records, queue reset, tile kernel.
+static int ragged_launch(sbf_filter* f, bool query, const TileParams& p, uint32_t ctas,
+                         cudaStream_t st) {
+    if (p.n_tiles == 0) return SBF_OK;
+    SBF_CUDA(launch_tile_records(p.ranges, p.n_ranges, p.sym_base, p.n_tiles,
+                                 const_cast<uint32_t*>(p.tile_rec), st));
+    SBF_CUDA(cudaMemsetAsync(p.queue, 0, sizeof(unsigned int), st));
+    void (*fn)(TileParams) = query ? f->ks->query_ragged : f->ks->insert_ragged;
+    fn<<<ragged_grid(f, query, p.n_tiles, ctas), kThreads,
+         query ? kQuerySlotBytes : kInsertSlotBytes, st>>>(p);
+    SBF_CUDA(cudaGetLastError());
+    f->launches += 2;
+    return SBF_OK;
+}
+
+// The same pass as a graph launch.  The graph of a slot is built once per
+// operation; later chunks only update the two kernel nodes' parameters.
+static int ragged_graph_launch(sbf_filter* f, RaggedSlot& s, bool query, const TileParams& p,
+                               uint32_t ctas, cudaStream_t st) {
+    if (p.n_tiles == 0) return SBF_OK;
+    const int op = query ? 1 : 0;
+    const DevRange* a_rng = p.ranges;
+    uint64_t a_n = p.n_ranges;
+    int64_t a_base = p.sym_base;
+    uint64_t a_tiles = p.n_tiles;
+    uint32_t* a_rec = const_cast<uint32_t*>(p.tile_rec);
+    void* rec_args[] = {&a_rng, &a_n, &a_base, &a_tiles, &a_rec};
+    TileParams tp = p;
+    void* tile_args[] = {&tp};
+    cudaKernelNodeParams rk{};
+    rk.func = const_cast<void*>(tile_records_kernel_ptr());
+    rk.gridDim = dim3(static_cast<unsigned>((p.n_tiles + 255) / 256));
+    rk.blockDim = dim3(256);
+    rk.kernelParams = rec_args;
+    cudaKernelNodeParams tk{};
+    tk.func = reinterpret_cast<void*>(query ? f->ks->query_ragged : f->ks->insert_ragged);
+    tk.gridDim = dim3(ragged_grid(f, query, p.n_tiles, ctas));
+    tk.blockDim = dim3(kThreads);
+    tk.sharedMemBytes = query ? kQuerySlotBytes : kInsertSlotBytes;
+    tk.kernelParams = tile_args;
+    if (!s.exec[op]) {
+        SBF_CUDA(cudaGraphCreate(&s.graph[op], 0));
+        SBF_CUDA(cudaGraphAddKernelNode(&s.n_rec[op], s.graph[op], nullptr, 0, &rk));
+        cudaMemsetParams ms{};
+        ms.dst = p.queue;
+        ms.value = 0;
+        ms.elementSize = sizeof(unsigned int);
+        ms.width = 1;
+        ms.height = 1;
+        cudaGraphNode_t n_ms;
+        SBF_CUDA(cudaGraphAddMemsetNode(&n_ms, s.graph[op], &s.n_rec[op], 1, &ms));
+        SBF_CUDA(cudaGraphAddKernelNode(&s.n_tile[op], s.graph[op], &n_ms, 1, &tk));
+        SBF_CUDA(cudaGraphInstantiate(&s.exec[op], s.graph[op], 0));
+    } else {
+        SBF_CUDA(cudaGraphExecKernelNodeSetParams(s.exec[op], s.n_rec[op], &rk));
+        SBF_CUDA(cudaGraphExecKernelNodeSetParams(s.exec[op], s.n_tile[op], &tk));
+    }
+    SBF_CUDA(cudaGraphLaunch(s.exec[op], st));
+    f->launches += 2;
+    return SBF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Tuning table
+// ---------------------------------------------------------------------------
+
+struct TuneKey {
+    int op, k, s, m, h, len_bucket, rec_bucket;
+};
+
+static int log2_bucket(double v) { return v < 1 ? 0 : static_cast<int>(std::floor(std::log2(v))); }
+
+static TuneKey tune_key(const sbf_filter* f, bool query, uint64_t len, uint64_t n) {
+    return TuneKey{query ? 1 : 0,
+                   static_cast<int>(f->k),
+                   static_cast<int>(f->s),
+                   static_cast<int>(f->m),
+                   static_cast<int>(f->h),
+                   log2_bucket(static_cast<double>(len)),
+                   log2_bucket(n ? static_cast<double>(len) / static_cast<double>(n) : 0.0)};
+}
+
+static std::string tune_table_path() {
+    if (const char* p = std::getenv("SBF_TUNE_TABLE")) return p;
+    const char* home = std::getenv("HOME");
+    return std::string(home ? home : "/tmp") + "/.cache/cusbf_b200/ragged_tuning.tsv";
+}
+
+static std::mutex g_tune_mutex;
+
+static bool tune_lookup(const TuneKey& key, sbf_ragged_tuning* out) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    FILE* fp = std::fopen(tune_table_path().c_str(), "r");
+    if (!fp) return false;
+    char line[256];
+    bool found = false;
+    while (std::fgets(line, sizeof line, fp)) {
+        TuneKey k{};
+        unsigned long long chunk = 0;
+        unsigned stages = 0, ctas = 0, graph = 0;
+        if (std::sscanf(line, "%d %d %d %d %d %d %d %llu %u %u %u", &k.op, &k.k, &k.s, &k.m, &k.h,
+                        &k.len_bucket, &k.rec_bucket, &chunk, &stages, &ctas, &graph) != 11)
+            continue;
+        if (std::memcmp(&k, &key, sizeof k) == 0) {  // the last matching line wins
+            out->chunk_bytes = chunk;
+            out->stages = stages;
+            out->ctas_per_sm = ctas;
+            out->use_graph = graph;
+            found = true;
+        }
+    }
+    std::fclose(fp);
+    return found;
+}
+
+static void tune_store(const TuneKey& key, const sbf_ragged_tuning& t, double ms) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    const std::string path = tune_table_path();
+    // Create the table's directory chain; existing directories are kept.
+    for (size_t i = 1; i < path.size(); ++i)
+        if (path[i] == '/') (void)mkdir(path.substr(0, i).c_str(), 0755);
+    FILE* fp = std::fopen(path.c_str(), "a");
+    if (!fp) return;
+    std::fprintf(fp, "%d %d %d %d %d %d %d %llu %u %u %u %.4f\n", key.op, key.k, key.s, key.m,
+                 key.h, key.len_bucket, key.rec_bucket,
+                 static_cast<unsigned long long>(t.chunk_bytes), t.stages, t.ctas_per_sm,
+                 t.use_graph, ms);
+    std::fclose(fp);
+}
+
+static sbf_ragged_tuning default_tuning() {
+    sbf_ragged_tuning t{};
+    t.chunk_bytes = uint64_t{64} << 20;
+    t.stages = 2;
+    t.ctas_per_sm = 0;
+    t.use_graph = 0;
+    return t;
+}
+
+static int check_tuning(sbf_ragged_tuning& t) {
+    if (t.chunk_bytes == 0) t.chunk_bytes = default_tuning().chunk_bytes;
+    if (t.chunk_bytes < 4096)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "ragged chunk_bytes must be at least 4096");
+    if (t.stages == 0) t.stages = 2;
+    if (t.stages < 1 || t.stages > kMaxStages)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "ragged stages must be 1..%d", kMaxStages);
+    return SBF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Host pipeline
+// ---------------------------------------------------------------------------
+
+// Windows [0, W) of the batch are cut into chunks of `cw` windows; chunk c
+// stages bytes [c*cw, c*cw + cw + K - 1) and the records clipped to them
+// (pieces shorter than K hold no window and are dropped: their bytes read as
+// outside every record, which invalidates exactly the windows that cross).
+static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_t len,
+                           const sbf_record_range* ranges, uint64_t n, sbf_ragged_tuning t,
+                           cudaStream_t st, uint8_t* h_out, unsigned long long counts[2]) {
+    counts[0] = counts[1] = 0;
+    const uint64_t K = f->k;
+    const uint64_t W = f->kmers_of(len);
+    if (W == 0 || n == 0) {
+        if (query && W) std::memset(h_out, 0, W);
+        return SBF_OK;
+    }
+    RaggedState* r = nullptr;
+    SBF_TRY(ragged_state(f, &r));
+    SBF_TRY(check_tuning(t));
+    const uint64_t cw = std::max<uint64_t>(t.chunk_bytes > K ? t.chunk_bytes - (K - 1) : 1, 1024);
+    const uint64_t n_chunks = (W + cw - 1) / cw;
+    const uint64_t max_bytes = cw + K - 1;
+    const uint64_t max_pieces = max_bytes / K + 2;
+    const bool pinned_in = is_pinned(h_seq);
+    unsigned long long* d_counts = ctl_counts(r);
+    SBF_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(unsigned long long), st));
+    const uint32_t S = t.stages;
+    for (uint32_t i = 0; i < S; ++i) {
+        RaggedSlot& s = r->slot[i];
+        if (!pinned_in) SBF_TRY(grow_pinned(s.pin_seq, s.pin_seq_cap, max_bytes + 16));
+        SBF_TRY(grow_pinned(s.pin_rng, s.pin_rng_cap, max_pieces * sizeof(DevRange)));
+        SBF_TRY(grow_device(s.d_seq, s.d_seq_cap, max_bytes + 16));
+        SBF_TRY(grow_device(s.d_rng, s.d_rng_cap, max_pieces * sizeof(DevRange)));
+        SBF_TRY(grow_device(s.d_tile_rec, s.tile_cap, ((cw + 16) / kTileKmers + 2) * 4));
+        if (query) SBF_TRY(grow_device(s.d_out, s.out_cap, cw + 16));
+        s.busy = false;
+    }
+    // The copy stream starts after work already queued on `st`.
+    cudaEvent_t ev_start = r->slot[0].ev_done;
+    SBF_CUDA(cudaEventRecord(ev_start, st));
+    SBF_CUDA(cudaStreamWaitEvent(r->copy_stream, ev_start, 0));
+    uint64_t rec = 0;  // first record whose end exceeds the chunk's first byte
+    for (uint64_t c = 0; c < n_chunks; ++c) {
+        RaggedSlot& s = r->slot[c % S];
+        if (s.busy) SBF_CUDA(cudaEventSynchronize(s.ev_done));
+        const uint64_t w_lo = c * cw;
+        const uint64_t w_hi = std::min<uint64_t>(W, w_lo + cw);
+        const uint64_t b_lo = w_lo, b_hi = w_hi + K - 1;
+        while (rec < n && ranges[rec].sequence_offset + ranges[rec].sequence_bytes <= b_lo) ++rec;
+        uint64_t np = 0;
+        for (uint64_t j = rec; j < n && ranges[j].sequence_offset < b_hi; ++j) {
+            const uint64_t a = std::max<uint64_t>(ranges[j].sequence_offset, b_lo);
+            const uint64_t e =
+                std::min<uint64_t>(ranges[j].sequence_offset + ranges[j].sequence_bytes, b_hi);
+            if (e >= a + K) s.pin_rng[np++] = DevRange{a - b_lo, e - a};
+        }
+        const uint8_t* src = reinterpret_cast<const uint8_t*>(h_seq) + b_lo;
+        if (!pinned_in) {
+            std::memcpy(s.pin_seq, src, b_hi - b_lo);
+            src = s.pin_seq;
+        }
+        SBF_CUDA(cudaMemcpyAsync(s.d_seq, src, b_hi - b_lo, cudaMemcpyHostToDevice,
+                                 r->copy_stream));
+        if (np)
+            SBF_CUDA(cudaMemcpyAsync(s.d_rng, s.pin_rng, np * sizeof(DevRange),
+                                     cudaMemcpyHostToDevice, r->copy_stream));
+        SBF_CUDA(cudaEventRecord(s.ev_copied, r->copy_stream));
+        SBF_CUDA(cudaStreamWaitEvent(st, s.ev_copied, 0));
+        if (np) {
+            const TileParams p = ragged_params(f, query, s.d_seq, b_hi - b_lo, s.d_rng, np,
+                                               s.d_tile_rec, s.d_out, r->d_ctl, d_counts);
+            if (t.use_graph)
+                SBF_TRY(ragged_graph_launch(f, s, query, p, t.ctas_per_sm, st));
+            else
+                SBF_TRY(ragged_launch(f, query, p, t.ctas_per_sm, st));
+        } else if (query) {
+            SBF_CUDA(cudaMemsetAsync(s.d_out, 0, w_hi - w_lo, st));
+        }
+        if (query)
+            SBF_CUDA(cudaMemcpyAsync(h_out + w_lo, s.d_out, w_hi - w_lo, cudaMemcpyDeviceToHost, st));
+        // The host waits for ev_done before it refills this slot, so the
+        // copy stream itself never waits on kernels.
+        SBF_CUDA(cudaEventRecord(s.ev_done, st));
+        s.busy = true;
+    }
+    unsigned long long h_counts[2] = {0, 0};
+    SBF_CUDA(cudaMemcpyAsync(h_counts, d_counts, sizeof h_counts, cudaMemcpyDeviceToHost, st));
+    SBF_CUDA(cudaStreamSynchronize(st));
+    for (uint32_t i = 0; i < S; ++i) r->slot[i].busy = false;
+    SBF_TRY(f->check_device_error(st));
+    counts[0] = h_counts[0];
+    counts[1] = h_counts[1];
+    return SBF_OK;
+}
+
+static int resolve_tuning(const sbf_filter* f, bool query, uint64_t len, uint64_t n,
+                          const sbf_ragged_tuning* given, sbf_ragged_tuning* out) {
+    if (given) {
+        *out = *given;
+    } else if (!tune_lookup(tune_key(f, query, len, n), out)) {
+        *out = default_tuning();
+    }
+    return check_tuning(*out);
+}
+
+}  // namespace sbf
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+static inline cudaStream_t S_(sbf_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+static int ragged_async(sbf_filter_t* f, bool query, const char* d_seq, uint64_t len,
+                        const sbf_record_range* d_ranges, uint64_t n, uint8_t* d_out,
+                        uint64_t out_len, uint64_t* d_counts, sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (n && !d_ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "ranges pointer is null");
+    if (n > 0xFFFFFFFFull) return set_error(SBF_ERR_INVALID_ARGUMENT, "too many records");
+    const uint64_t W = f->kmers_of(len);
+    if (W == 0) return SBF_OK;
+    if (!d_seq) return set_error(SBF_ERR_INVALID_ARGUMENT, "sequence pointer is null");
+    if (query && (!d_out || out_len < W))
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "ragged query output span is too small");
+    RaggedState* r = nullptr;
+    SBF_TRY(ragged_state(f, &r));
+    cudaStream_t st = S_(stream);
+    if (n == 0) {
+        if (query) SBF_CUDA(cudaMemsetAsync(d_out, 0, W, st));
+        return SBF_OK;
+    }
+    TileParams p = ragged_params(f, query, reinterpret_cast<const uint8_t*>(d_seq), len,
+                                 reinterpret_cast<const DevRange*>(d_ranges), n, nullptr, d_out,
+                                 r->d_ctl,
+                                 d_counts ? reinterpret_cast<unsigned long long*>(d_counts)
+                                          : ctl_counts(r));
+    SBF_TRY(r->direct_tile_rec.ensure(p.n_tiles * 4 + 64));
+    p.tile_rec = static_cast<const uint32_t*>(r->direct_tile_rec.ptr);
+    return ragged_launch(f, query, p, 0, st);
+}
+
+extern "C" int sbf_ragged_insert_async(sbf_filter_t* f, const char* d_seq, uint64_t len,
+                                       const sbf_record_range* d_ranges, uint64_t n,
+                                       uint64_t* d_counts, sbf_stream_t stream) {
+    return ragged_async(f, false, d_seq, len, d_ranges, n, nullptr, 0, d_counts, stream);
+}
+
+extern "C" int sbf_ragged_contains_async(const sbf_filter_t* f, const char* d_seq, uint64_t len,
+                                         const sbf_record_range* d_ranges, uint64_t n,
+                                         uint8_t* d_out, uint64_t out_len, uint64_t* d_counts,
+                                         sbf_stream_t stream) {
+    return ragged_async(const_cast<sbf_filter*>(f), true, d_seq, len, d_ranges, n, d_out, out_len,
+                        d_counts, stream);
+}
+
+extern "C" int sbf_ragged_insert(sbf_filter_t* f, const char* h_seq, uint64_t len,
+                                 const sbf_record_range* ranges, uint64_t n,
+                                 const sbf_ragged_tuning* tuning, sbf_stream_t stream,
+                                 sbf_insert_report* report) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    SBF_TRY(validate_ranges(len, ranges, n));
+    sbf_ragged_tuning t{};
+    SBF_TRY(resolve_tuning(f, false, len, n, tuning, &t));
+    unsigned long long counts[2];
+    SBF_TRY(ragged_pipeline(f, false, h_seq, len, ranges, n, t, S_(stream), nullptr, counts));
+    if (report) {
+        report->records_indexed = n;
+        report->indexed_bases = 0;
+        for (uint64_t i = 0; i < n; ++i) report->indexed_bases += ranges[i].sequence_bytes;
+        report->inserted_kmers = counts[0];
+    }
+    return SBF_OK;
+}
+
+extern "C" int sbf_ragged_query(const sbf_filter_t* cf, const char* h_seq, uint64_t len,
+                                const sbf_record_range* ranges, uint64_t n, uint8_t* h_out,
+                                uint64_t out_len, const sbf_ragged_tuning* tuning,
+                                sbf_stream_t stream, sbf_query_report* report) {
+    auto* f = const_cast<sbf_filter*>(cf);
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    SBF_TRY(validate_ranges(len, ranges, n));
+    const uint64_t W = f->kmers_of(len);
+    if (W && (!h_out || out_len < W))
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "ragged query output span is too small");
+    sbf_ragged_tuning t{};
+    SBF_TRY(resolve_tuning(f, true, len, n, tuning, &t));
+    unsigned long long counts[2];
+    SBF_TRY(ragged_pipeline(f, true, h_seq, len, ranges, n, t, S_(stream), h_out, counts));
+    if (report) {
+        report->records_queried = n;
+        report->queried_bases = 0;
+        for (uint64_t i = 0; i < n; ++i) report->queried_bases += ranges[i].sequence_bytes;
+        report->queried_kmers = counts[0];
+        report->positive_kmers = counts[1];
+    }
+    return SBF_OK;
+}
+
+extern "C" int sbf_ragged_tuning_lookup(const sbf_filter_t* f, int query, uint64_t len,
+                                        uint64_t n, sbf_ragged_tuning* out) {
+    if (!f || !out) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    if (tune_lookup(tune_key(f, query != 0, len, n), out)) return SBF_OK;
+    *out = default_tuning();
+    return set_error(SBF_ERR_INVALID_ARGUMENT, "no tuned entry for this shape (defaults returned)");
+}
+
+// Times candidate tunings on a prefix of the batch (records clipped to
+// `sample_bytes`) through the host pipeline, keeps the fastest and appends
+// it to the tuning table.  Inserting the prefix is idempotent for a batch
+// that is then inserted in full.
+extern "C" int sbf_ragged_autotune(sbf_filter_t* f, int query, const char* h_seq, uint64_t len,
+                                   const sbf_record_range* ranges, uint64_t n,
+                                   uint64_t sample_bytes, sbf_stream_t stream,
+                                   sbf_ragged_tuning* chosen) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    SBF_TRY(validate_ranges(len, ranges, n));
+    if (sample_bytes == 0) sample_bytes = uint64_t{256} << 20;
+    const uint64_t sl = std::min<uint64_t>(len, sample_bytes);
+    uint64_t sn = 0;
+    while (sn < n && ranges[sn].sequence_offset < sl) ++sn;
+    std::vector<sbf_record_range> sr(ranges, ranges + sn);
+    if (sn && sr[sn - 1].sequence_offset + sr[sn - 1].sequence_bytes > sl)
+        sr[sn - 1].sequence_bytes = sl - sr[sn - 1].sequence_offset;
+    std::vector<uint8_t> out(query ? std::max<uint64_t>(f->kmers_of(sl), 1) : 1);
+    const uint64_t chunks[] = {uint64_t{16} << 20, uint64_t{64} << 20, uint64_t{256} << 20};
+    const uint32_t stage_opts[] = {2, 3};
+    const uint32_t graph_opts[] = {0, 1};
+    sbf_ragged_tuning best = default_tuning();
+    double best_ms = 1e300;
+    for (uint64_t cb : chunks) {
+        if (cb > 2 * sl && cb != chunks[0]) continue;  // larger chunks only repeat the smaller
+        for (uint32_t stg : stage_opts)
+            for (uint32_t gr : graph_opts) {
+                sbf_ragged_tuning t{cb, stg, 0, gr};
+                unsigned long long counts[2];
+                double ms = 1e300;
+                for (int rep = 0; rep < 2; ++rep) {  // first run warms buffers and graphs
+                    const auto t0 = std::chrono::steady_clock::now();
+                    SBF_TRY(ragged_pipeline(f, query != 0, h_seq, sl, sr.data(), sn, t,
+                                            S_(stream), out.data(), counts));
+                    const auto t1 = std::chrono::steady_clock::now();
+                    ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = t;
+                }
+            }
+    }
+    tune_store(tune_key(f, query != 0, len, n), best, best_ms);
+    if (chosen) *chosen = best;
+    return SBF_OK;
+}

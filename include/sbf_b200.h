@@ -276,6 +276,67 @@ int sbf_record_batch_counts_noalloc(const sbf_filter_t* filter, const char* d_se
                                     sbf_stream_t stream, uint64_t* valid_out,
                                     uint64_t* positive_out);
 
+/* ---- Ragged batches (no reference counterpart) ------------------------
+ *
+ * Many records of uneven length in one buffer, processed in place by one
+ * persistent kernel launch whose CTAs take tiles from a device work queue.
+ * Records are (offset, bytes) ranges into the buffer, sorted by offset and
+ * non-overlapping (gaps allowed).  Exactly the windows that lie inside one
+ * record are inserted / queried: the result equals one insert_sequence /
+ * contains_sequence per record (filter.cuh:154-190, :464-533), the
+ * reference's "plain per-record launch".
+ *
+ * Query output layout: one byte per window of the whole buffer, the window
+ * starting at byte p at out[p]; record r's hits are
+ * out[offset_r, offset_r + bytes_r - k + 1).  Windows that cross a record
+ * boundary or touch a byte outside every record read 0.  Output length is
+ * len - k + 1 (0 when len < k). */
+
+/* Host pipeline knobs; zero fields take defaults. */
+typedef struct {
+    uint64_t chunk_bytes; /* bytes staged per chunk (default 64 MiB, min 4096) */
+    uint32_t stages;      /* chunks in flight, 1..4 (default 2) */
+    uint32_t ctas_per_sm; /* resident CTAs per SM, 0 = occupancy limit */
+    uint32_t use_graph;   /* replay each chunk's device work as a CUDA graph */
+} sbf_ragged_tuning;
+
+/* Device-resident ragged insert: d_seq (len bytes) and d_ranges (n records)
+ * on the device; ranges are trusted (unsorted ranges give unspecified
+ * results, never out-of-bounds access).  With d_counts non-NULL (device,
+ * 2 x uint64, zeroed by the caller) valid windows are added to d_counts[0].
+ * Asynchronous on `stream`. */
+int sbf_ragged_insert_async(sbf_filter_t* filter, const char* d_seq, uint64_t len,
+                            const sbf_record_range* d_ranges, uint64_t n, uint64_t* d_counts,
+                            sbf_stream_t stream);
+/* Device-resident ragged query into d_out (out_len >= len - k + 1); valid
+ * windows are added to d_counts[0] and positive ones to d_counts[1]. */
+int sbf_ragged_contains_async(const sbf_filter_t* filter, const char* d_seq, uint64_t len,
+                              const sbf_record_range* d_ranges, uint64_t n, uint8_t* d_out,
+                              uint64_t out_len, uint64_t* d_counts, sbf_stream_t stream);
+/* Host batches through the chunked pipeline (ranges validated as for
+ * record batches).  `tuning` NULL uses the tuning table entry for the
+ * batch's shape when there is one, else defaults.  Synchronous. */
+int sbf_ragged_insert(sbf_filter_t* filter, const char* h_seq, uint64_t len,
+                      const sbf_record_range* ranges, uint64_t n,
+                      const sbf_ragged_tuning* tuning, sbf_stream_t stream,
+                      sbf_insert_report* report);
+int sbf_ragged_query(const sbf_filter_t* filter, const char* h_seq, uint64_t len,
+                     const sbf_record_range* ranges, uint64_t n, uint8_t* h_out,
+                     uint64_t out_len, const sbf_ragged_tuning* tuning, sbf_stream_t stream,
+                     sbf_query_report* report);
+/* Times chunk size x stages x graph replay on a prefix of the batch
+ * (sample_bytes, 0 = 256 MiB), stores the fastest in the tuning table
+ * (SBF_TUNE_TABLE, default $HOME/.cache/cusbf_b200/ragged_tuning.tsv) under
+ * the batch's shape (operation, configuration, log2 bytes, log2 mean record
+ * bytes) and returns it.  An insert tune inserts the prefix. */
+int sbf_ragged_autotune(sbf_filter_t* filter, int query, const char* h_seq, uint64_t len,
+                        const sbf_record_range* ranges, uint64_t n, uint64_t sample_bytes,
+                        sbf_stream_t stream, sbf_ragged_tuning* chosen);
+/* Tuning table entry for a shape; SBF_ERR_INVALID_ARGUMENT (defaults in
+ * *out) when the table has none. */
+int sbf_ragged_tuning_lookup(const sbf_filter_t* filter, int query, uint64_t len, uint64_t n,
+                             sbf_ragged_tuning* out);
+
 /* ---- FASTA / FASTQ (filter.cuh:402-786, Fastx.hpp:297-481) ----------- */
 
 /* Record consumer of sbf_fastx_scan: header (without '>'/'@') and sequence
