@@ -214,6 +214,271 @@ def host_cores() -> int:
 
 
 # ---------------------------------------------------------------------------
+# Ragged batches (config c4)
+# ---------------------------------------------------------------------------
+
+RAGGED_METRIC = ("k-mers/s insert+query, ragged batch (200k log-normal records ~2 Gbp into a "
+                 "4 GiB filter + 50M log-normal reads, k=31) vs plain per-record launches")
+
+
+def ragged_spec(scale: float) -> dict:
+    return dict(name="ragged", n_records=max(int(200_000 * scale), 10), rec_median=5000,
+                rec_sigma=1.18, rec_lo=100, rec_hi=1_000_000, gc=0.45,
+                filter_bits=max(int((1 << 35) * scale), 1 << 20),
+                n_reads=max(int(50_000_000 * scale), 1000), read_median=150, read_sigma=1.0,
+                read_lo=50, read_hi=20_000, positive_frac=0.6, sub_rate=0.005)
+
+
+def _ev(torch):
+    return torch.cuda.Event(enable_timing=True)
+
+
+def run_ragged(args, world: int, rank: int, local_rank: int) -> None:
+    """One step = clear, one ragged insert launch over every record in place,
+    one ragged query launch over every read in place (device-resident
+    inputs).  Compared with plain per-record launches (insert_sequence_async
+    / contains_sequence_async per record, the reference's only per-record
+    form) on a sample, and end to end with the reference's single-launch
+    record batch (host normalisation + one launch)."""
+    from cusbf_b200.synthetic import lognormal_lengths, ragged_reads_device, uniform_dna
+
+    spec = ragged_spec(args.scale)
+    seed = args.seed + 1000 * rank
+    rec_len = lognormal_lengths(spec["n_records"], spec["rec_median"], spec["rec_sigma"],
+                                spec["rec_lo"], spec["rec_hi"], seed=seed)
+    rec_off = np.zeros_like(rec_len)
+    rec_off[1:] = np.cumsum(rec_len)[:-1]
+    genome = uniform_dna(int(rec_len.sum()), seed=seed + 1, gc=spec["gc"])
+    g_ranges = np.stack([rec_off, rec_len], axis=1).astype(np.uint64)
+    read_len = lognormal_lengths(spec["n_reads"], spec["read_median"], spec["read_sigma"],
+                                 spec["read_lo"], spec["read_hi"], seed=seed + 2)
+
+    import torch
+
+    import cusbf_b200 as sbf
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream(dev)
+    f = sbf.Filter(spec["filter_bits"], k=K, s=S, m=M, hashes=H)
+    d_genome = torch.from_numpy(genome).to(dev)
+    d_granges = torch.from_numpy(g_ranges.view(np.int64)).to(dev)
+    d_reads, r_ranges = ragged_reads_device(d_genome, rec_off, rec_len, read_len, seed + 3,
+                                            spec["positive_frac"], spec["sub_rate"], spec["gc"],
+                                            device=str(dev))
+    d_rranges = torch.from_numpy(r_ranges.view(np.int64)).to(dev)
+    n_out = f.kmer_count(d_reads.numel())
+    d_out = torch.empty(max(n_out, 1), dtype=torch.uint8, device=dev)
+    ins_counts = torch.zeros(2, dtype=torch.int64, device=dev)
+    q_counts = torch.zeros(2, dtype=torch.int64, device=dev)
+    torch.cuda.synchronize(dev)
+
+    def step(ev):
+        f.clear(stream)
+        ins_counts.zero_()
+        q_counts.zero_()
+        ev[0].record(stream)
+        f.ragged_insert_async(d_genome, d_granges, ins_counts, stream)
+        ev[1].record(stream)
+        f.ragged_contains_async(d_reads, d_rranges, d_out, q_counts, stream)
+        ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step([_ev(torch) for _ in range(3)])
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    evs = [[_ev(torch) for _ in range(3)] for _ in range(args.steps)]
+    t0, t1 = _ev(torch), _ev(torch)
+    t0.record(stream)
+    for i in range(args.steps):
+        step(evs[i])
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    clock_info = clocks.stop()
+    total_ms = t0.elapsed_time(t1)
+    ins_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
+    q_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
+    ins_valid, q_valid, q_pos = int(ins_counts[0]), int(q_counts[0]), int(q_counts[1])
+    if dist:
+        t = torch.tensor([total_ms, ins_ms, q_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, ins_ms, q_ms = (float(x) for x in t.tolist())
+    ms_per_step = total_ms / args.steps
+    kmers_step = ins_valid + q_valid
+    value = world * kmers_step / (ms_per_step / 1e3)
+    ragged_hits = d_out.clone()
+
+    # Plain per-record launches on a sample: the first records / reads up to
+    # ~16 MB each, one launch per record, same filter state.
+    plain = None
+    if not args.no_baselines:
+        n_rs = int(np.searchsorted(np.cumsum(rec_len), 16_000_000)) + 1
+        n_qs = int(np.searchsorted(np.cumsum(read_len), 16_000_000)) + 1
+        n_rs, n_qs = min(n_rs, rec_len.size), min(n_qs, read_len.size)
+        pf = sbf.Filter(spec["filter_bits"], k=K, s=S, m=M, hashes=H)
+        a, b = _ev(torch), _ev(torch)
+        torch.cuda.synchronize(dev)
+        a.record(stream)
+        for i in range(n_rs):
+            o, n = int(rec_off[i]), int(rec_len[i])
+            pf.insert_sequence_async(d_genome[o:o + n], stream)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        p_ins_ms = a.elapsed_time(b)
+        p_ins_k = int(np.maximum(rec_len[:n_rs] - K + 1, 0).sum())
+        # Query the sample against the full filter, compare with the ragged hits.
+        chk = torch.zeros_like(d_out[: int(r_ranges[n_qs - 1, 0] + r_ranges[n_qs - 1, 1])])
+        a.record(stream)
+        for i in range(n_qs):
+            o, n = int(r_ranges[i, 0]), int(r_ranges[i, 1])
+            if n >= K:
+                f.contains_sequence_async(d_reads[o:o + n], chk[o:o + n - K + 1], stream)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        p_q_ms = a.elapsed_time(b)
+        p_q_k = int(np.maximum(read_len[:n_qs] - K + 1, 0).sum())
+        same = True
+        for i in range(n_qs):
+            o, n = int(r_ranges[i, 0]), int(r_ranges[i, 1])
+            if n >= K and not torch.equal(chk[o:o + n - K + 1], ragged_hits[o:o + n - K + 1]):
+                same = False
+                break
+        plain = {"insert_kmers_per_s": p_ins_k / (p_ins_ms / 1e3),
+                 "query_kmers_per_s": p_q_k / (p_q_ms / 1e3),
+                 "kmers_per_s": (p_ins_k + p_q_k) / ((p_ins_ms + p_q_ms) / 1e3),
+                 "us_per_launch": 1e3 * (p_ins_ms + p_q_ms) / (n_rs + n_qs),
+                 "sample": f"{n_rs} records ({int(rec_len[:n_rs].sum()) / 1e6:.1f} Mbp) + "
+                           f"{n_qs} reads ({int(read_len[:n_qs].sum()) / 1e6:.1f} MB), one "
+                           "insert_sequence_async / contains_sequence_async per record from Python",
+                 "query_hits_identical_to_ragged": same}
+        pf.close()
+
+    # End to end through the host API: pinned inputs and outputs.
+    e2e = e2e_tuned = rb = None
+    if not args.no_e2e:
+        h_genome = torch.from_numpy(genome).pin_memory().numpy()
+        h_reads_t = torch.empty(d_reads.numel(), dtype=torch.uint8).pin_memory()
+        h_reads_t.copy_(d_reads)
+        h_reads = h_reads_t.numpy()
+        h_out = torch.empty(max(n_out, 1), dtype=torch.uint8).pin_memory().numpy()
+
+        def e2e_run(tuning):
+            f.clear(stream)
+            torch.cuda.synchronize(dev)
+            w0 = time.perf_counter()
+            ri = f.ragged_insert(h_genome, g_ranges, tuning=tuning, stream=stream)
+            w1 = time.perf_counter()
+            _, rq = f.ragged_query(h_reads, r_ranges, out=h_out, tuning=tuning, stream=stream)
+            w2 = time.perf_counter()
+            assert ri.inserted_kmers == ins_valid and rq.positive_kmers == q_pos
+            return (w1 - w0) * 1e3, (w2 - w1) * 1e3
+
+        def e2e_obj(res, tuning):
+            ims = float(np.median([r[0] for r in res]))
+            qms = float(np.median([r[1] for r in res]))
+            return {"value": world * kmers_step / ((ims + qms) / 1e3), "unit": "k-mers/s",
+                    "h2d_bytes_per_step": int(genome.size + h_reads.size + 32 * (
+                        g_ranges.shape[0] + r_ranges.shape[0])),
+                    "d2h_bytes_per_step": int(n_out), "ms_per_step": ims + qms,
+                    "insert_ms": ims, "query_ms": qms, "tuning": tuning,
+                    "api": "sbf_ragged_insert + sbf_ragged_query (host buffers, pinned)"}
+
+        e2e_run(None)
+        e2e = e2e_obj([e2e_run(None) for _ in range(max(1, args.e2e_steps))], "default")
+        ti = f.ragged_autotune(h_genome, g_ranges, query=False, stream=stream)
+        tq = f.ragged_autotune(h_reads, r_ranges, query=True, stream=stream)
+        res = []
+        for _ in range(max(1, args.e2e_steps)):
+            f.clear(stream)
+            torch.cuda.synchronize(dev)
+            w0 = time.perf_counter()
+            f.ragged_insert(h_genome, g_ranges, tuning=ti, stream=stream)
+            w1 = time.perf_counter()
+            f.ragged_query(h_reads, r_ranges, out=h_out, tuning=tq, stream=stream)
+            w2 = time.perf_counter()
+            res.append(((w1 - w0) * 1e3, (w2 - w1) * 1e3))
+        e2e_tuned = e2e_obj(res, {"insert": ti.as_dict(), "query": tq.as_dict()})
+        # The reference's single-launch record batch (host normalisation with
+        # separators, one plain launch), insert and aggregate query.
+        if not args.no_baselines:
+            f.clear(stream)
+            torch.cuda.synchronize(dev)
+            w0 = time.perf_counter()
+            f.insert_record_batch(h_genome, g_ranges, stream=stream)
+            w1 = time.perf_counter()
+            qr = f.query_record_batch(h_reads, r_ranges, stream=stream)
+            w2 = time.perf_counter()
+            assert qr.positive_kmers == q_pos
+            rb = {"value": kmers_step / (w2 - w0), "unit": "k-mers/s",
+                  "insert_ms": (w1 - w0) * 1e3, "query_ms": (w2 - w1) * 1e3,
+                  "api": "sbf_insert_record_batch + sbf_query_record_batch (normalised copy, "
+                         "one plain launch each, per-record counts only)"}
+
+    if rank != 0:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    q_sample = d_reads[: min(d_reads.numel(), 3_000_000)].cpu().numpy()
+    runs_q, valid_q = sample_runs(q_sample, f.num_shards())
+    r_per_q = runs_q / max(valid_q, 1)
+    q_bytes = d_reads.numel() + n_out + 32 * r_per_q * q_valid
+    peaks = {}
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peaks = json.load(open(peaks_path))
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    q_ach = q_bytes / (q_ms / 1e3) / 1e9
+    line = {
+        "metric": RAGGED_METRIC, "value": value, "unit": "k-mers/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded log-normal records and reads with the configuration's shapes)",
+        "config": {"workload": f"ragged: {spec['n_records']:,} records ({genome.size / 1e9:.2f} "
+                               f"Gbp, log-normal median 5 kbp) inserted, {spec['n_reads']:,} "
+                               f"reads ({d_reads.numel() / 1e9:.2f} GB, log-normal median 150 bp) "
+                               "queried, records in place",
+                   "k": K, "s": S, "m": M, "hashes": H, "filter_bits": f.filter_bits(),
+                   "insert_kmers": ins_valid, "query_kmers": q_valid,
+                   "parallelism": f"replicas x{world} (weak)",
+                   "l2": "inputs larger than L2 (no flush needed)",
+                   "step": "clear + one ragged insert launch + one ragged query launch"},
+        "insert": {"ms": ins_ms, "kmers_per_s": ins_valid / (ins_ms / 1e3)},
+        "query": {"ms": q_ms, "kmers_per_s": q_valid / (q_ms / 1e3), "positives": q_pos},
+        "roofline": {"bound": "hbm", "kernel": "query (tile_kernel<31,28,16,4> ragged query)",
+                     "achieved": round(q_ach, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(q_ach / peak, 4),
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                     "traffic": None, "algorithmic_bytes": int(q_bytes),
+                     "model": f"L + N + 32R (R/N={r_per_q:.4f} counted by the oracle on 3 MB)"},
+        "plain_per_record": plain,
+        "speedup_vs_plain": (value / plain["kmers_per_s"]) if plain else None,
+        "record_batch_e2e": rb,
+        "e2e": e2e,
+        "e2e_tuned": e2e_tuned,
+        "gpu_launches": 4 * args.steps,
+        "clocks": clock_info,
+    }
+    print(json.dumps(line), flush=True)
+    f.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
 # Main
 # ---------------------------------------------------------------------------
 
@@ -222,7 +487,7 @@ def main() -> None:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3"])
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0,
                     help="size multiplier for small profiling runs (1.0 = the named config)")
@@ -230,6 +495,8 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-baselines", action="store_true",
+                    help="c4: skip the per-record and record-batch comparisons")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours" and args.scale == 1.0:
         print("note: at least 3 warm-up steps are used for reported numbers", file=sys.stderr)
@@ -237,6 +504,15 @@ def main() -> None:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.config == "c4":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "metric": RAGGED_METRIC,
+                              "unavailable": "the ragged form has no reference counterpart; "
+                                             "its baselines (plain per-record launches, record "
+                                             "batch) are inside the c4 line"}))
+            return
+        run_ragged(args, world, rank, local_rank)
+        return
     spec = workload_spec(args.config, args.scale)
 
     # Host data is generated before any CUDA call (the generator may fork a

@@ -218,3 +218,55 @@ def reads_device(source, n_reads: int, length: int, seed: int, sub_rate: float =
             mutated = sub[((code + shift) & 3).long()]
             blk[:k] = torch.where(mask, mutated, src)
     return out
+
+
+def ragged_reads_device(source, rec_off: np.ndarray, rec_len: np.ndarray, lengths: np.ndarray,
+                        seed: int, positive_frac: float, sub_rate: float, gc: float,
+                        device: str = "cuda", chunk_bytes: int = 1 << 26):
+    """Reads of the given lengths, back to back in one uint8 CUDA tensor, and
+    their (offset, bytes) ranges.  A `positive_frac` share (chosen at random)
+    is copied from `source` (records at rec_off/rec_len, picked with
+    probability proportional to length) with substitutions at `sub_rate`;
+    the rest are i.i.d. bases at the given GC fraction."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    n = lengths.size
+    lengths = lengths.astype(np.int64)
+    offsets = np.zeros(n, np.int64)
+    if n > 1:
+        offsets[1:] = np.cumsum(lengths)[:-1]
+    total = int(lengths.sum())
+    positive = rng.random(n) < positive_frac
+    rec = rng.choice(rec_len.size, size=n, p=rec_len / rec_len.sum())
+    room = np.maximum(rec_len[rec] - lengths, 0)
+    starts = rec_off[rec] + np.floor(rng.random(n) * (room + 1)).astype(np.int64)
+    starts = np.minimum(starts, source.numel() - lengths)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    lut = torch.from_numpy(_base_lut(gc)).to(device)
+    sub = torch.tensor(list(b"ACTG"), dtype=torch.uint8, device=device)
+    out = torch.empty(total, dtype=torch.uint8, device=device)
+    d_len = torch.from_numpy(lengths).to(device)
+    d_off = torch.from_numpy(offsets).to(device)
+    d_start = torch.from_numpy(starts).to(device)
+    d_pos = torch.from_numpy(positive).to(device)
+    ends = offsets + lengths
+    i = 0
+    while i < n:
+        j = int(np.searchsorted(ends, offsets[i] + chunk_bytes, side="right"))
+        j = max(j, i + 1)
+        b0, b1 = int(offsets[i]), int(ends[j - 1])
+        nb = b1 - b0
+        rid = torch.repeat_interleave(torch.arange(i, j, device=device), d_len[i:j])
+        rel = torch.arange(b0, b1, device=device, dtype=torch.int64) - d_off[rid]
+        src = source[d_start[rid] + rel]
+        code = ((src >> 1) & 3).to(torch.int32)
+        shift = torch.randint(1, 4, (nb,), device=device, generator=g, dtype=torch.int32)
+        mutated = torch.where(torch.rand(nb, device=device, generator=g) < sub_rate,
+                              sub[((code + shift) & 3).long()], src)
+        rand = lut[torch.randint(0, 256, (nb,), device=device, generator=g,
+                                 dtype=torch.int32).long()]
+        out[b0:b1] = torch.where(d_pos[rid], mutated, rand)
+        i = j
+    return out, np.stack([offsets, lengths], axis=1).astype(np.uint64)
