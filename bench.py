@@ -479,6 +479,204 @@ def run_ragged(args, world: int, rank: int, local_rank: int) -> None:
 
 
 # ---------------------------------------------------------------------------
+# Serving (config c5)
+# ---------------------------------------------------------------------------
+
+SERVED_METRIC = ("served k-mers/s and p50/p99/p999 latency, Poisson 20k req/s (log-uniform "
+                 "1-100k x 150 bp reads, 5% inserts of 1-10 Mbp) on the resident 100 Mbp filter")
+
+
+def _poisson_schedule(seed: int, rate: float, duration: float, pool_reads: int,
+                      ins_pool: int, scale: float):
+    """Arrival offsets (s), insert flags, reads per query, first read, insert
+    bytes and insert offsets of the requests."""
+    rng = np.random.default_rng(seed)
+    n = int(rate * duration * 1.2) + 16
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    t = t[t < duration]
+    n = t.size
+    is_ins = rng.random(n) < 0.05
+    n_reads = np.floor(np.exp(rng.uniform(0.0, np.log(100_001 * scale), size=n))).astype(np.int64)
+    n_reads = np.clip(n_reads, 1, pool_reads)
+    first = (rng.random(n) * (pool_reads - n_reads + 1)).astype(np.int64)
+    ins_bytes = np.clip((rng.uniform(1e6, 10e6, size=n) * scale).astype(np.int64), 1000, ins_pool)
+    ins_off = (rng.random(n) * (ins_pool - ins_bytes + 1)).astype(np.int64)
+    return t, is_ins, n_reads, first, ins_bytes, ins_off
+
+
+def run_served(args, world: int, rank: int, local_rank: int) -> None:
+    """Open-loop load: requests arrive on a seeded Poisson schedule and are
+    submitted at their arrival times; latency is completion minus scheduled
+    arrival.  The same schedule is replayed against one-request-per-launch
+    serving, and the per-read launch cost of the plain per-record path is
+    measured.  Query requests are slices of a pinned pool of reads (half
+    sampled from the genome with 1% substitutions, half random); insert
+    requests are slices of a pinned pool of uniform sequence."""
+    import torch
+
+    import cusbf_b200 as sbf
+    from cusbf_b200.synthetic import reads_device, uniform_dna
+
+    scale = args.scale
+    spec = workload_spec("c2", 1.0)
+    joined, _, n_valid = build_host_genome(spec, seed=args.seed + 1000 * rank)
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    bits = int(round(spec["bits_per_kmer"] * n_valid))
+    rate = (args.rate or 20_000.0) * min(scale, 1.0)
+    duration = args.duration
+    pool_reads = int(26_000_000 * min(1.0, max(scale, 0.02)))
+    read_len = 150
+    d_genome = torch.from_numpy(joined).to(dev)
+    reads = reads_device(d_genome, pool_reads, read_len, seed=args.seed + 11, sub_rate=0.01,
+                         positive_frac=0.5, device=str(dev))
+    perm = torch.randperm(pool_reads, device=dev,
+                          generator=torch.Generator(device=dev).manual_seed(args.seed + 12))
+    reads = reads[perm].reshape(-1)
+    pool = torch.empty(reads.numel(), dtype=torch.uint8).pin_memory()
+    pool.copy_(reads)
+    del reads, perm
+    pool_np = pool.numpy()
+    rng_t = torch.empty((pool_reads, 2), dtype=torch.int64).pin_memory()
+    rng_np = rng_t.numpy().view(np.uint64)
+    rng_np[:, 0] = np.arange(pool_reads, dtype=np.uint64) * read_len
+    rng_np[:, 1] = read_len
+    ins_pool_bytes = int(1 << 30) if scale >= 1 else int(max((1 << 30) * scale, 1 << 24))
+    ins_pool = torch.from_numpy(uniform_dna(ins_pool_bytes, seed=args.seed + 13)).pin_memory()
+    ins_np = ins_pool.numpy()
+    t_arr, is_ins, n_reads, first, ins_bytes, ins_off = _poisson_schedule(
+        args.seed + 14, rate, duration, pool_reads, ins_pool_bytes, min(scale, 1.0))
+    n_req = t_arr.size
+    out_ring_bytes = int(min(8 << 30, max(pool_np.size * 2, 1 << 26)))
+    out_ring = torch.empty(out_ring_bytes, dtype=torch.uint8).pin_memory()
+    out_np = out_ring.numpy()
+    check_idx = set(range(0, n_req, max(1, n_req // 64)))
+    check_out = {i: np.zeros(max(int(n_reads[i]) * read_len - K + 1, 1), np.uint8)
+                 for i in check_idx if not is_ins[i]}
+    ins_range_t = torch.empty((n_req, 2), dtype=torch.int64).pin_memory()
+    ins_range = ins_range_t.numpy().view(np.uint64)
+    ins_range[:, 0] = ins_off.astype(np.uint64)
+    ins_range[:, 1] = ins_bytes.astype(np.uint64)
+
+    def run_stream(srv):
+        """Submits the schedule at its arrival times."""
+        ring_pos = 0
+        ring_live = []  # (ticket, start, end) of output regions in use, oldest first
+        lags = []
+        t0 = sbf.Server.now() + 0.05
+        for i in range(n_req):
+            arrival = t0 + float(t_arr[i])
+            while sbf.Server.now() < arrival:
+                pass
+            if is_ins[i]:
+                srv.submit_raw(0, ins_np.ctypes.data, ins_range.ctypes.data + 16 * i, 1, None, 0,
+                               arrival)
+            else:
+                nr = int(n_reads[i])
+                w = nr * read_len - K + 1
+                if i in check_out:
+                    optr = check_out[i].ctypes.data
+                else:
+                    if ring_pos + w > out_ring_bytes:
+                        ring_pos = 0
+                    lo, hi = ring_pos, ring_pos + w
+                    while ring_live and ring_live[0][1] < hi and ring_live[0][2] > lo:
+                        srv.wait(ring_live.pop(0)[0])
+                    optr = out_np.ctypes.data + lo
+                    ring_pos = hi
+                t = srv.submit_raw(1, pool_np.ctypes.data, rng_np.ctypes.data + 16 * int(first[i]),
+                                   nr, optr, w, arrival)
+                if i not in check_out:
+                    ring_live.append((t, lo, hi))
+                    while len(ring_live) > 4096:
+                        srv.wait(ring_live.pop(0)[0])
+            lags.append(sbf.Server.now() - arrival)
+        srv.drain()
+        return {"submit_lag_p50_ms": float(np.median(lags)) * 1e3,
+                "submit_lag_p99_ms": float(np.quantile(lags, 0.99)) * 1e3}
+
+    def serve(**cfg):
+        f = sbf.Filter(bits, k=K, s=S, m=M, hashes=H)
+        f.insert_sequence(joined)
+        srv = sbf.Server(f, staging_bytes=16 << 30, **cfg)
+        lag = run_stream(srv)
+        st = srv.stats()
+        srv.close()
+        words_sum = int(np.bitwise_xor.reduce(f.words_host()))
+        f.close()
+        kmers = st["query_windows"] + st["insert_windows"]
+        return {"kmers_per_s": kmers / st["wall_s"] if st["wall_s"] else None,
+                "config": cfg, "requests": st["requests"],
+                "requests_per_s": st["requests"] / st["wall_s"] if st["wall_s"] else None,
+                "batches": st["batches"], "mean_batch_requests": st["mean_batch_requests"],
+                "latency_ms": {"p50": st["p50_s"] * 1e3, "p99": st["p99_s"] * 1e3,
+                               "p999": st["p999_s"] * 1e3, "max": st["max_s"] * 1e3,
+                               "mean": st["mean_s"] * 1e3},
+                "wall_s": st["wall_s"], "worker_busy_s": st["worker_busy_s"],
+                "admission_wait_s": st["admission_wait_s"], "slot_wait_s": st["slot_wait_s"],
+                **lag}, words_sum, {i: o.copy() for i, o in check_out.items()}
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    served, served_words, served_checks = serve(max_inflight=args.server_inflight,
+                                                max_batch_bytes=args.server_batch_mb << 20,
+                                                use_graph=args.server_graph)
+    clock_info = clocks.stop()
+    serial = identical = None
+    if not args.no_serial:
+        serial, serial_words, serial_checks = serve(max_batch_requests=1, max_inflight=1)
+        identical = bool(served_words == serial_words and all(
+            np.array_equal(served_checks[i], serial_checks[i]) for i in served_checks))
+
+    # Plain per-record launches: one contains_sequence_async per read.
+    f = sbf.Filter(bits, k=K, s=S, m=M, hashes=H)
+    f.insert_sequence(joined)
+    d_pool = torch.from_numpy(pool_np[: 4000 * read_len].copy()).to(dev)
+    d_o = torch.empty(4000 * read_len, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    a, b = _ev(torch), _ev(torch)
+    torch.cuda.synchronize(dev)
+    a.record(stream)
+    for r in range(4000):
+        f.contains_sequence_async(d_pool[r * read_len:(r + 1) * read_len],
+                                  d_o[r * read_len:(r + 1) * read_len - K + 1], stream)
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    per_read_ms = a.elapsed_time(b) / 4000
+    mean_reads = float(np.mean(n_reads[~is_ins]))
+    plain = {"us_per_read_launch": per_read_ms * 1e3,
+             "kmers_per_s": (read_len - K + 1) / (per_read_ms / 1e3),
+             "service_ms_per_mean_request": per_read_ms * mean_reads,
+             "sustainable_requests_per_s": 1e3 / (per_read_ms * mean_reads),
+             "note": "device-resident reads, one launch per read from Python; the offered "
+                     f"{rate:.0f} req/s is far beyond it"}
+    f.close()
+    offered = float(np.sum(np.where(is_ins, ins_bytes, n_reads * read_len)))
+    line = {
+        "metric": SERVED_METRIC, "value": served["kmers_per_s"], "unit": "k-mers/s",
+        "n_gpus": world, "steps": 1, "warmup": 0, "ms_per_step": served["wall_s"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded Poisson request stream over seeded reads and sequences)",
+        "config": {"workload": f"served: {n_req:,} requests over {duration:.1f} s at "
+                               f"{rate:.0f} req/s, filter of the 100 Mbp genome resident",
+                   "k": K, "s": S, "m": M, "hashes": H, "filter_bits": bits,
+                   "staging_budget_bytes": 16 << 30, "offered_bytes": int(offered),
+                   "offered_gb_per_s": offered / duration / 1e9,
+                   "read_pool": f"{pool_reads:,} reads of 150 bp (half sampled with 1% "
+                                "substitutions, half random); requests are pool slices",
+                   "l2": "inputs larger than L2 (no flush needed)"},
+        "served": served,
+        "one_request_per_launch": serial,
+        "plain_per_record": plain,
+        "identical_to_one_at_a_time": identical,
+        "checked_requests": len(served_checks),
+        "gpu_launches": 2 * served["batches"],
+        "clocks": clock_info,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # Main
 # ---------------------------------------------------------------------------
 
@@ -487,7 +685,13 @@ def main() -> None:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--duration", type=float, default=2.0, help="c5: seconds of arrivals")
+    ap.add_argument("--server-inflight", type=int, default=0, help="c5: batches in flight")
+    ap.add_argument("--server-batch-mb", type=int, default=0, help="c5: batch cap in MiB")
+    ap.add_argument("--server-graph", type=int, default=0, help="c5: graph replay")
+    ap.add_argument("--no-serial", action="store_true", help="c5: skip the one-per-launch run")
+    ap.add_argument("--rate", type=float, default=0.0, help="c5: offered req/s (default 20k)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0,
                     help="size multiplier for small profiling runs (1.0 = the named config)")
@@ -512,6 +716,15 @@ def main() -> None:
                                              "batch) are inside the c4 line"}))
             return
         run_ragged(args, world, rank, local_rank)
+        return
+    if args.config == "c5":
+        if args.impl == "reference" or rank != 0:
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "metric": SERVED_METRIC,
+                                  "unavailable": "the served form has no reference counterpart; "
+                                                 "its baselines are inside the c5 line"}))
+            return
+        run_served(args, world, rank, local_rank)
         return
     spec = workload_spec(args.config, args.scale)
 

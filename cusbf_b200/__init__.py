@@ -15,6 +15,7 @@ integers, or ``None`` for the legacy default stream.
 from __future__ import annotations
 
 import ctypes as C
+import threading
 import os
 from dataclasses import dataclass
 
@@ -108,6 +109,34 @@ class RaggedTuning(C.Structure):
 
     _fields_ = [("chunk_bytes", C.c_uint64), ("stages", C.c_uint32),
                 ("ctas_per_sm", C.c_uint32), ("use_graph", C.c_uint32)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class ServerConfig(C.Structure):
+    """sbf_server_config (0 = default)."""
+
+    _fields_ = [("staging_bytes", C.c_uint64), ("max_batch_bytes", C.c_uint64),
+                ("pinned_bytes", C.c_uint64), ("max_inflight", C.c_uint32),
+                ("max_batch_requests", C.c_uint32), ("use_graph", C.c_uint32)]
+
+
+class ServerRequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("latency_s", C.c_double), ("windows", C.c_uint64),
+                ("arrival_s", C.c_double), ("done_s", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("requests", C.c_uint64), ("batches", C.c_uint64),
+                ("query_windows", C.c_uint64), ("insert_windows", C.c_uint64),
+                ("wall_s", C.c_double), ("p50_s", C.c_double), ("p99_s", C.c_double),
+                ("p999_s", C.c_double), ("max_s", C.c_double), ("mean_s", C.c_double),
+                ("mean_batch_requests", C.c_double), ("worker_busy_s", C.c_double),
+                ("admission_wait_s", C.c_double), ("slot_wait_s", C.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -212,6 +241,14 @@ _sig("sbf_ragged_query", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, C.POINTE
 _sig("sbf_ragged_autotune", C.c_int, _vp, C.c_int, _vp, _u64, _vp, _u64, _u64, _vp,
      C.POINTER(RaggedTuning))
 _sig("sbf_ragged_tuning_lookup", C.c_int, _vp, C.c_int, _u64, _u64, C.POINTER(RaggedTuning))
+_sig("sbf_server_create", C.c_int, _vp, C.POINTER(ServerConfig), C.POINTER(_vp))
+_sig("sbf_server_destroy", None, _vp)
+_sig("sbf_server_now", C.c_double)
+_sig("sbf_server_submit", C.c_int, _vp, C.c_int, _vp, _vp, _u64, _vp, _u64, C.c_double,
+     C.POINTER(_u64))
+_sig("sbf_server_wait", C.c_int, _vp, _u64, C.c_double, C.POINTER(ServerRequestInfo))
+_sig("sbf_server_drain", C.c_int, _vp)
+_sig("sbf_server_get_stats", C.c_int, _vp, C.c_int, C.POINTER(ServerStats))
 _sig("sbf_record_batch_counts_noalloc", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _vp,
      _vp, _vp)
 _sig("sbf_fastx_scan", C.c_int, READ_FN, _vp, C.c_char_p, SCAN_CB, _vp, C.POINTER(_u64))
@@ -800,3 +837,92 @@ __all__ = [
     "fastx_scan", "fastx_scan_file",
     "pack_dense_sequence", "pack_dense_sequence_device", "lib", "version", "LIBRARY_PATH",
 ]
+
+
+class Server:
+    """Request server over a resident filter (sbf_server_*): continuous
+    batching of insert and query requests from any number of threads; every
+    result equals one-request-at-a-time execution in arrival order.  While it
+    runs, the filter must not be used directly."""
+
+    INSERT, QUERY = 0, 1
+
+    def __init__(self, filt: "Filter", **config):
+        self._filter = filt
+        cfg = ServerConfig(**config)
+        h = _vp()
+        _check(_lib.sbf_server_create(filt._h, C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._refs: dict[int, tuple] = {}
+        self._lock = threading.Lock()
+
+    @staticmethod
+    def now() -> float:
+        return _lib.sbf_server_now()
+
+    def submit_raw(self, op: int, base_ptr: int, ranges_ptr: int, n: int, out_ptr, out_len: int,
+                   arrival: float = 0.0) -> int:
+        """Pointer-level submit: the caller keeps the buffers alive."""
+        t = _u64()
+        _check(_lib.sbf_server_submit(self._h, op, base_ptr, ranges_ptr, n, out_ptr, out_len,
+                                      arrival, C.byref(t)))
+        return t.value
+
+    def submit(self, op: int, base, ranges, out=None, arrival: float = 0.0) -> int:
+        b = _host_bytes(base)
+        r = _ranges(ranges)
+        o = out
+        if op == self.QUERY and o is None:
+            span = max(int(r[-1, 0] + r[-1, 1]) - int(r[0, 0]), 0) if r.shape[0] else 0
+            o = np.zeros(max(self._filter.kmer_count(span), 1), np.uint8)
+        t = self.submit_raw(op, _np_ptr(b), _np_ptr(r), r.shape[0],
+                            _np_ptr(o) if o is not None else None,
+                            o.size if o is not None else 0, arrival)
+        with self._lock:
+            self._refs[t] = (b, r, o)
+        return t
+
+    def submit_query(self, base, ranges, out=None, arrival: float = 0.0) -> int:
+        return self.submit(self.QUERY, base, ranges, out, arrival)
+
+    def submit_insert(self, base, ranges, arrival: float = 0.0) -> int:
+        return self.submit(self.INSERT, base, ranges, None, arrival)
+
+    def wait(self, ticket: int, timeout: float = 0.0):
+        """Waits for a request; returns (info dict, query hits or None)."""
+        info = ServerRequestInfo()
+        st = _lib.sbf_server_wait(self._h, ticket, timeout, C.byref(info))
+        with self._lock:
+            refs = self._refs.pop(ticket, None)
+        _check(st)
+        out = None
+        if refs is not None and refs[2] is not None:
+            out = refs[2][:info.windows]
+        return info.as_dict(), out
+
+    def drain(self) -> None:
+        _check(_lib.sbf_server_drain(self._h))
+
+    def stats(self, reset: bool = False) -> dict:
+        s = ServerStats()
+        _check(_lib.sbf_server_get_stats(self._h, int(reset), C.byref(s)))
+        return s.as_dict()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.sbf_server_destroy(self._h)
+            self._h = None
+            self._refs.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -30,6 +30,7 @@
 #include "../../include/sbf_b200.h"
 #include "sbf_host.h"
 #include "sbf_internal.h"
+#include "sbf_ragged.h"
 
 using namespace sbf;
 
@@ -69,11 +70,7 @@ struct RaggedSlot {
     size_t out_cap = 0;
     cudaEvent_t ev_copied = nullptr, ev_done = nullptr;
     bool busy = false;
-    // Device work of one chunk as a graph: tile records -> queue reset ->
-    // tile kernel.  Built on first use per (slot, operation).
-    cudaGraph_t graph[2] = {nullptr, nullptr};
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
-    cudaGraphNode_t n_rec[2] = {}, n_tile[2] = {};
+    RaggedGraph graph[2];  // per operation (insert, query)
 };
 
 struct RaggedState {
@@ -125,10 +122,7 @@ static void release_slot(RaggedSlot& s) {
     if (s.d_out) cudaFree(s.d_out);
     if (s.ev_copied) cudaEventDestroy(s.ev_copied);
     if (s.ev_done) cudaEventDestroy(s.ev_done);
-    for (int i = 0; i < 2; ++i) {
-        if (s.exec[i]) cudaGraphExecDestroy(s.exec[i]);
-        if (s.graph[i]) cudaGraphDestroy(s.graph[i]);
-    }
+    for (auto& g : s.graph) ragged_graph_release(g);
     s = RaggedSlot{};
 }
 
@@ -166,8 +160,7 @@ static unsigned long long* ctl_counts(RaggedState* r) {
     return reinterpret_cast<unsigned long long*>(r->d_ctl + 2);
 }
 
-// Kernel parameters of one ragged launch over `len` bytes at d_seq.
-static TileParams ragged_params(const sbf_filter* f, bool query, const uint8_t* d_seq,
+TileParams ragged_params(const sbf_filter* f, bool query, const uint8_t* d_seq,
                                 uint64_t len, const DevRange* d_rng, uint64_t n,
                                 const uint32_t* d_tile_rec, uint8_t* d_out, unsigned int* queue,
                                 unsigned long long* counts) {
@@ -202,8 +195,7 @@ static unsigned ragged_grid(const sbf_filter* f, bool query, uint64_t n_tiles, u
     return static_cast<unsigned>(std::max<uint64_t>(std::min<uint64_t>(n_tiles, resident), 1));
 }
 
-// Stream launch of one ragged pass: tile records, queue reset, tile kernel.
-static int ragged_launch(sbf_filter* f, bool query, const TileParams& p, uint32_t ctas,
+int ragged_launch(sbf_filter* f, bool query, const TileParams& p, uint32_t ctas,
                          cudaStream_t st) {
     if (p.n_tiles == 0) return SBF_OK;
     SBF_CUDA(launch_tile_records(p.ranges, p.n_ranges, p.sym_base, p.n_tiles,
@@ -217,12 +209,11 @@ static int ragged_launch(sbf_filter* f, bool query, const TileParams& p, uint32_
     return SBF_OK;
 }
 
-// The same pass as a graph launch.  The graph of a slot is built once per
-// operation; later chunks only update the two kernel nodes' parameters.
-static int ragged_graph_launch(sbf_filter* f, RaggedSlot& s, bool query, const TileParams& p,
-                               uint32_t ctas, cudaStream_t st) {
+// The graph is built on first use; later launches only update the two
+// kernel nodes' parameters.
+int ragged_graph_launch(sbf_filter* f, RaggedGraph& g, bool query, const TileParams& p,
+                        uint32_t ctas, cudaStream_t st) {
     if (p.n_tiles == 0) return SBF_OK;
-    const int op = query ? 1 : 0;
     const DevRange* a_rng = p.ranges;
     uint64_t a_n = p.n_ranges;
     int64_t a_base = p.sym_base;
@@ -242,9 +233,9 @@ static int ragged_graph_launch(sbf_filter* f, RaggedSlot& s, bool query, const T
     tk.blockDim = dim3(kThreads);
     tk.sharedMemBytes = query ? kQuerySlotBytes : kInsertSlotBytes;
     tk.kernelParams = tile_args;
-    if (!s.exec[op]) {
-        SBF_CUDA(cudaGraphCreate(&s.graph[op], 0));
-        SBF_CUDA(cudaGraphAddKernelNode(&s.n_rec[op], s.graph[op], nullptr, 0, &rk));
+    if (!g.exec) {
+        SBF_CUDA(cudaGraphCreate(&g.graph, 0));
+        SBF_CUDA(cudaGraphAddKernelNode(&g.n_rec, g.graph, nullptr, 0, &rk));
         cudaMemsetParams ms{};
         ms.dst = p.queue;
         ms.value = 0;
@@ -252,16 +243,22 @@ static int ragged_graph_launch(sbf_filter* f, RaggedSlot& s, bool query, const T
         ms.width = 1;
         ms.height = 1;
         cudaGraphNode_t n_ms;
-        SBF_CUDA(cudaGraphAddMemsetNode(&n_ms, s.graph[op], &s.n_rec[op], 1, &ms));
-        SBF_CUDA(cudaGraphAddKernelNode(&s.n_tile[op], s.graph[op], &n_ms, 1, &tk));
-        SBF_CUDA(cudaGraphInstantiate(&s.exec[op], s.graph[op], 0));
+        SBF_CUDA(cudaGraphAddMemsetNode(&n_ms, g.graph, &g.n_rec, 1, &ms));
+        SBF_CUDA(cudaGraphAddKernelNode(&g.n_tile, g.graph, &n_ms, 1, &tk));
+        SBF_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
     } else {
-        SBF_CUDA(cudaGraphExecKernelNodeSetParams(s.exec[op], s.n_rec[op], &rk));
-        SBF_CUDA(cudaGraphExecKernelNodeSetParams(s.exec[op], s.n_tile[op], &tk));
+        SBF_CUDA(cudaGraphExecKernelNodeSetParams(g.exec, g.n_rec, &rk));
+        SBF_CUDA(cudaGraphExecKernelNodeSetParams(g.exec, g.n_tile, &tk));
     }
-    SBF_CUDA(cudaGraphLaunch(s.exec[op], st));
+    SBF_CUDA(cudaGraphLaunch(g.exec, st));
     f->launches += 2;
     return SBF_OK;
+}
+
+void ragged_graph_release(RaggedGraph& g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g = RaggedGraph{};
 }
 
 // ---------------------------------------------------------------------------
@@ -425,7 +422,8 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
             const TileParams p = ragged_params(f, query, s.d_seq, b_hi - b_lo, s.d_rng, np,
                                                s.d_tile_rec, s.d_out, r->d_ctl, d_counts);
             if (t.use_graph)
-                SBF_TRY(ragged_graph_launch(f, s, query, p, t.ctas_per_sm, st));
+                SBF_TRY(ragged_graph_launch(f, s.graph[query ? 1 : 0], query, p, t.ctas_per_sm,
+                                            st));
             else
                 SBF_TRY(ragged_launch(f, query, p, t.ctas_per_sm, st));
         } else if (query) {

@@ -337,6 +337,73 @@ int sbf_ragged_autotune(sbf_filter_t* filter, int query, const char* h_seq, uint
 int sbf_ragged_tuning_lookup(const sbf_filter_t* filter, int query, uint64_t len, uint64_t n,
                              sbf_ragged_tuning* out);
 
+/* ---- Request server (no reference counterpart) ------------------------
+ *
+ * Keeps a filter resident and serves insert and query requests from any
+ * number of host threads with continuous batching: a worker thread forms
+ * each batch from the longest run of queued requests of one operation (in
+ * arrival order) that fits max_batch_bytes, admits it when the device
+ * staging ring (staging_bytes, the memory budget) has room and fewer than
+ * max_inflight batches are on the GPU, and runs it as one ragged pass with
+ * uploads, kernels and downloads on separate streams.  Kernels run in
+ * arrival order, so every result equals one-request-at-a-time execution.
+ * While a server runs, its filter must not be used directly. */
+typedef struct sbf_server sbf_server_t;
+
+typedef struct {
+    uint64_t staging_bytes;      /* device staging budget (default 16 GiB) */
+    uint64_t max_batch_bytes;    /* sequence bytes per batch (default 256 MiB) */
+    uint64_t pinned_bytes;       /* pinned host staging (default 1 GiB) */
+    uint32_t max_inflight;       /* batches on the GPU at once (default 16) */
+    uint32_t max_batch_requests; /* 0 = unlimited; 1 = one request per launch */
+    uint32_t use_graph;          /* replay each batch's kernels as a CUDA graph */
+} sbf_server_config;
+
+typedef struct {
+    int status;        /* SBF_OK or the failure */
+    double latency_s;  /* completion - arrival */
+    uint64_t windows;  /* k-mer windows of the request's span */
+    double arrival_s;  /* sbf_server_now() clock */
+    double done_s;
+} sbf_server_request_info;
+
+typedef struct {
+    uint64_t requests, batches, query_windows, insert_windows;
+    double wall_s; /* first arrival to last completion */
+    double p50_s, p99_s, p999_s, max_s, mean_s;
+    double mean_batch_requests;
+    double worker_busy_s;    /* worker time spent staging and launching batches */
+    double admission_wait_s; /* worker time waiting for staging-ring space */
+    double slot_wait_s;      /* worker time waiting for a free in-flight slot with work queued */
+} sbf_server_stats;
+
+/* config NULL = defaults.  Allocates the staging ring and starts the worker
+ * and completion threads. */
+int sbf_server_create(sbf_filter_t* filter, const sbf_server_config* config,
+                      sbf_server_t** out);
+/* Finishes queued work, then stops the threads and frees the server. */
+void sbf_server_destroy(sbf_server_t* server);
+/* The server's clock (seconds, monotonic) for arrival stamps. */
+double sbf_server_now(void);
+/* Queues a request: op 0 = insert, 1 = query.  Records are (offset, bytes)
+ * ranges into `base`, ordered and non-overlapping; the request's span is
+ * [ranges[0].offset, end of ranges[n-1]).  A query writes one byte per
+ * window of the span to out[0 .. span - k] (out_len >= span - k + 1): the
+ * hit of the window starting at base + ranges[0].offset + i is out[i], and
+ * windows not inside one record read 0.  base, ranges and out must stay
+ * valid until the request completes; pinned buffers are copied directly.
+ * arrival <= 0 stamps the request with sbf_server_now().  Returns a ticket. */
+int sbf_server_submit(sbf_server_t* server, int op, const char* base,
+                      const sbf_record_range* ranges, uint64_t n, uint8_t* out, uint64_t out_len,
+                      double arrival, uint64_t* ticket);
+/* Waits for a request (timeout_s <= 0: no limit) and forgets its ticket. */
+int sbf_server_wait(sbf_server_t* server, uint64_t ticket, double timeout_s,
+                    sbf_server_request_info* info);
+/* Waits until every queued request has completed. */
+int sbf_server_drain(sbf_server_t* server);
+/* Latency percentiles and throughput counters since the last reset. */
+int sbf_server_get_stats(sbf_server_t* server, int reset, sbf_server_stats* out);
+
 /* ---- FASTA / FASTQ (filter.cuh:402-786, Fastx.hpp:297-481) ----------- */
 
 /* Record consumer of sbf_fastx_scan: header (without '>'/'@') and sequence
