@@ -692,6 +692,8 @@ def main() -> None:
     ap.add_argument("--server-graph", type=int, default=0, help="c5: graph replay")
     ap.add_argument("--no-serial", action="store_true", help="c5: skip the one-per-launch run")
     ap.add_argument("--rate", type=float, default=0.0, help="c5: offered req/s (default 20k)")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="c3: skip the ragged-batch and served child runs")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0,
                     help="size multiplier for small profiling runs (1.0 = the named config)")
@@ -946,11 +948,65 @@ def main() -> None:
         "gpu_launches": 2 * args.steps,
         "clocks": clock_info,
     }
-    print(json.dumps(line), flush=True)
     f.close()
+    if world == 1 and args.config == "c3" and args.scale == 1.0 and not args.no_forms:
+        # The ragged-batch and served forms of the metric, each measured in a
+        # child process on this GPU once this workload's buffers are freed.
+        del d_genome, d_query, d_out
+        if not args.no_e2e:
+            del h_genome, h_query, h_out, gnp, qnp, onp
+        torch.cuda.synchronize(dev)
+        torch.cuda.empty_cache()
+        line["ragged_batch"] = run_form(["--config", "c4", "--steps", "5", "--warmup", "3"],
+                                        summarize_ragged)
+        line["served"] = run_form(["--config", "c5", "--duration", "2.0"], summarize_served)
+    print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_form(extra: list[str], summarize) -> dict:
+    """Runs bench.py with `extra` arguments in a child process and returns the
+    summary of its JSON line (or the failure)."""
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), *extra]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    except subprocess.TimeoutExpired:
+        return {"error": "timed out", "command": " ".join(extra)}
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return {"error": f"exit {r.returncode}: {r.stderr.strip()[-300:]}",
+                "command": " ".join(extra)}
+    out = summarize(json.loads(lines[-1]))
+    out["command"] = "python bench.py " + " ".join(extra)
+    return out
+
+
+def summarize_ragged(d: dict) -> dict:
+    pl = d.get("plain_per_record") or {}
+    e2e, tuned, rb = d.get("e2e") or {}, d.get("e2e_tuned") or {}, d.get("record_batch_e2e") or {}
+    return {"metric": d["metric"], "workload": d["config"]["workload"],
+            "kmers_per_s": d["value"], "insert_kmers_per_s": d["insert"]["kmers_per_s"],
+            "query_kmers_per_s": d["query"]["kmers_per_s"],
+            "roofline_frac": d["roofline"]["frac"],
+            "plain_per_record_kmers_per_s": pl.get("kmers_per_s"),
+            "speedup_vs_plain_per_record": d.get("speedup_vs_plain"),
+            "plain_hits_identical": pl.get("query_hits_identical_to_ragged"),
+            "e2e_kmers_per_s": e2e.get("value"), "e2e_tuned_kmers_per_s": tuned.get("value"),
+            "record_batch_e2e_kmers_per_s": rb.get("value")}
+
+
+def summarize_served(d: dict) -> dict:
+    sv, one, pl = d["served"], d.get("one_request_per_launch") or {}, d["plain_per_record"]
+    return {"metric": d["metric"], "workload": d["config"]["workload"],
+            "offered_gb_per_s": d["config"]["offered_gb_per_s"],
+            "kmers_per_s": sv["kmers_per_s"], "requests_per_s": sv["requests_per_s"],
+            "latency_ms": sv["latency_ms"], "mean_batch_requests": sv["mean_batch_requests"],
+            "one_request_per_launch": {"requests_per_s": one.get("requests_per_s"),
+                                       "latency_ms": one.get("latency_ms")},
+            "plain_per_record_sustainable_requests_per_s": pl["sustainable_requests_per_s"],
+            "identical_to_one_at_a_time": d.get("identical_to_one_at_a_time")}
 
 
 def run_reference_arm(args, spec, world) -> None:
