@@ -692,6 +692,8 @@ def main() -> None:
     ap.add_argument("--server-graph", type=int, default=0, help="c5: graph replay")
     ap.add_argument("--no-serial", action="store_true", help="c5: skip the one-per-launch run")
     ap.add_argument("--rate", type=float, default=0.0, help="c5: offered req/s (default 20k)")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="reference arm: skip timing the reference GPU path")
     ap.add_argument("--no-forms", action="store_true",
                     help="c3: skip the ragged-batch and served child runs")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -1051,7 +1053,70 @@ def run_reference_arm(args, spec, world) -> None:
         "e2e": {"value": res["value"], "unit": "k-mers/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if not args.no_reference_gpu:
+        line["reference_gpu"] = reference_gpu_run(args, spec)
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_run(args, spec) -> dict:
+    """The unmodified reference cuSBF GPU path (oracle/_ref, compiled from the
+    reference headers) on this workload at full size, device-resident inputs,
+    timed like the main arm: insert_sequence_async over the genome joined with
+    separators, contains_sequence_async over the reads joined with separators."""
+    from oracle.oracle import RefGpu
+
+    if not RefGpu.available():
+        return {"unavailable": "oracle/_ref/libsbf_refgpu.so was not built"}
+    import torch
+
+    from cusbf_b200.synthetic import SEPARATOR, reads_device, uniform_dna
+
+    joined, _, n_ins_valid = build_host_genome(spec, seed=args.seed)
+    dev = torch.device("cuda", 0)
+    d_genome = torch.from_numpy(joined).to(dev)
+    if spec["n_reads"] > 0:
+        rl = spec["read_len"]
+        reads = reads_device(d_genome, spec["n_reads"], rl, seed=args.seed + 7,
+                             sub_rate=spec["sub_rate"], positive_frac=spec["positive_frac"],
+                             device=str(dev))
+        d_query = torch.full((spec["n_reads"], rl + 1), SEPARATOR, dtype=torch.uint8, device=dev)
+        d_query[:, :rl] = reads
+        d_query = d_query.reshape(-1)[:-1].contiguous()
+        del reads
+        n_q_valid = spec["n_reads"] * (rl - K + 1)
+    else:
+        fresh = uniform_dna(spec["fresh_query_bp"], seed=1337, gc=spec["gc"])
+        q_host = np.concatenate([joined, np.frombuffer(b"N", np.uint8), fresh])
+        d_query = torch.from_numpy(q_host).to(dev)
+        n_q_valid = valid_windows(q_host)
+    n_out = max(d_query.numel() - K + 1, 1)
+    d_out = torch.empty(n_out, dtype=torch.uint8, device=dev)
+    ref = RefGpu(int(round(spec["bits_per_kmer"] * n_ins_valid)))
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    ins, qry = [], []
+    for i in range(3 + max(args.steps, 1)):
+        ref.clear(sp)
+        a, b, c = _ev(torch), _ev(torch), _ev(torch)
+        a.record(stream)
+        assert ref.lib.sbf_refgpu_insert_async(ref.h, d_genome.data_ptr(), d_genome.numel(),
+                                               sp) == 0
+        b.record(stream)
+        assert ref.lib.sbf_refgpu_contains_async(ref.h, d_query.data_ptr(), d_query.numel(),
+                                                 d_out.data_ptr(), n_out, sp) == 0
+        c.record(stream)
+        torch.cuda.synchronize(dev)
+        if i >= 3:
+            ins.append(a.elapsed_time(b))
+            qry.append(b.elapsed_time(c))
+    ref.close()
+    ins_ms, q_ms = float(np.mean(ins)), float(np.mean(qry))
+    return {"kmers_per_s": (n_ins_valid + n_q_valid) / ((ins_ms + q_ms) / 1e3),
+            "insert_kmers_per_s": n_ins_valid / (ins_ms / 1e3), "insert_ms": ins_ms,
+            "query_kmers_per_s": n_q_valid / (q_ms / 1e3), "query_ms": q_ms,
+            "steps": len(ins), "warmup": 3,
+            "path": "reference cuSBF filter<Config<31,28,16,4>> insert_sequence_async + "
+                    "contains_sequence_async, device-resident inputs, CUDA events"}
 
 
 if __name__ == "__main__":
