@@ -15,6 +15,9 @@
 namespace {
 using C31 = cusbf::Config<31, 28, 16, 4>;
 using C5 = cusbf::Config<5, 4, 3, 4>;
+using C31H8 = cusbf::Config<31, 28, 16, 8>;
+using C31H16 = cusbf::Config<31, 28, 16, 16>;
+using C21 = cusbf::Config<21, 19, 11, 4>;
 
 struct Handle {
     int cfg;
@@ -28,30 +31,35 @@ template <typename Tag, typename Tag::type Member>
 struct ShardAccess {
     friend typename Tag::type shard_member(Tag) { return Member; }
 };
-struct Shards31 {
-    using type = thrust::device_vector<cusbf::filter_block<C31>> cusbf::filter<C31>::*;
-    friend type shard_member(Shards31);
-};
-struct Shards5 {
-    using type = thrust::device_vector<cusbf::filter_block<C5>> cusbf::filter<C5>::*;
-    friend type shard_member(Shards5);
-};
-template struct ShardAccess<Shards31, &cusbf::filter<C31>::d_shards_>;
-template struct ShardAccess<Shards5, &cusbf::filter<C5>::d_shards_>;
 
-const void* shard_ptr(cusbf::filter<C31>& f) {
-    return thrust::raw_pointer_cast((f.*shard_member(Shards31{})).data());
-}
-const void* shard_ptr(cusbf::filter<C5>& f) {
-    return thrust::raw_pointer_cast((f.*shard_member(Shards5{})).data());
-}
+#define SBF_REF_SHARDS(Tag, Cfg)                                                          \
+    struct Tag {                                                                          \
+        using type = thrust::device_vector<cusbf::filter_block<Cfg>> cusbf::filter<Cfg>::*; \
+        friend type shard_member(Tag);                                                    \
+    };                                                                                    \
+    template struct ShardAccess<Tag, &cusbf::filter<Cfg>::d_shards_>;                     \
+    const void* shard_ptr(cusbf::filter<Cfg>& f) {                                        \
+        return thrust::raw_pointer_cast((f.*shard_member(Tag{})).data());                 \
+    }
 
+SBF_REF_SHARDS(Shards31, C31)
+SBF_REF_SHARDS(Shards5, C5)
+SBF_REF_SHARDS(Shards31H8, C31H8)
+SBF_REF_SHARDS(Shards31H16, C31H16)
+SBF_REF_SHARDS(Shards21, C21)
+
+// Configuration ids as in oracle/oracle.py REF_CONFIGS (DNA alphabet only).
 template <typename Fn>
 int with(Handle* h, Fn&& fn) {
     if (!h) return -1;
-    if (h->cfg == 0) return fn(*static_cast<cusbf::filter<C31>*>(h->f));
-    if (h->cfg == 1) return fn(*static_cast<cusbf::filter<C5>*>(h->f));
-    return -1;
+    switch (h->cfg) {
+        case 0: return fn(*static_cast<cusbf::filter<C31>*>(h->f));
+        case 1: return fn(*static_cast<cusbf::filter<C5>*>(h->f));
+        case 4: return fn(*static_cast<cusbf::filter<C31H8>*>(h->f));
+        case 5: return fn(*static_cast<cusbf::filter<C31H16>*>(h->f));
+        case 6: return fn(*static_cast<cusbf::filter<C21>*>(h->f));
+        default: return -1;
+    }
 }
 }  // namespace
 
@@ -59,8 +67,14 @@ extern "C" {
 
 void* sbf_refgpu_create(int cfg, uint64_t bits) {
     try {
-        if (cfg == 0) return new Handle{0, new cusbf::filter<C31>(bits)};
-        if (cfg == 1) return new Handle{1, new cusbf::filter<C5>(bits)};
+        switch (cfg) {
+            case 0: return new Handle{0, new cusbf::filter<C31>(bits)};
+            case 1: return new Handle{1, new cusbf::filter<C5>(bits)};
+            case 4: return new Handle{4, new cusbf::filter<C31H8>(bits)};
+            case 5: return new Handle{5, new cusbf::filter<C31H16>(bits)};
+            case 6: return new Handle{6, new cusbf::filter<C21>(bits)};
+            default: break;
+        }
     } catch (...) {
     }
     return nullptr;
@@ -69,8 +83,10 @@ void* sbf_refgpu_create(int cfg, uint64_t bits) {
 void sbf_refgpu_destroy(void* p) {
     auto* h = static_cast<Handle*>(p);
     if (!h) return;
-    if (h->cfg == 0) delete static_cast<cusbf::filter<C31>*>(h->f);
-    if (h->cfg == 1) delete static_cast<cusbf::filter<C5>*>(h->f);
+    with(h, [](auto& f) {
+        delete &f;
+        return 0;
+    });
     delete h;
 }
 
