@@ -90,6 +90,24 @@ def build_host_genome(spec: dict, seed: int):
     return joined, ranges, valid
 
 
+def max_over_ranks(values: list[float], dist=None, device="cpu") -> list[float]:
+    """Element-wise maximum of per-rank timings over all ranks (the slowest
+    rank sets the step time); the values themselves for one process."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def whole_job_rate(world: int, units_per_rank: float, ms_per_step: float) -> float:
+    """Weak scaling: every rank processes `units_per_rank` per step, and the
+    step takes the slowest rank's time."""
+    return world * units_per_rank / (ms_per_step / 1e3)
+
+
 def valid_windows(seq: np.ndarray) -> int:
     """Windows of `seq` whose K bases are all A/C/G/T (any case)."""
     up = seq & 0xDF
@@ -311,13 +329,10 @@ def run_ragged(args, world: int, rank: int, local_rank: int) -> None:
     ins_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
     q_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
     ins_valid, q_valid, q_pos = int(ins_counts[0]), int(q_counts[0]), int(q_counts[1])
-    if dist:
-        t = torch.tensor([total_ms, ins_ms, q_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, ins_ms, q_ms = (float(x) for x in t.tolist())
+    total_ms, ins_ms, q_ms = max_over_ranks([total_ms, ins_ms, q_ms], dist, dev)
     ms_per_step = total_ms / args.steps
     kmers_step = ins_valid + q_valid
-    value = world * kmers_step / (ms_per_step / 1e3)
+    value = whole_job_rate(world, kmers_step, ms_per_step)
     ragged_hits = d_out.clone()
 
     # Plain per-record launches on a sample: the first records / reads up to
@@ -820,12 +835,9 @@ def main() -> None:
     kmers_step = n_ins_valid + n_q_valid
 
     # Max over ranks of the timed region; sum of the work.
-    if dist:
-        t = torch.tensor([total_ms, ins_ms, q_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, ins_ms, q_ms = (float(x) for x in t.tolist())
+    total_ms, ins_ms, q_ms = max_over_ranks([total_ms, ins_ms, q_ms], dist, dev)
     ms_per_step = total_ms / args.steps
-    value = world * kmers_step / (ms_per_step / 1e3)
+    value = whole_job_rate(world, kmers_step, ms_per_step)
 
     # Parity spot check of this run against the oracle on a slice.
     positives = int(d_out.sum(dtype=torch.int64).item())
@@ -859,10 +871,7 @@ def main() -> None:
         res = [e2e_step() for _ in range(max(1, args.e2e_steps))]
         e_ms = float(np.mean([r[0] for r in res]))
         e_wall = float(np.mean([r[1] for r in res]))
-        if dist:
-            t = torch.tensor([e_ms, e_wall], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms, e_wall = (float(x) for x in t.tolist())
+        e_ms, e_wall = max_over_ranks([e_ms, e_wall], dist, dev)
         assert int(h_out[:n_q_windows].sum(dtype=torch.int64)) == positives, \
             "host-API query disagrees with the device-resident query"
         e2e = {"value": world * kmers_step / (max(e_ms, e_wall) / 1e3), "unit": "k-mers/s",

@@ -5,23 +5,31 @@
 // and their dense-packed twins).  Results are bit-identical to it; the work
 // decomposition is new:
 //
-//   * A persistent CTA walks tiles of 4096 consecutive windows.  Each tile's
-//     input bytes are staged into shared memory by a 1D bulk async copy (TMA)
-//     on an mbarrier, double-buffered so the next tile's copy overlaps the
-//     current tile's hashing.  Only the 16-byte aligned interior goes through
-//     the bulk copy; ragged edges are read with plain loads, so nothing
-//     outside the caller's buffer is touched.
+//   * A persistent CTA (two per SM) walks tiles of 8192 consecutive windows
+//     (kTileKmers).  Each tile's input bytes are staged into shared memory by
+//     a 1D bulk async copy (TMA) on an mbarrier, double-buffered and issued
+//     two tiles ahead, so copies overlap hashing.  Only the 16-byte aligned
+//     interior goes through the bulk copy; ragged edges are read with plain
+//     loads, so nothing outside the caller's buffer is touched.  Every wait
+//     is bounded and reports kDevErrStageTimeout instead of hanging.
 //   * Staged bytes are encoded with SWAR into 2-bit code words (16 bases per
 //     32-bit word, earliest base in the top bits) plus invalid masks.
-//   * Each thread owns a strip of 16 consecutive windows.  Every m-mer and
-//     s-mer of the strip is one funnel shift of the code words, every
-//     absolute position is hashed once, and the per-window minimizer is a
+//   * Each of the 256 threads owns a strip of 32 consecutive windows.  Every
+//     m-mer and s-mer of the strip is a funnel shift of the code words,
+//     every position is hashed once, and the per-window minimizer is a
 //     Gil-Werman sliding minimum (about 3 comparisons per window instead of
 //     the reference's 16 multiplies).
 //   * Insert merges consecutive windows that select the same shard (a
-//     super-k-mer run) in registers and issues one red.or.b64 per shard word
-//     per run.  Query loads each run's 32-byte shard once with a 256-bit
-//     load and tests the findere rule (all k-s+1 s-mers present).
+//     super-k-mer run) in registers and flushes each run with one 32-byte
+//     bulk OR-reduction (cp.reduce.async.bulk .or.b64) from a per-thread
+//     shared-memory ring: one L2 sector operation per run.
+//   * Query copies each run head's 32-byte shard into per-thread shared
+//     slots with cp.async while the strip's s-mers are hashed, borrows the
+//     left neighbour's staged shard when a run crosses the strip boundary,
+//     and tests the findere rule (all k-s+1 s-mers present) per window.
+//   * Ragged launches take tiles from a device work-queue counter and drop
+//     windows that cross a record boundary or touch a byte outside every
+//     record (marked per tile in shared memory).
 #include <cuda_runtime.h>
 
 #include <cstdint>

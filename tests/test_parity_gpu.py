@@ -3,9 +3,10 @@
 Every case inserts the same seeded bytes into the engine (through the C ABI)
 and into the oracle, then compares the full shard word array, and compares
 every query byte.  Cases cover the tile/strip boundaries of the kernels
-(4096-window tiles, 16-window strips), misaligned input and output pointers,
+(8192-window tiles, 32-window strips), misaligned input and output pointers,
 invalid bases, lower case, tiny filters (heavy shard collisions, so many runs
-hit the same words through atomics), and the other compiled configurations.
+hit the same shard words through bulk OR-reductions), and the other compiled
+configurations.
 """
 import numpy as np
 import pytest
