@@ -93,30 +93,30 @@ static uint64_t host_chunk_bytes() {
 
 int Staging::ensure_device(size_t bytes) {
     if (bytes <= dev_cap) return SBF_OK;
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kPipeSlots; ++i) {
         if (dev[i]) cudaFree(dev[i]);
         dev[i] = nullptr;
     }
     dev_cap = 0;
-    for (int i = 0; i < 2; ++i) SBF_CUDA(cudaMalloc(&dev[i], bytes));
+    for (int i = 0; i < kPipeSlots; ++i) SBF_CUDA(cudaMalloc(&dev[i], bytes));
     dev_cap = bytes;
     return SBF_OK;
 }
 
 int Staging::ensure_pinned(size_t bytes) {
     if (bytes <= pin_cap) return SBF_OK;
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kPipeSlots; ++i) {
         if (pin[i]) cudaFreeHost(pin[i]);
         pin[i] = nullptr;
     }
     pin_cap = 0;
-    for (int i = 0; i < 2; ++i) SBF_CUDA(cudaMallocHost(&pin[i], bytes));
+    for (int i = 0; i < kPipeSlots; ++i) SBF_CUDA(cudaMallocHost(&pin[i], bytes));
     pin_cap = bytes;
     return SBF_OK;
 }
 
 void Staging::release() {
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kPipeSlots; ++i) {
         if (dev[i]) cudaFree(dev[i]);
         if (pin[i]) cudaFreeHost(pin[i]);
         dev[i] = nullptr;
@@ -186,8 +186,8 @@ int sbf_filter::check_device_error(cudaStream_t st) const {
 }
 
 // Host bytes -> device in chunks of whole windows with a (k-1)-symbol overlap,
-// double-buffered: the copy of chunk c+1 (on copy_stream) overlaps the kernel
-// of chunk c (on `st`).  `out_host`/`out_dev` receive query bytes.
+// kPipeSlots chunks in flight: uploads on copy_stream, kernels on `st`,
+// downloads on d2h_stream, so the three overlap across chunks.  `out_host`/`out_dev` receive query bytes.
 int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t in_bytes,
                               uint64_t n_kmers, uint8_t* out_host, uint8_t* out_dev,
                               cudaStream_t st) {
@@ -225,18 +225,24 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
     if (query && out_dev == nullptr) SBF_TRY(stage_out.ensure_device(chunk_kmers));
     if (query && out_host != nullptr && !out_pinned) SBF_TRY(stage_out.ensure_pinned(chunk_kmers));
 
+    // The upload of a chunk waits for nothing but its slot; downloads run on
+    // their own stream, so chunk c+1's kernel never queues behind chunk c's
+    // download.
+    SBF_CUDA(cudaEventRecord(ev_kernel[0], st));
+    SBF_CUDA(cudaStreamWaitEvent(copy_stream, ev_kernel[0], 0));
+    SBF_CUDA(cudaStreamWaitEvent(d2h_stream, ev_kernel[0], 0));
     for (uint64_t c = 0; c < n_chunks; ++c) {
-        const int slot = static_cast<int>(c & 1);
+        const int slot = static_cast<int>(c % kPipeSlots);
         uint64_t first_byte, bytes, kmers, sym_offset;
         chunk_span(c, first_byte, bytes, kmers, sym_offset);
-        // The slot's previous kernel (and output copy) must be finished
-        // before its buffers are reused.
+        // The slot's previous kernel and download must be finished before
+        // its buffers are reused.
         SBF_CUDA(cudaEventSynchronize(ev_done[slot]));
-        if (query && out_host != nullptr && !out_pinned && c >= 2) {
-            // Drain the host output of chunk c-2 which used this slot.
+        if (query && out_host != nullptr && !out_pinned && c >= kPipeSlots) {
+            // Drain the host output of the chunk that used this slot before.
             uint64_t pf, pb, pk, po;
-            chunk_span(c - 2, pf, pb, pk, po);
-            std::memcpy(out_host + (c - 2) * chunk_kmers, stage_out.pin[slot], pk);
+            chunk_span(c - kPipeSlots, pf, pb, pk, po);
+            std::memcpy(out_host + (c - kPipeSlots) * chunk_kmers, stage_out.pin[slot], pk);
         }
         const char* src = static_cast<const char*>(h_in) + first_byte;
         if (!in_pinned) {
@@ -253,22 +259,27 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
                            : static_cast<uint8_t*>(stage_out.dev[slot]);
         }
         SBF_TRY(launch(query, dense, stage_in.dev[slot], bytes, kmers, dout, st));
+        SBF_CUDA(cudaEventRecord(ev_kernel[slot], st));
         if (query && out_host != nullptr) {
             void* hdst = out_pinned ? static_cast<void*>(out_host + c * chunk_kmers)
                                     : stage_out.pin[slot];
-            SBF_CUDA(cudaMemcpyAsync(hdst, dout, kmers, cudaMemcpyDeviceToHost, st));
+            SBF_CUDA(cudaStreamWaitEvent(d2h_stream, ev_kernel[slot], 0));
+            SBF_CUDA(cudaMemcpyAsync(hdst, dout, kmers, cudaMemcpyDeviceToHost, d2h_stream));
+            SBF_CUDA(cudaEventRecord(ev_done[slot], d2h_stream));
+        } else {
+            SBF_CUDA(cudaEventRecord(ev_done[slot], st));
         }
-        // The host waits on this event before reusing the slot (top of the
-        // loop), so the copy of chunk c+2 never overwrites a buffer that a
-        // kernel is still reading, while chunk c+1's copy overlaps this kernel.
-        SBF_CUDA(cudaEventRecord(ev_done[slot], st));
     }
+    // `st` completes after every kernel and download of this call.
+    SBF_CUDA(cudaEventRecord(ev_kernel[0], d2h_stream));
+    SBF_CUDA(cudaStreamWaitEvent(st, ev_kernel[0], 0));
     SBF_CUDA(cudaStreamSynchronize(st));
     if (query && out_host != nullptr && !out_pinned) {
-        for (uint64_t c = (n_chunks >= 2 ? n_chunks - 2 : 0); c < n_chunks; ++c) {
+        const uint64_t first = n_chunks > kPipeSlots ? n_chunks - kPipeSlots : 0;
+        for (uint64_t c = first; c < n_chunks; ++c) {
             uint64_t pf, pb, pk, po;
             chunk_span(c, pf, pb, pk, po);
-            std::memcpy(out_host + c * chunk_kmers, stage_out.pin[c & 1], pk);
+            std::memcpy(out_host + c * chunk_kmers, stage_out.pin[c % kPipeSlots], pk);
         }
     }
     return check_device_error(st);
@@ -346,9 +357,11 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
         e = cudaMemset(f->d_err, 0, 64);
         if (e != cudaSuccess) { rc = cuda_fail(e, "cudaMemset(err)"); break; }
         e = cudaStreamCreateWithFlags(&f->copy_stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&f->d2h_stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) { rc = cuda_fail(e, "cudaStreamCreate"); break; }
-        for (int i = 0; i < 2 && rc == SBF_OK; ++i) {
+        for (int i = 0; i < kPipeSlots && rc == SBF_OK; ++i) {
             e = cudaEventCreateWithFlags(&f->ev_copied[i], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->ev_kernel[i], cudaEventDisableTiming);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f->ev_done[i], cudaEventDisableTiming);
             if (e != cudaSuccess) rc = cuda_fail(e, "cudaEventCreate");
         }
@@ -378,11 +391,13 @@ extern "C" void sbf_filter_destroy(sbf_filter_t* f) {
     f->rb_stats.release();
     if (f->d_words) cudaFree(f->d_words);
     if (f->d_err) cudaFree(f->d_err);
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kPipeSlots; ++i) {
         if (f->ev_copied[i]) cudaEventDestroy(f->ev_copied[i]);
+        if (f->ev_kernel[i]) cudaEventDestroy(f->ev_kernel[i]);
         if (f->ev_done[i]) cudaEventDestroy(f->ev_done[i]);
     }
     if (f->copy_stream) cudaStreamDestroy(f->copy_stream);
+    if (f->d2h_stream) cudaStreamDestroy(f->d2h_stream);
     delete f;
 }
 

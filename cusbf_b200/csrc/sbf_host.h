@@ -19,9 +19,12 @@ bool is_pinned(const void* p);
 
 // A pair of device buffers and a pair of pinned host buffers, grown on
 // demand and reused across calls.
+// Chunks of a host-input call in flight at once (upload, kernel, download).
+constexpr int kPipeSlots = 3;
+
 struct Staging {
-    void* dev[2] = {nullptr, nullptr};
-    void* pin[2] = {nullptr, nullptr};
+    void* dev[kPipeSlots] = {};
+    void* pin[kPipeSlots] = {};
     size_t dev_cap = 0;
     size_t pin_cap = 0;
     int ensure_device(size_t bytes);
@@ -55,9 +58,11 @@ struct sbf_filter {
 
     sbf::Staging stage_in;
     sbf::Staging stage_out;
-    cudaStream_t copy_stream = nullptr;
-    cudaEvent_t ev_copied[2] = {nullptr, nullptr};
-    cudaEvent_t ev_done[2] = {nullptr, nullptr};
+    cudaStream_t copy_stream = nullptr;  // host -> device chunk uploads
+    cudaStream_t d2h_stream = nullptr;   // device -> host result downloads
+    cudaEvent_t ev_copied[sbf::kPipeSlots] = {};
+    cudaEvent_t ev_kernel[sbf::kPipeSlots] = {};
+    cudaEvent_t ev_done[sbf::kPipeSlots] = {};
 
     // Ragged-batch engine state (sbf_ragged.cu), created on first use.
     sbf::RaggedState* ragged = nullptr;
