@@ -108,6 +108,29 @@ def whole_job_rate(world: int, units_per_rank: float, ms_per_step: float) -> flo
     return world * units_per_rank / (ms_per_step / 1e3)
 
 
+def random_sector_rate(words_tensor, torch, n_reads: int = 1 << 26, reps: int = 3) -> float:
+    """Random 32-byte sectors per second that this GPU's memory system
+    serves: torch.take of one 8-byte word from each of `n_reads` uniformly
+    random 32-byte sectors of the filter words (one sector access each),
+    best of `reps`, CUDA events.  The denominator for kernels whose traffic
+    is one random sector per super-k-mer run."""
+    flat = words_tensor.view(torch.int64)
+    g = torch.Generator(device=flat.device).manual_seed(7)
+    idx = torch.randint(0, flat.numel() // 4, (n_reads,), device=flat.device, generator=g) * 4
+    best = None
+    for _ in range(reps + 1):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        out = torch.take(flat, idx)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        best = ms if best is None else min(best, ms)
+        del out
+    return n_reads / (best / 1e3)
+
+
 def valid_windows(seq: np.ndarray) -> int:
     """Windows of `seq` whose K bases are all A/C/G/T (any case)."""
     up = seq & 0xDF
@@ -914,6 +937,14 @@ def main() -> None:
             i_traffic = int(tr["insert_bytes_per_kmer"] * n_ins_valid)
     q_achieved = q_bytes / (q_ms / 1e3) / 1e9
     i_achieved = i_bytes / (ins_ms / 1e3) / 1e9
+    sector_rate = random_sector_rate(f.words(), torch)
+    sector = {"random_32B_sectors_per_s": sector_rate,
+              "calibration": "torch.take of one 8-byte word from each of 2^26 random 32-byte "
+                             "sectors of the filter words, best of 3",
+              "query_runs_per_s": r_per_q * n_q_valid / (q_ms / 1e3),
+              "insert_runs_per_s": r_per_i * n_ins_valid / (ins_ms / 1e3)}
+    sector["query_frac"] = round(sector["query_runs_per_s"] / sector_rate, 4)
+    sector["insert_frac"] = round(sector["insert_runs_per_s"] / sector_rate, 4)
     roofline = {"bound": "hbm", "kernel": "query (tile_kernel<31,28,16,4> query, bytes)",
                 "achieved": round(q_achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(q_achieved / peak, 4), "peak_source": peak_src,
@@ -954,6 +985,7 @@ def main() -> None:
         "query": {"ms": q_ms, "kmers_per_s": n_q_valid / (q_ms / 1e3),
                   "positives": positives},
         "roofline": roofline,
+        "sector_roofline": sector,
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": 2 * args.steps,

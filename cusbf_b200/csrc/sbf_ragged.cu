@@ -68,14 +68,15 @@ struct RaggedSlot {
     size_t tile_cap = 0;
     uint8_t* d_out = nullptr;
     size_t out_cap = 0;
-    cudaEvent_t ev_copied = nullptr, ev_done = nullptr;
+    cudaEvent_t ev_copied = nullptr, ev_kernel = nullptr, ev_done = nullptr;
     bool busy = false;
     RaggedGraph graph[2];  // per operation (insert, query)
 };
 
 struct RaggedState {
     RaggedSlot slot[kMaxStages];
-    cudaStream_t copy_stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // chunk uploads
+    cudaStream_t d2h_stream = nullptr;   // query result downloads
     // [0] work-queue counter; [2..3] (as u64) batch counts.
     unsigned int* d_ctl = nullptr;
     DevBuf direct_tile_rec;
@@ -121,6 +122,7 @@ static void release_slot(RaggedSlot& s) {
     if (s.d_tile_rec) cudaFree(s.d_tile_rec);
     if (s.d_out) cudaFree(s.d_out);
     if (s.ev_copied) cudaEventDestroy(s.ev_copied);
+    if (s.ev_kernel) cudaEventDestroy(s.ev_kernel);
     if (s.ev_done) cudaEventDestroy(s.ev_done);
     for (auto& g : s.graph) ragged_graph_release(g);
     s = RaggedSlot{};
@@ -131,6 +133,7 @@ void ragged_release(sbf_filter* f) {
     RaggedState* r = f->ragged;
     for (auto& s : r->slot) release_slot(s);
     if (r->copy_stream) cudaStreamDestroy(r->copy_stream);
+    if (r->d2h_stream) cudaStreamDestroy(r->d2h_stream);
     if (r->d_ctl) cudaFree(r->d_ctl);
     r->direct_tile_rec.release();
     delete r;
@@ -142,6 +145,7 @@ static int ragged_state(sbf_filter* f, RaggedState** out) {
         auto* r = new RaggedState();
         f->ragged = r;
         cudaError_t e = cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&r->d2h_stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
         if ((e = cudaMalloc(&r->d_ctl, 64)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(ctl)");
         if ((e = cudaMemset(r->d_ctl, 0, 64)) != cudaSuccess) return cuda_fail(e, "cudaMemset(ctl)");
@@ -149,6 +153,8 @@ static int ragged_state(sbf_filter* f, RaggedState** out) {
             if ((e = cudaEventCreateWithFlags(&s.ev_copied, cudaEventDisableTiming)) != cudaSuccess)
                 return cuda_fail(e, "cudaEventCreate");
             if ((e = cudaEventCreateWithFlags(&s.ev_done, cudaEventDisableTiming)) != cudaSuccess)
+                return cuda_fail(e, "cudaEventCreate");
+            if ((e = cudaEventCreateWithFlags(&s.ev_kernel, cudaEventDisableTiming)) != cudaSuccess)
                 return cuda_fail(e, "cudaEventCreate");
         }
     }
@@ -391,6 +397,7 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
     cudaEvent_t ev_start = r->slot[0].ev_done;
     SBF_CUDA(cudaEventRecord(ev_start, st));
     SBF_CUDA(cudaStreamWaitEvent(r->copy_stream, ev_start, 0));
+    SBF_CUDA(cudaStreamWaitEvent(r->d2h_stream, ev_start, 0));
     uint64_t rec = 0;  // first record whose end exceeds the chunk's first byte
     for (uint64_t c = 0; c < n_chunks; ++c) {
         RaggedSlot& s = r->slot[c % S];
@@ -429,13 +436,23 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
         } else if (query) {
             SBF_CUDA(cudaMemsetAsync(s.d_out, 0, w_hi - w_lo, st));
         }
-        if (query)
-            SBF_CUDA(cudaMemcpyAsync(h_out + w_lo, s.d_out, w_hi - w_lo, cudaMemcpyDeviceToHost, st));
-        // The host waits for ev_done before it refills this slot, so the
-        // copy stream itself never waits on kernels.
-        SBF_CUDA(cudaEventRecord(s.ev_done, st));
+        // Downloads run on their own stream so the next chunk's kernel does
+        // not queue behind this chunk's download.  The host waits for
+        // ev_done before it refills this slot, so no stream waits on a later
+        // chunk's work.
+        if (query) {
+            SBF_CUDA(cudaEventRecord(s.ev_kernel, st));
+            SBF_CUDA(cudaStreamWaitEvent(r->d2h_stream, s.ev_kernel, 0));
+            SBF_CUDA(cudaMemcpyAsync(h_out + w_lo, s.d_out, w_hi - w_lo, cudaMemcpyDeviceToHost,
+                                     r->d2h_stream));
+            SBF_CUDA(cudaEventRecord(s.ev_done, r->d2h_stream));
+        } else {
+            SBF_CUDA(cudaEventRecord(s.ev_done, st));
+        }
         s.busy = true;
     }
+    SBF_CUDA(cudaEventRecord(r->slot[0].ev_kernel, r->d2h_stream));
+    SBF_CUDA(cudaStreamWaitEvent(st, r->slot[0].ev_kernel, 0));
     unsigned long long h_counts[2] = {0, 0};
     SBF_CUDA(cudaMemcpyAsync(h_counts, d_counts, sizeof h_counts, cudaMemcpyDeviceToHost, st));
     SBF_CUDA(cudaStreamSynchronize(st));
