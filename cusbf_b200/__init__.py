@@ -249,6 +249,12 @@ _sig("sbf_server_submit", C.c_int, _vp, C.c_int, _vp, _vp, _u64, _vp, _u64, C.c_
 _sig("sbf_server_wait", C.c_int, _vp, _u64, C.c_double, C.POINTER(ServerRequestInfo))
 _sig("sbf_server_drain", C.c_int, _vp)
 _sig("sbf_server_get_stats", C.c_int, _vp, C.c_int, C.POINTER(ServerStats))
+_sig("sbf_contains_sequence_bits_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp)
+_sig("sbf_contains_sequence_bits", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp)
+_sig("sbf_filter_save", C.c_int, _vp, C.c_char_p, _vp)
+_sig("sbf_filter_file_info", C.c_int, C.c_char_p, C.POINTER(_u32), C.POINTER(_u32),
+     C.POINTER(_u32), C.POINTER(_u32), C.POINTER(_u64))
+_sig("sbf_filter_load", C.c_int, _vp, C.c_char_p, _vp)
 _sig("sbf_record_batch_counts_noalloc", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _vp,
      _vp, _vp)
 _sig("sbf_fastx_scan", C.c_int, READ_FN, _vp, C.c_char_p, SCAN_CB, _vp, C.POINTER(_u64))
@@ -598,6 +604,52 @@ def _tuning(t):
     if isinstance(t, RaggedTuning):
         return C.byref(t)
     return C.byref(RaggedTuning(**t))
+
+
+def _persist_methods():
+    """Filter persistence (sbf_filter_save / sbf_filter_load)."""
+
+    def save(self, path, stream=None) -> None:
+        _check(_lib.sbf_filter_save(self._h, os.fsencode(path), _stream(stream)))
+
+    def load_words(self, path, stream=None) -> None:
+        """Replaces this filter's words with a saved filter of the same
+        configuration and size."""
+        _check(_lib.sbf_filter_load(self._h, os.fsencode(path), _stream(stream)))
+
+    def load(cls, path, stream=None) -> "Filter":
+        """A new filter holding a saved filter."""
+        k, s, m, h, bits = _u32(), _u32(), _u32(), _u32(), _u64()
+        _check(_lib.sbf_filter_file_info(os.fsencode(path), C.byref(k), C.byref(s), C.byref(m),
+                                         C.byref(h), C.byref(bits)))
+        f = cls(bits.value, k=k.value, s=s.value, m=m.value, hashes=h.value)
+        f.load_words(path, stream)
+        return f
+
+    def contains_sequence_bits_async(self, d_seq, d_bits, stream=None) -> None:
+        """Bit-packed query of device bytes into a device int32/uint32 tensor:
+        bit i % 32 of word i // 32 is window i's hit."""
+        p, n = _dev_ptr(d_seq)
+        o, on = _dev_ptr(d_bits)
+        _check(_lib.sbf_contains_sequence_bits_async(self._h, p, n, o, on // 4, _stream(stream)))
+
+    def contains_sequence_bits(self, seq, out=None, stream=None) -> np.ndarray:
+        """Bit-packed query of host bytes; returns uint32 words."""
+        b = _host_bytes(seq)
+        n_words = (self.kmer_count(b.size) + 31) // 32
+        o = np.zeros(max(n_words, 1), np.uint32) if out is None else out
+        _check(_lib.sbf_contains_sequence_bits(self._h, _np_ptr(b), b.size, _np_ptr(o), o.size,
+                                               _stream(stream)))
+        return o[:n_words]
+
+    Filter.contains_sequence_bits_async = contains_sequence_bits_async
+    Filter.contains_sequence_bits = contains_sequence_bits
+    Filter.save = save
+    Filter.load_words = load_words
+    Filter.load = classmethod(load)
+
+
+_persist_methods()
 
 
 def _ragged_methods():

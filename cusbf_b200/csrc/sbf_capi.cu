@@ -141,23 +141,28 @@ uint64_t sbf_filter::kmers_of(uint64_t symbols) const {
 }
 
 int sbf_filter::launch(bool query, bool dense, const void* input, uint64_t input_bytes,
-                       uint64_t n_kmers, uint8_t* out, cudaStream_t st) const {
+                       uint64_t n_kmers, uint8_t* out, cudaStream_t st,
+                       uint32_t* out_bits) const {
     if (n_kmers == 0) return SBF_OK;
     TileParams p{};
     p.input = static_cast<const uint8_t*>(input);
     p.input_bytes = input_bytes;
     p.n_kmers = n_kmers;
-    // Grid phase: aligns query output strips (16 windows) to 16 bytes, or the
-    // staged input to 16 bytes for inserts.
+    // Grid phase: aligns query output strips to 16 bytes, or the staged input
+    // to 16 bytes for inserts; bit-packed queries keep phase 0 so that every
+    // strip starts at a multiple of 32 windows.
     int64_t phase = 0;
-    if (query)
+    if (query && out_bits)
+        phase = 0;
+    else if (query)
         phase = static_cast<int64_t>(reinterpret_cast<uintptr_t>(out) & 15u);
     else if (!dense)
         phase = static_cast<int64_t>(reinterpret_cast<uintptr_t>(input) & 15u);
     p.sym_base = -phase;
     p.words = d_words;
     p.shard_mask = static_cast<uint32_t>(num_shards - 1);
-    p.out = out;
+    p.out = out_bits ? nullptr : out;
+    p.out_bits = out_bits;
     p.n_tiles = (n_kmers + static_cast<uint64_t>(phase) + kTileKmers - 1) / kTileKmers;
     p.err = d_err;
     const int which = (query ? 1 : 0) + (dense ? 2 : 0);
@@ -190,7 +195,11 @@ int sbf_filter::check_device_error(cudaStream_t st) const {
 // downloads on d2h_stream, so the three overlap across chunks.  `out_host`/`out_dev` receive query bytes.
 int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t in_bytes,
                               uint64_t n_kmers, uint8_t* out_host, uint8_t* out_dev,
-                              cudaStream_t st) {
+                              cudaStream_t st, uint32_t* bits_host) {
+    // Bit-packed results (bits_host) are written as bytes of 32-bit words:
+    // chunks hold a multiple of 32 windows, so chunk c's words start at word
+    // c * chunk_kmers / 32.
+    const bool bits = bits_host != nullptr;
     if (n_kmers == 0) return SBF_OK;
     // Symbols <-> bytes: byte input has one byte per symbol; dense input has
     // 32 symbols per 8-byte word, so chunks are cut at word boundaries.
@@ -199,7 +208,7 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
     if (dense) {
         chunk_kmers = std::max<uint64_t>((chunk_target * 4) / 32 * 32, 1024);
     } else {
-        chunk_kmers = chunk_target;
+        chunk_kmers = bits ? std::max<uint64_t>(chunk_target / 32 * 32, 1024) : chunk_target;
     }
     const uint64_t n_chunks = (n_kmers + chunk_kmers - 1) / chunk_kmers;
     auto chunk_span = [&](uint64_t c, uint64_t& first_byte, uint64_t& bytes, uint64_t& kmers,
@@ -219,11 +228,16 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
     };
     const uint64_t max_in = dense ? ((chunk_kmers + k - 1 + 31) / 32) * 8 + 8 : chunk_kmers + k;
     const bool in_pinned = is_pinned(h_in);
+    if (bits) out_host = reinterpret_cast<uint8_t*>(bits_host);
+    // Output bytes of a chunk of `kmers` windows, and the chunk's output offset.
+    auto out_size = [&](uint64_t kmers) { return bits ? (kmers + 31) / 32 * 4 : kmers; };
+    auto out_offset = [&](uint64_t c) { return bits ? c * chunk_kmers / 8 : c * chunk_kmers; };
     const bool out_pinned = out_host != nullptr && is_pinned(out_host);
     SBF_TRY(stage_in.ensure_device(max_in));
     if (!in_pinned) SBF_TRY(stage_in.ensure_pinned(max_in));
-    if (query && out_dev == nullptr) SBF_TRY(stage_out.ensure_device(chunk_kmers));
-    if (query && out_host != nullptr && !out_pinned) SBF_TRY(stage_out.ensure_pinned(chunk_kmers));
+    if (query && out_dev == nullptr) SBF_TRY(stage_out.ensure_device(out_size(chunk_kmers)));
+    if (query && out_host != nullptr && !out_pinned)
+        SBF_TRY(stage_out.ensure_pinned(out_size(chunk_kmers)));
 
     // The upload of a chunk waits for nothing but its slot; downloads run on
     // their own stream, so chunk c+1's kernel never queues behind chunk c's
@@ -242,7 +256,7 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
             // Drain the host output of the chunk that used this slot before.
             uint64_t pf, pb, pk, po;
             chunk_span(c - kPipeSlots, pf, pb, pk, po);
-            std::memcpy(out_host + (c - kPipeSlots) * chunk_kmers, stage_out.pin[slot], pk);
+            std::memcpy(out_host + out_offset(c - kPipeSlots), stage_out.pin[slot], out_size(pk));
         }
         const char* src = static_cast<const char*>(h_in) + first_byte;
         if (!in_pinned) {
@@ -258,13 +272,15 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
             dout = out_dev ? out_dev + c * chunk_kmers
                            : static_cast<uint8_t*>(stage_out.dev[slot]);
         }
-        SBF_TRY(launch(query, dense, stage_in.dev[slot], bytes, kmers, dout, st));
+        SBF_TRY(launch(query, dense, stage_in.dev[slot], bytes, kmers, bits ? nullptr : dout, st,
+                       bits ? reinterpret_cast<uint32_t*>(dout) : nullptr));
         SBF_CUDA(cudaEventRecord(ev_kernel[slot], st));
         if (query && out_host != nullptr) {
-            void* hdst = out_pinned ? static_cast<void*>(out_host + c * chunk_kmers)
+            void* hdst = out_pinned ? static_cast<void*>(out_host + out_offset(c))
                                     : stage_out.pin[slot];
             SBF_CUDA(cudaStreamWaitEvent(d2h_stream, ev_kernel[slot], 0));
-            SBF_CUDA(cudaMemcpyAsync(hdst, dout, kmers, cudaMemcpyDeviceToHost, d2h_stream));
+            SBF_CUDA(cudaMemcpyAsync(hdst, dout, out_size(kmers), cudaMemcpyDeviceToHost,
+                                     d2h_stream));
             SBF_CUDA(cudaEventRecord(ev_done[slot], d2h_stream));
         } else {
             SBF_CUDA(cudaEventRecord(ev_done[slot], st));
@@ -279,7 +295,7 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
         for (uint64_t c = first; c < n_chunks; ++c) {
             uint64_t pf, pb, pk, po;
             chunk_span(c, pf, pb, pk, po);
-            std::memcpy(out_host + c * chunk_kmers, stage_out.pin[c % kPipeSlots], pk);
+            std::memcpy(out_host + out_offset(c), stage_out.pin[c % kPipeSlots], out_size(pk));
         }
     }
     return check_device_error(st);
@@ -490,6 +506,37 @@ extern "C" int sbf_contains_sequence(const sbf_filter_t* f, const char* h_seq, u
     if (out_len < n) return set_error(SBF_ERR_INVALID_ARGUMENT, "query output span is too small");
     return const_cast<sbf_filter*>(f)->host_pipeline(true, false, h_seq, bytes, n, h_out, nullptr,
                                                      S(stream));
+}
+
+// ---- bit-packed query results (no reference counterpart) ------------------------
+
+extern "C" int sbf_contains_sequence_bits_async(const sbf_filter_t* f, const char* d_seq,
+                                                uint64_t bytes, uint32_t* d_bits,
+                                                uint64_t n_words, sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    const uint64_t n = f->kmers_of(bytes);
+    if (n == 0) return SBF_OK;
+    if (!d_seq || !d_bits) return set_error(SBF_ERR_INVALID_ARGUMENT, "null device pointer");
+    if (reinterpret_cast<uintptr_t>(d_bits) & 3u)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "bit output must be 4-byte aligned");
+    if (n_words < (n + 31) / 32)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "bit output span is too small (%llu < %llu words)",
+                         static_cast<unsigned long long>(n_words),
+                         static_cast<unsigned long long>((n + 31) / 32));
+    return f->launch(true, false, d_seq, bytes, n, nullptr, S(stream), d_bits);
+}
+
+extern "C" int sbf_contains_sequence_bits(const sbf_filter_t* f, const char* h_seq,
+                                          uint64_t bytes, uint32_t* h_bits, uint64_t n_words,
+                                          sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    const uint64_t n = f->kmers_of(bytes);
+    if (n == 0) return SBF_OK;
+    if (!h_seq || !h_bits) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    if (n_words < (n + 31) / 32)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "bit output span is too small");
+    return const_cast<sbf_filter*>(f)->host_pipeline(true, false, h_seq, bytes, n, nullptr,
+                                                     nullptr, S(stream), h_bits);
 }
 
 // ---- dense input --------------------------------------------------------------

@@ -77,9 +77,10 @@ struct sbf_filter {
                      cudaStream_t st, std::vector<uint64_t>& valid,
                      std::vector<uint64_t>& positive);
     int launch(bool query, bool dense, const void* input, uint64_t input_bytes, uint64_t n_kmers,
-               uint8_t* out, cudaStream_t st) const;
+               uint8_t* out, cudaStream_t st, uint32_t* out_bits = nullptr) const;
     int host_pipeline(bool query, bool dense, const void* h_in, uint64_t in_bytes,
-                      uint64_t n_kmers, uint8_t* out_host, uint8_t* out_dev, cudaStream_t st);
+                      uint64_t n_kmers, uint8_t* out_host, uint8_t* out_dev, cudaStream_t st,
+                      uint32_t* bits_host = nullptr);
     int check_device_error(cudaStream_t st) const;
 };
 

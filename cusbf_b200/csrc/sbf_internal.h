@@ -37,7 +37,8 @@ struct TileParams {
     int64_t sym_base;        // symbol index of grid position 0 (= -phase)
     uint64_t* words;         // filter: num_shards * 4 words
     uint32_t shard_mask;     // (uint32_t)(num_shards - 1)
-    uint8_t* out;            // query: one byte per window
+    uint8_t* out;            // query: one byte per window (null in bit-packed mode)
+    uint32_t* out_bits;      // query, bit-packed mode: bit i % 32 of word i / 32
     uint64_t n_tiles;
     int* err;                // device error word (non-zero = failure code)
     // Ragged launches only.  Records sorted by offset and non-overlapping; a

@@ -535,7 +535,7 @@ __device__ __forceinline__ uint32_t query_strip(const uint32_t* c, uint32_t vmas
         cp_async_wait_all();
         __syncwarp();
         const uint32_t direct = query_strip_direct<C>(c, vmask, shard_mask, words);
-        store_strip_bytes(direct, out, first_kmer, n_kmers);
+        if (out) store_strip_bytes(direct, out, first_kmer, n_kmers);
         return direct;
     }
     // Hash the strip's s-mers while the shard copies are in flight.
@@ -601,7 +601,7 @@ __device__ __forceinline__ uint32_t query_strip(const uint32_t* c, uint32_t vmas
         }
         result |= (present & 1u) << j;
     }
-    store_strip_bytes(result, out, first_kmer, n_kmers);
+    if (out) store_strip_bytes(result, out, first_kmer, n_kmers);
     return result;
 }
 
@@ -771,6 +771,10 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
                                reinterpret_cast<uint32_t*>(slots + kSlots * kThreads * 4) + tid,
                                p.out, first_kmer, p.n_kmers);
             if constexpr (kRagged) n_pos += __popc(hits & vmask);
+            // Bit-packed mode (grid phase 0, so strips start at multiples of
+            // 32 windows): one 32-bit word per strip, coalesced across the warp.
+            if (p.out_bits && first_kmer < static_cast<int64_t>(p.n_kmers))
+                p.out_bits[first_kmer >> 5] = hits;
         } else {
             if (vmask) insert_strip<C>(c, vmask, p.shard_mask, p.words, ring);
         }

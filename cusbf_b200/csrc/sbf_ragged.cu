@@ -600,25 +600,44 @@ extern "C" int sbf_ragged_autotune(sbf_filter_t* f, int query, const char* h_seq
     const uint32_t graph_opts[] = {0, 1};
     sbf_ragged_tuning best = default_tuning();
     double best_ms = 1e300;
+    auto time_one = [&](const sbf_ragged_tuning& t, double* ms_out) -> int {
+        unsigned long long counts[2];
+        double ms = 1e300;
+        for (int rep = 0; rep < 2; ++rep) {  // the first run warms buffers and graphs
+            const auto t0 = std::chrono::steady_clock::now();
+            SBF_TRY(ragged_pipeline(f, query != 0, h_seq, sl, sr.data(), sn, t, S_(stream),
+                                    out.data(), counts));
+            const auto t1 = std::chrono::steady_clock::now();
+            ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        }
+        *ms_out = ms;
+        return SBF_OK;
+    };
+    // Chunk length x staging depth x graph replay, at the occupancy limit.
     for (uint64_t cb : chunks) {
         if (cb > 2 * sl && cb != chunks[0]) continue;  // larger chunks only repeat the smaller
         for (uint32_t stg : stage_opts)
             for (uint32_t gr : graph_opts) {
-                sbf_ragged_tuning t{cb, stg, 0, gr};
-                unsigned long long counts[2];
-                double ms = 1e300;
-                for (int rep = 0; rep < 2; ++rep) {  // first run warms buffers and graphs
-                    const auto t0 = std::chrono::steady_clock::now();
-                    SBF_TRY(ragged_pipeline(f, query != 0, h_seq, sl, sr.data(), sn, t,
-                                            S_(stream), out.data(), counts));
-                    const auto t1 = std::chrono::steady_clock::now();
-                    ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-                }
+                const sbf_ragged_tuning t{cb, stg, 0, gr};
+                double ms;
+                SBF_TRY(time_one(t, &ms));
                 if (ms < best_ms) {
                     best_ms = ms;
                     best = t;
                 }
             }
+    }
+    // Warps per SM for the winner: one CTA (8 warps) instead of the
+    // occupancy limit, which leaves SM room for concurrent work.
+    {
+        sbf_ragged_tuning t = best;
+        t.ctas_per_sm = 1;
+        double ms;
+        SBF_TRY(time_one(t, &ms));
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = t;
+        }
     }
     tune_store(tune_key(f, query != 0, len, n), best, best_ms);
     if (chosen) *chosen = best;

@@ -165,6 +165,31 @@ int sbf_filter_load_factor(sbf_filter_t* filter, sbf_stream_t stream, double* ou
 /* Windows of a byte sequence of `bytes` bytes (symbols - k + 1, or 0). */
 uint64_t sbf_filter_kmer_count(const sbf_filter_t* filter, uint64_t bytes);
 
+/* ---- bit-packed query results (no reference counterpart) ----------------
+ * The same answers as sbf_contains_sequence*, one bit per window: bit i % 32
+ * of word i / 32 is window i's hit (bits past the last window are 0), an 8x
+ * smaller result to store or copy back.  n_words >= ceil(windows / 32). */
+int sbf_contains_sequence_bits_async(const sbf_filter_t* filter, const char* d_seq,
+                                     uint64_t bytes, uint32_t* d_bits, uint64_t n_words,
+                                     sbf_stream_t stream);
+/* Host input and host bit output through the pinned chunk pipeline. */
+int sbf_contains_sequence_bits(const sbf_filter_t* filter, const char* h_seq, uint64_t bytes,
+                               uint32_t* h_bits, uint64_t n_words, sbf_stream_t stream);
+
+/* ---- persistence (no reference counterpart) ------------------------------
+ * A saved filter is a 40-byte header (magic "SBFB200", version, k, s, m,
+ * hashes, alphabet, shard count) followed by the shard words in the
+ * reference's filter_block layout.  Synchronous on `stream`. */
+int sbf_filter_save(const sbf_filter_t* filter, const char* path, sbf_stream_t stream);
+/* Configuration and size of a saved filter (to create a matching filter). */
+int sbf_filter_file_info(const char* path, uint32_t* k, uint32_t* s, uint32_t* m,
+                         uint32_t* hashes, uint64_t* filter_bits);
+/* Replaces the filter's words with a saved filter of the same configuration
+ * and shard count; on any error the filter is left unchanged
+ * (SBF_ERR_IO: unreadable or malformed file; SBF_ERR_INVALID_ARGUMENT:
+ * another configuration or size). */
+int sbf_filter_load(sbf_filter_t* filter, const char* path, sbf_stream_t stream);
+
 /* ---- byte sequences -------------------------------------------------- */
 
 /* insert_sequence_async (filter.cuh:179-190): device bytes; `kmers_out`
@@ -324,7 +349,8 @@ int sbf_ragged_query(const sbf_filter_t* filter, const char* h_seq, uint64_t len
                      const sbf_record_range* ranges, uint64_t n, uint8_t* h_out,
                      uint64_t out_len, const sbf_ragged_tuning* tuning, sbf_stream_t stream,
                      sbf_query_report* report);
-/* Times chunk size x stages x graph replay on a prefix of the batch
+/* Times chunk size x stages x graph replay, then CTAs per SM for the
+ * winner, on a prefix of the batch
  * (sample_bytes, 0 = 256 MiB), stores the fastest in the tuning table
  * (SBF_TUNE_TABLE, default $HOME/.cache/cusbf_b200/ragged_tuning.tsv) under
  * the batch's shape (operation, configuration, log2 bytes, log2 mean record
