@@ -589,7 +589,12 @@ def run_served(args, world: int, rank: int, local_rank: int) -> None:
     out_ring = torch.empty(out_ring_bytes, dtype=torch.uint8).pin_memory()
     out_np = out_ring.numpy()
     check_idx = set(range(0, n_req, max(1, n_req // 64)))
-    check_out = {i: np.zeros(max(int(n_reads[i]) * read_len - K + 1, 1), np.uint8)
+    op_q = 2 if args.server_bits else 1
+
+    def result_bytes(w):
+        return 4 * ((w + 31) // 32) if op_q == 2 else w
+
+    check_out = {i: np.zeros(max(result_bytes(int(n_reads[i]) * read_len - K + 1), 1), np.uint8)
                  for i in check_idx if not is_ins[i]}
     ins_range_t = torch.empty((n_req, 2), dtype=torch.int64).pin_memory()
     ins_range = ins_range_t.numpy().view(np.uint64)
@@ -611,7 +616,7 @@ def run_served(args, world: int, rank: int, local_rank: int) -> None:
                                arrival)
             else:
                 nr = int(n_reads[i])
-                w = nr * read_len - K + 1
+                w = result_bytes(nr * read_len - K + 1)
                 if i in check_out:
                     optr = check_out[i].ctypes.data
                 else:
@@ -622,8 +627,8 @@ def run_served(args, world: int, rank: int, local_rank: int) -> None:
                         srv.wait(ring_live.pop(0)[0])
                     optr = out_np.ctypes.data + lo
                     ring_pos = hi
-                t = srv.submit_raw(1, pool_np.ctypes.data, rng_np.ctypes.data + 16 * int(first[i]),
-                                   nr, optr, w, arrival)
+                t = srv.submit_raw(op_q, pool_np.ctypes.data,
+                                   rng_np.ctypes.data + 16 * int(first[i]), nr, optr, w, arrival)
                 if i not in check_out:
                     ring_live.append((t, lo, hi))
                     while len(ring_live) > 4096:
@@ -697,6 +702,7 @@ def run_served(args, world: int, rank: int, local_rank: int) -> None:
         "data": "synthetic (seeded Poisson request stream over seeded reads and sequences)",
         "config": {"workload": f"served: {n_req:,} requests over {duration:.1f} s at "
                                f"{rate:.0f} req/s, filter of the 100 Mbp genome resident",
+                   "query_results": "bit-packed (op 2)" if op_q == 2 else "one byte per window",
                    "k": K, "s": S, "m": M, "hashes": H, "filter_bits": bits,
                    "staging_budget_bytes": 16 << 30, "offered_bytes": int(offered),
                    "offered_gb_per_s": offered / duration / 1e9,
@@ -729,6 +735,8 @@ def main() -> None:
     ap.add_argument("--server-batch-mb", type=int, default=0, help="c5: batch cap in MiB")
     ap.add_argument("--server-graph", type=int, default=0, help="c5: graph replay")
     ap.add_argument("--no-serial", action="store_true", help="c5: skip the one-per-launch run")
+    ap.add_argument("--server-bits", action="store_true",
+                    help="c5: queries ask for bit-packed results")
     ap.add_argument("--rate", type=float, default=0.0, help="c5: offered req/s (default 20k)")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip timing the reference GPU path")
@@ -866,7 +874,7 @@ def main() -> None:
     positives = int(d_out.sum(dtype=torch.int64).item())
 
     # End-to-end through the host API with pinned buffers.
-    e2e = None
+    e2e = e2e_bits = None
     if not args.no_e2e:
         h_genome = torch.from_numpy(joined).pin_memory()
         h_query = torch.empty(d_query.numel(), dtype=torch.uint8).pin_memory()
@@ -902,6 +910,32 @@ def main() -> None:
                "d2h_bytes_per_step": int(n_q_windows), "ms_per_step": max(e_ms, e_wall),
                "steps": len(res),
                "api": "sbf_insert_sequence + sbf_contains_sequence (host buffers, pinned)"}
+        # The same step with bit-packed results (one bit per window).
+        n_words = (n_q_windows + 31) // 32
+        h_bits = torch.empty(max(n_words, 1), dtype=torch.int32).pin_memory()
+        bnp = h_bits.numpy()
+
+        def e2e_bits_step():
+            f.clear(stream)
+            torch.cuda.synchronize(dev)
+            w0 = time.perf_counter()
+            f.insert_sequence(gnp, stream)
+            sbf._check(sbf._lib.sbf_contains_sequence_bits(f.handle, qnp.ctypes.data, qnp.size,
+                                                            bnp.ctypes.data, n_words,
+                                                            stream.cuda_stream))
+            return (time.perf_counter() - w0) * 1e3
+
+        e2e_bits_step()
+        b_ms = float(np.mean([e2e_bits_step() for _ in range(max(1, args.e2e_steps))]))
+        (b_ms,) = max_over_ranks([b_ms], dist, dev)
+        got_pos = int(np.unpackbits(bnp.view(np.uint8), bitorder="little")[:n_q_windows].sum())
+        assert got_pos == positives, "bit-packed query disagrees with the byte query"
+        e2e_bits = {"value": world * kmers_step / (b_ms / 1e3), "unit": "k-mers/s",
+                    "h2d_bytes_per_step": int(joined.size + qnp.size),
+                    "d2h_bytes_per_step": int(4 * n_words), "ms_per_step": b_ms,
+                    "api": "sbf_insert_sequence + sbf_contains_sequence_bits (host buffers, "
+                           "pinned; one result bit per window)"}
+        del h_bits, bnp
 
     if rank != 0:
         if dist:
@@ -988,6 +1022,7 @@ def main() -> None:
         "sector_roofline": sector,
         "cpu_baseline": cpu,
         "e2e": e2e,
+        "e2e_bits": e2e_bits,
         "gpu_launches": 2 * args.steps,
         "clocks": clock_info,
     }
@@ -1003,6 +1038,8 @@ def main() -> None:
         line["ragged_batch"] = run_form(["--config", "c4", "--steps", "5", "--warmup", "3"],
                                         summarize_ragged)
         line["served"] = run_form(["--config", "c5", "--duration", "2.0"], summarize_served)
+        line["served_bits"] = run_form(["--config", "c5", "--duration", "2.0", "--server-bits",
+                                        "--no-serial"], summarize_served)
     print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

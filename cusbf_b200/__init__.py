@@ -897,7 +897,7 @@ class Server:
     result equals one-request-at-a-time execution in arrival order.  While it
     runs, the filter must not be used directly."""
 
-    INSERT, QUERY = 0, 1
+    INSERT, QUERY, QUERY_BITS = 0, 1, 2
 
     def __init__(self, filt: "Filter", **config):
         self._filter = filt
@@ -924,12 +924,14 @@ class Server:
         b = _host_bytes(base)
         r = _ranges(ranges)
         o = out
-        if op == self.QUERY and o is None:
+        if op != self.INSERT and o is None:
             span = max(int(r[-1, 0] + r[-1, 1]) - int(r[0, 0]), 0) if r.shape[0] else 0
-            o = np.zeros(max(self._filter.kmer_count(span), 1), np.uint8)
+            w = self._filter.kmer_count(span)
+            o = (np.zeros(max(w, 1), np.uint8) if op == self.QUERY
+                 else np.zeros(max((w + 31) // 32, 1), np.uint32))
         t = self.submit_raw(op, _np_ptr(b), _np_ptr(r), r.shape[0],
                             _np_ptr(o) if o is not None else None,
-                            o.size if o is not None else 0, arrival)
+                            o.nbytes if o is not None else 0, arrival)
         with self._lock:
             self._refs[t] = (b, r, o)
         return t
@@ -949,7 +951,8 @@ class Server:
         _check(st)
         out = None
         if refs is not None and refs[2] is not None:
-            out = refs[2][:info.windows]
+            o = refs[2]
+            out = o[:info.windows] if o.dtype == np.uint8 else o[:(info.windows + 31) // 32]
         return info.as_dict(), out
 
     def drain(self) -> None:

@@ -169,20 +169,23 @@ static unsigned long long* ctl_counts(RaggedState* r) {
 TileParams ragged_params(const sbf_filter* f, bool query, const uint8_t* d_seq,
                                 uint64_t len, const DevRange* d_rng, uint64_t n,
                                 const uint32_t* d_tile_rec, uint8_t* d_out, unsigned int* queue,
-                                unsigned long long* counts) {
+                                unsigned long long* counts, bool out_bits) {
     TileParams p{};
     p.input = d_seq;
     p.input_bytes = len;
     p.n_kmers = f->kmers_of(len);
     int64_t phase = 0;
-    if (query)
+    if (query && out_bits)
+        phase = 0;  // strips start at multiples of 32 windows
+    else if (query)
         phase = static_cast<int64_t>(reinterpret_cast<uintptr_t>(d_out) & 15u);
     else
         phase = static_cast<int64_t>(reinterpret_cast<uintptr_t>(d_seq) & 15u);
     p.sym_base = -phase;
     p.words = f->d_words;
     p.shard_mask = static_cast<uint32_t>(f->num_shards - 1);
-    p.out = d_out;
+    p.out = out_bits ? nullptr : d_out;
+    p.out_bits = out_bits ? reinterpret_cast<uint32_t*>(d_out) : nullptr;
     p.n_tiles = (p.n_kmers + static_cast<uint64_t>(phase) + kTileKmers - 1) / kTileKmers;
     p.err = f->d_err;
     p.ranges = d_rng;

@@ -11,10 +11,13 @@
 
 namespace sbf {
 
-// Kernel parameters of one ragged launch over `len` bytes at d_seq.
+// Kernel parameters of one ragged launch over `len` bytes at d_seq.  With
+// out_bits, query results are bit-packed 32-bit words at d_out (window i ->
+// bit i % 32 of word i / 32).
 TileParams ragged_params(const sbf_filter* f, bool query, const uint8_t* d_seq, uint64_t len,
                          const DevRange* d_rng, uint64_t n, const uint32_t* d_tile_rec,
-                         uint8_t* d_out, unsigned int* queue, unsigned long long* counts);
+                         uint8_t* d_out, unsigned int* queue, unsigned long long* counts,
+                         bool out_bits = false);
 
 // Stream launch of one ragged pass: tile records, queue reset, tile kernel.
 int ragged_launch(sbf_filter* f, bool query, const TileParams& p, uint32_t ctas,

@@ -53,6 +53,15 @@ constexpr uint64_t kDirectBytes = 256 << 10;  // pinned spans at least this size
 
 uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
+// Operations: 0 insert, 1 query (one byte per window), 2 query with
+// bit-packed results.  Bit-packed requests start at multiples of 32 bytes
+// of the batch, so each request's bits start on a word boundary.
+constexpr int kOpInsert = 0, kOpQuery = 1, kOpQueryBits = 2;
+uint64_t pad_of(int op) { return op == kOpQueryBits ? 32 : 16; }
+uint64_t result_bytes(int op, uint64_t windows) {
+    return op == kOpQueryBits ? (windows + 31) / 32 * 4 : op == kOpQuery ? windows : 0;
+}
+
 // FIFO ring allocator: regions are released in allocation order.  The
 // live regions occupy [tail, head) when head > tail and wrap around the end
 // of the ring otherwise; a region never straddles the end.
@@ -183,7 +192,7 @@ void Server::complete(SrvBatch* b, int status) {
         r->status = status;
         r->done = true;
         latencies.push_back(t - r->t_arrival);
-        (r->op ? q_windows : i_windows) += r->windows;
+        (r->op != kOpInsert ? q_windows : i_windows) += r->windows;
         ++n_reqs;
         if (t_first == 0 || r->t_arrival < t_first) t_first = r->t_arrival;
         t_last = std::max(t_last, t);
@@ -254,7 +263,7 @@ void Server::run() {
         for (SrvRequest* r : pending) {
             if (r->op != b->op) break;
             if (cfg.max_batch_requests && take >= cfg.max_batch_requests) break;
-            const uint64_t span = align_up(r->hi - r->lo, 16);
+            const uint64_t span = align_up(r->hi - r->lo, pad_of(r->op));
             if (take > 0 && (seq + span > cfg.max_batch_bytes ||
                              (nr + r->n) * sizeof(DevRange) > cfg.max_batch_bytes))
                 break;
@@ -346,7 +355,8 @@ void Server::run() {
 }
 
 int Server::launch(SrvBatch* b) {
-    const bool query = b->op == 1;
+    const bool query = b->op != kOpInsert;
+    const bool bits = b->op == kOpQueryBits;
     uint8_t* dbase = d_ring + b->dev_off;
     uint8_t* d_seq = dbase;
     uint8_t* d_out = query ? dbase + align_up(b->seq_bytes, kAlign) : nullptr;
@@ -378,7 +388,7 @@ int Server::launch(SrvBatch* b) {
     for (size_t i = 0; i < b->reqs.size(); ++i) {
         SrvRequest* r = b->reqs[i];
         const uint64_t span = r->hi - r->lo;
-        const uint64_t padded = align_up(span, 16);
+        const uint64_t padded = align_up(span, pad_of(r->op));
         b->req_off[i] = o;
         if (r->n) {
             // One bulk copy of the client's ranges; offsets are rebased on the GPU.
@@ -424,7 +434,8 @@ int Server::launch(SrvBatch* b) {
     if (k) {
         const TileParams p =
             ragged_params(f, query, d_seq, b->seq_bytes, d_rng, k, d_tile, d_out, d_ctl,
-                          reinterpret_cast<unsigned long long*>(d_ctl + 2) + (query ? 2 : 0));
+                          reinterpret_cast<unsigned long long*>(d_ctl + 2) + (query ? 2 : 0),
+                          bits);
         const int rc = cfg.use_graph
                            ? ragged_graph_launch(f, graph[query ? 1 : 0], query, p, 0, comp)
                            : ragged_launch(f, query, p, 0, comp);
@@ -444,8 +455,9 @@ int Server::launch(SrvBatch* b) {
     for (size_t i = 0; i < b->reqs.size(); ++i) {
         SrvRequest* r = b->reqs[i];
         if (r->windows == 0) continue;
-        if ((e = cudaMemcpyAsync(r->out, d_out + b->req_off[i], r->windows, cudaMemcpyDeviceToHost,
-                                 down)) != cudaSuccess)
+        const uint64_t src = bits ? b->req_off[i] / 8 : b->req_off[i];
+        if ((e = cudaMemcpyAsync(r->out, d_out + src, result_bytes(b->op, r->windows),
+                                 cudaMemcpyDeviceToHost, down)) != cudaSuccess)
             return cuda_fail(e, "cudaMemcpyAsync(hits)");
     }
     if ((e = cudaEventRecord(b->ev_done, down)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
@@ -533,8 +545,9 @@ extern "C" int sbf_server_submit(sbf_server_t* h, int op, const char* base,
                                  uint64_t out_len, double arrival, uint64_t* ticket) {
     if (!h || !ticket) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     Server& s = h->s;
-    if (op != 0 && op != 1)
-        return set_error(SBF_ERR_INVALID_ARGUMENT, "op must be 0 (insert) or 1 (query)");
+    if (op != kOpInsert && op != kOpQuery && op != kOpQueryBits)
+        return set_error(SBF_ERR_INVALID_ARGUMENT,
+                         "op must be 0 (insert), 1 (query) or 2 (query, bit-packed)");
     if (n && (!ranges || !base)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     auto r = std::make_unique<SrvRequest>();
     r->op = op;
@@ -552,9 +565,9 @@ extern "C" int sbf_server_submit(sbf_server_t* h, int op, const char* base,
     }
     const uint64_t span = r->hi - r->lo;
     r->windows = span >= s.f->k ? span - s.f->k + 1 : 0;
-    if (op == 1 && r->windows && (!out || out_len < r->windows))
+    if (op != kOpInsert && r->windows && (!out || out_len < result_bytes(op, r->windows)))
         return set_error(SBF_ERR_INVALID_ARGUMENT, "query output span is too small");
-    if (align_up(span, 16) > s.cfg.max_batch_bytes || n * sizeof(DevRange) > s.cfg.max_batch_bytes)
+    if (align_up(span, pad_of(op)) > s.cfg.max_batch_bytes || n * sizeof(DevRange) > s.cfg.max_batch_bytes)
         return set_error(SBF_ERR_INVALID_ARGUMENT,
                          "request of %llu bytes exceeds the server's batch cap of %llu bytes",
                          static_cast<unsigned long long>(span),

@@ -411,7 +411,9 @@ int sbf_server_create(sbf_filter_t* filter, const sbf_server_config* config,
 void sbf_server_destroy(sbf_server_t* server);
 /* The server's clock (seconds, monotonic) for arrival stamps. */
 double sbf_server_now(void);
-/* Queues a request: op 0 = insert, 1 = query.  Records are (offset, bytes)
+/* Queues a request: op 0 = insert, 1 = query, 2 = query with bit-packed
+ * results (out[] as 32-bit words, bit i % 32 of word i / 32 for window i;
+ * out_len >= 4 * ceil((span - k + 1) / 32)).  Records are (offset, bytes)
  * ranges into `base`, ordered and non-overlapping; the request's span is
  * [ranges[0].offset, end of ranges[n-1]).  A query writes one byte per
  * window of the span to out[0 .. span - k] (out_len >= span - k + 1): the

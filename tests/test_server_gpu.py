@@ -214,3 +214,28 @@ def test_server_rejects_bad_requests(sbf, cuda):
     assert info["windows"] == 370 and hits.size == 370 and not hits.any()
     srv.drain()
     srv.close()
+
+
+def test_bit_packed_requests_match_bytes(sbf, cuda):
+    """Op 2 returns the byte results packed one bit per window, in the same
+    order relative to inserts (bit-packed and byte queries interleaved)."""
+    rng = np.random.default_rng(31)
+    genome = random_dna(rng, 300_000)
+    reqs = _make_requests(rng, genome, 120)
+    bits = 1 << 22
+    want, want_words = _serial(sbf, genome, reqs, bits)
+    f = sbf.Filter(bits, **K31)
+    f.insert_sequence(genome)
+    srv = sbf.Server(f, staging_bytes=1 << 28, pinned_bytes=1 << 26)
+    ops = [op if op == 0 else (2 if i % 2 else 1) for i, (op, _, _) in enumerate(reqs)]
+    tickets = [srv.submit(op, base, ranges) for op, (_, base, ranges) in zip(ops, reqs)]
+    for op, t, w in zip(ops, tickets, want):
+        _, hits = srv.wait(t, timeout=60.0)
+        if op == 1:
+            np.testing.assert_array_equal(hits, w)
+        elif op == 2:
+            b = np.packbits(w.astype(np.uint8), bitorder="little")
+            b = np.concatenate([b, np.zeros(hits.size * 4 - b.size, np.uint8)])
+            np.testing.assert_array_equal(hits, b.view(np.uint32))
+    srv.close()
+    np.testing.assert_array_equal(f.words_host(), want_words)
