@@ -398,6 +398,7 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
 extern "C" void sbf_filter_destroy(sbf_filter_t* f) {
     if (!f) return;
     ragged_release(f);
+    fastq_device_release(f);
     f->stage_in.release();
     f->stage_out.release();
     f->rb_dense.release();

@@ -1,0 +1,361 @@
+// sbf_fastq_gpu.cu -- FASTQ parsing on the GPU for the FASTX insert/query
+// entry points.  The reference parses on the host (FastxReader,
+// include/cusbf/Fastx.hpp:297-462, detail/fastx_buffer_reader.hpp:90-169);
+// here a block of raw FASTQ text is uploaded as it is and
+//
+//   1. every newline is located (per-tile counts, one exclusive scan, then
+//      each tile writes the positions of its newlines in order);
+//   2. each record's four lines are checked in parallel (header starting
+//      with '@', a sequence line that does not start with '+', a '+' line,
+//      a quality line of the sequence's length; '\r' before '\n' ignored);
+//   3. the sequence lines become the records of a ragged pass over the raw
+//      text (records in place, no copy), so headers, '+' lines, qualities
+//      and newlines are bytes outside every record.
+//
+// Blocks whose structure is anything else (wrapped lines, blank lines,
+// malformed records) are reported as irregular and the caller parses the
+// rest of the input on the host with the reference's rules, so results and
+// error locations are the reference's in every case.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "../../include/sbf_b200.h"
+#include "sbf_fastq_gpu.h"
+#include "sbf_host.h"
+#include "sbf_internal.h"
+#include "sbf_ragged.h"
+
+namespace sbf {
+
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr uint64_t kTileBytes = uint64_t{kScanThreads} * 256;  // 256 bytes per thread
+
+__device__ __forceinline__ uint32_t newlines_in(const uint8_t* t, uint64_t a, uint64_t b) {
+    uint32_t c = 0;
+    uint64_t x = a;
+    // 16-byte words where aligned (tiles and thread slices start aligned).
+    for (; x + 16 <= b; x += 16) {
+        const uint4 v = *reinterpret_cast<const uint4*>(t + x);
+        c += __popc(__vcmpeq4(v.x, 0x0A0A0A0Au)) + __popc(__vcmpeq4(v.y, 0x0A0A0A0Au)) +
+             __popc(__vcmpeq4(v.z, 0x0A0A0A0Au)) + __popc(__vcmpeq4(v.w, 0x0A0A0A0Au));
+    }
+    uint32_t bytes = c / 8;
+    for (; x < b; ++x) bytes += t[x] == '\n';
+    return bytes;
+}
+
+// Exclusive scan of the block's per-thread values (shared memory, 256 threads).
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* sh,
+                                                         uint32_t* total) {
+    const int tid = threadIdx.x;
+    sh[tid] = v;
+    __syncthreads();
+    for (int o = 1; o < kScanThreads; o <<= 1) {
+        const uint32_t add = tid >= o ? sh[tid - o] : 0u;
+        __syncthreads();
+        sh[tid] += add;
+        __syncthreads();
+    }
+    const uint32_t incl = sh[tid];
+    *total = sh[kScanThreads - 1];
+    __syncthreads();
+    return incl - v;
+}
+
+__global__ void tile_newlines_kernel(const uint8_t* t, uint64_t n, uint64_t* tile_count) {
+    __shared__ uint32_t sh[kScanThreads];
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kTileBytes;
+    const uint64_t a = base + static_cast<uint64_t>(threadIdx.x) * 256;
+    const uint64_t b = a + 256 < n ? a + 256 : n;
+    const uint32_t c = a < n ? newlines_in(t, a, b) : 0u;
+    uint32_t total;
+    (void)block_exclusive_scan(c, sh, &total);
+    if (threadIdx.x == 0) tile_count[blockIdx.x] = total;
+}
+
+// In-place exclusive scan of up to a few hundred thousand counts (one CTA).
+__global__ void scan_counts_kernel(uint64_t* v, uint64_t n, uint64_t* total) {
+    __shared__ uint64_t part[1024];
+    const uint64_t per = (n + 1023) / 1024;
+    const uint64_t a = threadIdx.x * per;
+    const uint64_t b = a + per < n ? a + per : n;
+    uint64_t s = 0;
+    for (uint64_t i = a; i < b; ++i) s += v[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        const uint64_t add = threadIdx.x >= static_cast<unsigned>(o) ? part[threadIdx.x - o] : 0;
+        __syncthreads();
+        part[threadIdx.x] += add;
+        __syncthreads();
+    }
+    uint64_t run = part[threadIdx.x] - s;
+    for (uint64_t i = a; i < b; ++i) {
+        const uint64_t x = v[i];
+        v[i] = run;
+        run += x;
+    }
+    if (threadIdx.x == 1023) *total = part[1023];
+}
+
+__global__ void newline_positions_kernel(const uint8_t* t, uint64_t n, const uint64_t* tile_off,
+                                         uint64_t* line_end) {
+    __shared__ uint32_t sh[kScanThreads];
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kTileBytes;
+    const uint64_t a = base + static_cast<uint64_t>(threadIdx.x) * 256;
+    const uint64_t b = a + 256 < n ? a + 256 : n;
+    const uint32_t c = a < n ? newlines_in(t, a, b) : 0u;
+    uint32_t total;
+    const uint32_t before = block_exclusive_scan(c, sh, &total);
+    uint64_t out = tile_off[blockIdx.x] + before;
+    for (uint64_t x = a; x < b; ++x)
+        if (t[x] == '\n') line_end[out++] = x;
+}
+
+enum : unsigned int { kIrregular = 1u };
+
+// One thread per record: lines 4r .. 4r+3.
+__global__ void fastq_records_kernel(const uint8_t* t, const uint64_t* line_end, uint64_t n_rec,
+                                     DevRange* seq, DevRange* hdr, unsigned int* flags,
+                                     unsigned long long* bases) {
+    unsigned long long local = 0;
+    for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n_rec;
+         r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t l = 4 * r;
+        const uint64_t h0 = l == 0 ? 0 : line_end[l - 1] + 1;
+        uint64_t h1 = line_end[l];
+        const uint64_t s0 = h1 + 1;
+        uint64_t s1 = line_end[l + 1];
+        const uint64_t p0 = s1 + 1;
+        const uint64_t q0 = line_end[l + 2] + 1;
+        uint64_t q1 = line_end[l + 3];
+        if (h1 > h0 && t[h1 - 1] == '\r') --h1;
+        if (s1 > s0 && t[s1 - 1] == '\r') --s1;
+        if (q1 > q0 && t[q1 - 1] == '\r') --q1;
+        const bool ok = h1 > h0 && t[h0] == '@' && (s1 == s0 || t[s0] != '+') &&
+                        line_end[l + 2] > p0 - 1 && t[p0] == '+' && q1 - q0 == s1 - s0;
+        if (!ok) atomicOr(flags, kIrregular);
+        seq[r] = DevRange{s0, s1 - s0};
+        hdr[r] = DevRange{h0 + 1, h1 - h0 - 1};
+        local += s1 - s0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xFFFFFFFFu, local, o);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(bases, local);
+}
+
+__device__ __forceinline__ bool dna_byte(uint8_t b) {
+    const uint8_t u = b & 0xDFu;
+    return u == 'A' || u == 'C' || u == 'G' || u == 'T';
+}
+
+// Per-record valid and positive windows (one warp per record).
+__global__ void fastq_record_counts_kernel(const uint8_t* t, const DevRange* seq, uint64_t n,
+                                           uint32_t k, const uint8_t* hits,
+                                           unsigned long long* valid_out,
+                                           unsigned long long* pos_out) {
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint64_t r = warp; r < n; r += warps) {
+        const uint64_t off = seq[r].offset, size = seq[r].bytes;
+        unsigned long long valid = 0, pos = 0;
+        if (size >= k) {
+            const uint8_t* rec = t + off;
+            int64_t last_inv = -1;
+            for (uint64_t base = 0; base < size; base += 32) {
+                const uint64_t e = base + lane;
+                const bool in = e < size;
+                const bool inv = in && !dna_byte(rec[e]);
+                const uint32_t m = __ballot_sync(0xFFFFFFFFu, inv);
+                const uint32_t upto = m & (0xFFFFFFFFu >> (31 - lane));
+                const int64_t li = upto ? static_cast<int64_t>(base) + (31 - __clz(upto)) : last_inv;
+                const bool ok = in && e + 1 >= k && static_cast<int64_t>(e) - li >= k;
+                valid += __popc(__ballot_sync(0xFFFFFFFFu, ok));
+                if (m) last_inv = static_cast<int64_t>(base) + (31 - __clz(m));
+            }
+            const uint64_t windows = size - k + 1;
+            unsigned long long l = 0;
+            for (uint64_t p = lane; p < windows; p += 32) l += hits[off + p];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xFFFFFFFFu, l, o);
+            pos = l;
+        }
+        if (lane == 0) {
+            valid_out[r] = valid;
+            pos_out[r] = pos;
+        }
+    }
+}
+
+template <class T>
+int grow(DevBuf& b, uint64_t count) {
+    return b.ensure(count * sizeof(T) + 64);
+}
+
+}  // namespace
+
+int FastqDevice::parse(sbf_filter* f, const uint8_t* h_text, uint64_t len, cudaStream_t st,
+                       FastqBlock* out) {
+    *out = FastqBlock{};
+    if (len == 0) return SBF_OK;
+    const uint64_t tiles = (len + kTileBytes - 1) / kTileBytes;
+    if (tiles > (uint64_t{1} << 20))
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "FASTQ block too large for the device parser");
+    int s;
+    if ((s = text.ensure(len + 64)) != SBF_OK) return s;
+    if ((s = grow<uint64_t>(tile_off, tiles + 2)) != SBF_OK) return s;
+    if ((s = ctl.ensure(64)) != SBF_OK) return s;
+    auto* d_text = static_cast<uint8_t*>(text.ptr);
+    auto* d_tiles = static_cast<uint64_t*>(tile_off.ptr);
+    auto* d_ctl = static_cast<unsigned long long*>(ctl.ptr);  // [0] lines, [1] flags, [2] bases
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(d_text, h_text, len, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return cuda_fail(e, "cudaMemcpyAsync(fastq block)");
+    if ((e = cudaMemsetAsync(d_ctl, 0, 64, st)) != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    tile_newlines_kernel<<<static_cast<unsigned>(tiles), kScanThreads, 0, st>>>(d_text, len, d_tiles);
+    scan_counts_kernel<<<1, 1024, 0, st>>>(d_tiles, tiles, reinterpret_cast<uint64_t*>(d_ctl));
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "newline scan");
+    unsigned long long n_lines = 0;
+    if ((e = cudaMemcpyAsync(&n_lines, d_ctl, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "cudaMemcpyAsync(lines)");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    out->lines = n_lines;
+    const uint64_t n_rec = n_lines / 4;
+    out->records = n_rec;
+    if (n_rec == 0) return SBF_OK;
+    if ((s = grow<uint64_t>(line_end, n_lines + 1)) != SBF_OK) return s;
+    if ((s = grow<DevRange>(seq, n_rec)) != SBF_OK) return s;
+    if ((s = grow<DevRange>(hdr, n_rec)) != SBF_OK) return s;
+    auto* d_le = static_cast<uint64_t*>(line_end.ptr);
+    newline_positions_kernel<<<static_cast<unsigned>(tiles), kScanThreads, 0, st>>>(d_text, len,
+                                                                                    d_tiles, d_le);
+    const uint64_t threads = std::min<uint64_t>(n_rec, static_cast<uint64_t>(f->sms) * 2048);
+    fastq_records_kernel<<<static_cast<unsigned>((threads + 255) / 256), 256, 0, st>>>(
+        d_text, d_le, n_rec, static_cast<DevRange*>(seq.ptr), static_cast<DevRange*>(hdr.ptr),
+        reinterpret_cast<unsigned int*>(d_ctl + 1), d_ctl + 2);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "fastq_records_kernel");
+    unsigned long long h[3] = {0, 0, 0};
+    uint64_t last_end = 0;
+    if ((e = cudaMemcpyAsync(h, d_ctl, sizeof h, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "cudaMemcpyAsync(flags)");
+    if ((e = cudaMemcpyAsync(&last_end, d_le + 4 * n_rec - 1, 8, cudaMemcpyDeviceToHost, st)) !=
+        cudaSuccess)
+        return cuda_fail(e, "cudaMemcpyAsync(line end)");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    out->regular = (h[1] & kIrregular) == 0;
+    out->bases = h[2];
+    out->consumed = last_end + 1;
+    out->d_text = d_text;
+    out->d_seq = static_cast<const DevRange*>(seq.ptr);
+    out->d_hdr = static_cast<const DevRange*>(hdr.ptr);
+    return SBF_OK;
+}
+
+int FastqDevice::run(sbf_filter* f, bool query, const FastqBlock& b, cudaStream_t st,
+                     bool want_views, uint64_t* valid, uint64_t* positive) {
+    *valid = *positive = 0;
+    if (b.records == 0) return SBF_OK;
+    int s;
+    if ((s = counts.ensure(64)) != SBF_OK) return s;
+    auto* d_counts = static_cast<unsigned long long*>(counts.ptr);
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(d_counts, 0, 16, st)) != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    // The records of this block end at b.consumed: the ragged pass covers
+    // exactly those bytes.
+    const uint64_t len = b.consumed;
+    const uint64_t windows = f->kmers_of(len);
+    uint8_t* d_hits = nullptr;
+    if (query) {
+        if ((s = out.ensure(windows + 64)) != SBF_OK) return s;
+        d_hits = static_cast<uint8_t*>(out.ptr);
+        s = sbf_ragged_contains_async(f, reinterpret_cast<const char*>(b.d_text), len,
+                                      reinterpret_cast<const sbf_record_range*>(b.d_seq),
+                                      b.records, d_hits, windows,
+                                      reinterpret_cast<uint64_t*>(d_counts),
+                                      reinterpret_cast<sbf_stream_t>(st));
+    } else {
+        s = sbf_ragged_insert_async(f, reinterpret_cast<const char*>(b.d_text), len,
+                                    reinterpret_cast<const sbf_record_range*>(b.d_seq), b.records,
+                                    reinterpret_cast<uint64_t*>(d_counts),
+                                    reinterpret_cast<sbf_stream_t>(st));
+    }
+    if (s != SBF_OK) return s;
+    unsigned long long h[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(h, d_counts, 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "cudaMemcpyAsync(counts)");
+    if (query && want_views) {
+        // Per-record counts, the record table and the hits for the callbacks.
+        if ((s = rec_counts.ensure(b.records * 16 + 64)) != SBF_OK) return s;
+        auto* d_valid = static_cast<unsigned long long*>(rec_counts.ptr);
+        auto* d_pos = d_valid + b.records;
+        const uint64_t warps = std::min<uint64_t>(b.records, static_cast<uint64_t>(f->sms) * 64);
+        fastq_record_counts_kernel<<<static_cast<unsigned>((warps * 32 + 255) / 256), 256, 0, st>>>(
+            b.d_text, b.d_seq, b.records, f->k, d_hits, d_valid, d_pos);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "fastq_record_counts_kernel");
+        h_seq.resize(b.records);
+        h_hdr.resize(b.records);
+        h_valid.resize(b.records);
+        h_pos.resize(b.records);
+        if ((s = h_hits.ensure(windows + 64)) != SBF_OK) return s;
+        if ((e = cudaMemcpyAsync(h_seq.data(), b.d_seq, b.records * 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(h_hdr.data(), b.d_hdr, b.records * 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(h_valid.data(), d_valid, b.records * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(h_pos.data(), d_pos, b.records * 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(h_hits.p, d_hits, windows, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return cuda_fail(e, "cudaMemcpyAsync(record views)");
+    }
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    if ((s = f->check_device_error(st)) != SBF_OK) return s;
+    *valid = h[0];
+    *positive = h[1];
+    return SBF_OK;
+}
+
+int PinnedBuf::ensure(size_t bytes) {
+    if (bytes <= cap) return SBF_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = std::max<size_t>(bytes, 4096);
+    if (cudaMallocHost(&p, want) != cudaSuccess) {
+        cudaGetLastError();
+        p = nullptr;
+        return set_error(SBF_ERR_RESOURCE, "cannot allocate %zu bytes of pinned memory", want);
+    }
+    cap = want;
+    return SBF_OK;
+}
+
+void PinnedBuf::release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+}
+
+void fastq_device_release(sbf_filter* f) {
+    f->fastq_block.release();
+    if (!f->fastq) return;
+    f->fastq->release();
+    delete f->fastq;
+    f->fastq = nullptr;
+}
+
+void FastqDevice::release() {
+    text.release();
+    tile_off.release();
+    line_end.release();
+    seq.release();
+    hdr.release();
+    ctl.release();
+    counts.release();
+    out.release();
+    rec_counts.release();
+    h_hits.release();
+}
+
+}  // namespace sbf

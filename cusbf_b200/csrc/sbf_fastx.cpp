@@ -30,6 +30,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/sbf_b200.h"
+#include "sbf_fastq_gpu.h"
 #include "sbf_host.h"
 
 namespace sbf {
@@ -94,8 +95,10 @@ enum class Format { unknown, fasta, fastq };
 
 class FastxParser {
    public:
-    FastxParser(sbf_read_fn read, void* user, std::string source)
-        : lines_(read, user), source_(std::move(source)) {}
+    // line_base: lines of the input already consumed before `read`'s first
+    // byte (error locations count from the start of the whole input).
+    FastxParser(sbf_read_fn read, void* user, std::string source, uint64_t line_base = 0)
+        : lines_(read, user), source_(std::move(source)), line_no_(line_base) {}
 
     // 1 = record, 0 = end of input, or an sbf_status error (negated).
     int next(std::string& header, std::string& seq) {
@@ -266,17 +269,18 @@ int chunk_record_cb(void* u, const sbf_record_view* v) {
     return ctx->consume(ctx->user, &fv);
 }
 
-int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const char* source,
-              double fill_fraction, sbf_stream_t stream, sbf_insert_report* irep,
-              sbf_query_report* qrep, sbf_fastx_record_cb consume, void* cuser) {
-    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    if (!read) return set_error(SBF_ERR_INVALID_ARGUMENT, "read callback is null");
-    FastxParser parser(read, ruser, source ? source : "<stream>");
+// Host parsing (FastxReader semantics) of the input from `read`, whose first
+// byte starts line line_base + 1 and record index_base; reports are added to
+// `it` / `qt`.
+int run_fastx_host(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const char* source,
+                   double fill_fraction, sbf_stream_t stream, sbf_insert_report& it,
+                   sbf_query_report& qt, sbf_fastx_record_cb consume, void* cuser,
+                   uint64_t line_base, uint64_t index_base) {
+    FastxParser parser(read, ruser, source ? source : "<stream>", line_base);
     const size_t budget = staging_budget(fill_fraction);
     Chunk chunk;
-    sbf_insert_report it{0, 0, 0};
-    sbf_query_report qt{0, 0, 0, 0};
-    uint64_t next_index = 0;
+    chunk.first_index = index_base;
+    uint64_t next_index = index_base;
     std::string header, seq;
     auto flush = [&]() -> int {
         if (chunk.ranges.empty()) return SBF_OK;
@@ -318,11 +322,139 @@ int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const ch
             if (s != SBF_OK) return s;
         }
     }
-    const int s = flush();
+    return flush();
+}
+
+// Serves `data` first, then the rest of the input from `inner`.
+struct PrefixReader {
+    const char* data;
+    size_t len, pos;
+    sbf_read_fn inner;
+    void* inner_user;
+    static int64_t read(void* u, char* buf, uint64_t cap) {
+        auto* r = static_cast<PrefixReader*>(u);
+        if (r->pos < r->len) {
+            const size_t n = std::min<size_t>(cap, r->len - r->pos);
+            std::memcpy(buf, r->data + r->pos, n);
+            r->pos += n;
+            return static_cast<int64_t>(n);
+        }
+        return r->inner(r->inner_user, buf, cap);
+    }
+};
+
+bool device_fastq_enabled() {
+    const char* v = std::getenv("SBF_FASTX_PARSER");
+    return !(v && std::strcmp(v, "host") == 0);
+}
+
+uint64_t fastq_block_bytes() {
+    if (const char* v = std::getenv("SBF_FASTQ_BLOCK_BYTES")) {
+        const long long b = std::strtoll(v, nullptr, 10);
+        if (b >= 4096) return static_cast<uint64_t>(b);
+    }
+    return uint64_t{256} << 20;
+}
+
+// FASTQ input through the GPU parser in blocks of complete four-line
+// records; falls back to run_fastx_host for the rest of the input at the
+// first block that is not strictly four-line (or not FASTQ at all, or a
+// record longer than a block), so results and errors are always the host
+// parser's.
+int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const char* source,
+              double fill_fraction, sbf_stream_t stream, sbf_insert_report* irep,
+              sbf_query_report* qrep, sbf_fastx_record_cb consume, void* cuser) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (!read) return set_error(SBF_ERR_INVALID_ARGUMENT, "read callback is null");
+    sbf_insert_report it{0, 0, 0};
+    sbf_query_report qt{0, 0, 0, 0};
+    auto finish = [&](int s) -> int {
+        if (s != SBF_OK) return s;
+        if (irep) *irep = it;
+        if (qrep) *qrep = qt;
+        return SBF_OK;
+    };
+    if (!device_fastq_enabled())
+        return finish(run_fastx_host(f, query, read, ruser, source, fill_fraction, stream, it, qt,
+                                     consume, cuser, 0, 0));
+    if (!f->fastq) f->fastq = new FastqDevice();
+    FastqDevice& dev = *f->fastq;
+    const uint64_t cap = fastq_block_bytes();
+    PinnedBuf& buf = f->fastq_block;
+    int s = buf.ensure(cap + 1);
     if (s != SBF_OK) return s;
-    if (irep) *irep = it;
-    if (qrep) *qrep = qt;
-    return SBF_OK;
+    auto* text = static_cast<char*>(buf.p);
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    uint64_t len = 0, line_base = 0, index_base = 0;
+    bool eof = false;
+    auto fallback = [&](uint64_t valid_len) -> int {
+        PrefixReader pr{text, valid_len, 0, read, ruser};
+        return finish(run_fastx_host(f, query, &PrefixReader::read, &pr, source, fill_fraction,
+                                     stream, it, qt, consume, cuser, line_base, index_base));
+    };
+    for (;;) {
+        while (!eof && len < cap) {
+            const int64_t n = read(ruser, text + len, cap - len);
+            if (n < 0)
+                return set_error(SBF_ERR_IO, "Failed to read FASTA/FASTQ input from %s",
+                                 source ? source : "<stream>");
+            if (n == 0)
+                eof = true;
+            else
+                len += static_cast<uint64_t>(n);
+        }
+        if (len == 0) break;
+        if (text[0] != '@') return fallback(len);  // FASTA, blank lines, or not FASTX
+        uint64_t parse_len = len;
+        bool added_newline = false;
+        if (eof && text[len - 1] != '\n') {
+            text[len] = '\n';  // the last line ends at end of input
+            parse_len = len + 1;
+            added_newline = true;
+        }
+        FastqBlock b;
+        if ((s = dev.parse(f, reinterpret_cast<const uint8_t*>(text), parse_len, st, &b)) != SBF_OK)
+            return s;
+        if (!b.regular || b.records == 0 || (eof && b.consumed < parse_len)) return fallback(len);
+        uint64_t valid = 0, positive = 0;
+        const bool views = query && consume;
+        if ((s = dev.run(f, query, b, st, views, &valid, &positive)) != SBF_OK) return s;
+        if (query) {
+            qt.records_queried += b.records;
+            qt.queried_bases += b.bases;
+            qt.queried_kmers += valid;
+            qt.positive_kmers += positive;
+        } else {
+            it.records_indexed += b.records;
+            it.indexed_bases += b.bases;
+            it.inserted_kmers += valid;
+        }
+        if (views) {
+            for (uint64_t r = 0; r < b.records; ++r) {
+                const DevRange sq = dev.h_seq[r], hd = dev.h_hdr[r];
+                sbf_fastx_record_view v{index_base + r,
+                                        text + hd.offset,
+                                        hd.bytes,
+                                        text + sq.offset,
+                                        sq.bytes,
+                                        sq.bytes,
+                                        dev.h_valid[r],
+                                        dev.h_pos[r],
+                                        dev.hits_host() + sq.offset,
+                                        sq.bytes >= f->k ? sq.bytes - f->k + 1 : 0};
+                if (consume(cuser, &v) != 0)
+                    return set_error(SBF_ERR_ABORTED, "record consumer aborted the query");
+            }
+        }
+        index_base += b.records;
+        line_base += 4 * b.records;
+        const uint64_t consumed = std::min<uint64_t>(b.consumed, len);
+        (void)added_newline;
+        std::memmove(text, text + consumed, len - consumed);
+        len -= consumed;
+        if (eof && len == 0) break;
+    }
+    return finish(SBF_OK);
 }
 
 int64_t gz_read(void* user, char* buf, uint64_t cap) {

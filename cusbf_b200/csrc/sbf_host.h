@@ -32,6 +32,14 @@ struct Staging {
     void release();
 };
 
+// A grow-only pinned host buffer.
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes);
+    void release();
+};
+
 // A grow-only device buffer.
 struct DevBuf {
     void* ptr = nullptr;
@@ -41,6 +49,7 @@ struct DevBuf {
 };
 
 struct RaggedState;
+struct FastqDevice;
 
 }  // namespace sbf
 
@@ -66,6 +75,10 @@ struct sbf_filter {
 
     // Ragged-batch engine state (sbf_ragged.cu), created on first use.
     sbf::RaggedState* ragged = nullptr;
+    // FASTQ device parser buffers (sbf_fastq_gpu.cu), created on first use,
+    // and the pinned block of input text it parses.
+    sbf::FastqDevice* fastq = nullptr;
+    sbf::PinnedBuf fastq_block;
 
     // Record-batch staging (sbf_records.cu).
     sbf::DevBuf rb_dense, rb_norm, rb_meta, rb_hits, rb_stats;
@@ -86,4 +99,5 @@ struct sbf_filter {
 
 namespace sbf {
 void ragged_release(sbf_filter* f);
+void fastq_device_release(sbf_filter* f);
 }  // namespace sbf

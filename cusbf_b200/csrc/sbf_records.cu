@@ -67,20 +67,44 @@ uint64_t normalized_offsets(const sbf_record_range* r, uint64_t n, uint64_t* out
 // Device kernels
 // ---------------------------------------------------------------------------
 
-// One warp per record (grid-strided): copies the record's bytes from the
-// dense source to its normalised offset and writes the separator before it.
+// Normalised batch = record contents at their normalised offsets and the
+// separator symbol everywhere else.  Each CTA builds segments of
+// kGatherSegment output bytes (grid-strided): it fills the segment with
+// separators, then copies the parts of the records that overlap it, so a
+// single huge record is spread over the whole grid and many small ones share
+// a CTA.
+constexpr uint64_t kGatherSegment = 1u << 16;
+
 __global__ void normalize_gather_kernel(const uint8_t* dense, uint64_t dense_base,
                                         const sbf_record_range* ranges, const uint64_t* out_off,
-                                        uint64_t n, uint8_t* out) {
-    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    for (uint64_t r = warp; r < n; r += warps) {
-        const uint64_t dst = out_off[r];
-        const uint64_t src = ranges[r].sequence_offset - dense_base;
-        const uint64_t len = ranges[r].sequence_bytes;
-        if (dst != 0 && lane == 0) out[dst - 1] = kSeparator;
-        for (uint64_t x = lane; x < len; x += 32) out[dst + x] = dense[src + x];
+                                        uint64_t n, uint8_t* out, uint64_t norm_len) {
+    __shared__ uint64_t first;
+    for (uint64_t seg = blockIdx.x; seg * kGatherSegment < norm_len; seg += gridDim.x) {
+        const uint64_t s0 = seg * kGatherSegment;
+        const uint64_t s1 = s0 + kGatherSegment < norm_len ? s0 + kGatherSegment : norm_len;
+        for (uint64_t x = s0 + threadIdx.x; x < s1; x += blockDim.x) out[x] = kSeparator;
+        if (threadIdx.x == 0) {
+            // First record whose normalised end is past the segment start.
+            uint64_t lo = 0, hi = n;
+            while (lo < hi) {
+                const uint64_t mid = (lo + hi) >> 1;
+                if (out_off[mid] + ranges[mid].sequence_bytes > s0)
+                    hi = mid;
+                else
+                    lo = mid + 1;
+            }
+            first = lo;
+        }
+        __syncthreads();
+        for (uint64_t r = first; r < n && out_off[r] < s1; ++r) {
+            const uint64_t beg = out_off[r];
+            const uint64_t end = beg + ranges[r].sequence_bytes;
+            const uint64_t a = beg > s0 ? beg : s0;
+            const uint64_t b = end < s1 ? end : s1;
+            const uint8_t* src = dense + (ranges[r].sequence_offset - dense_base) + (a - beg);
+            for (uint64_t x = threadIdx.x; a + x < b; x += blockDim.x) out[a + x] = src[x];
+        }
+        __syncthreads();
     }
 }
 
@@ -209,10 +233,11 @@ int sbf_filter::stage_record_batch(const char* h_seq, uint64_t len, const sbf_re
     SBF_CUDA(cudaMemcpyAsync(rb_dense.ptr, h_seq + lo, span, cudaMemcpyHostToDevice, st));
     SBF_CUDA(cudaMemcpyAsync(d_ranges, r, n * sizeof(sbf_record_range), cudaMemcpyHostToDevice, st));
     SBF_CUDA(cudaMemcpyAsync(d_off, out_off.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
-    const uint64_t warps = std::min<uint64_t>(n, static_cast<uint64_t>(sms) * 64);
-    normalize_gather_kernel<<<static_cast<unsigned>((warps * 32 + 255) / 256), 256, 0, st>>>(
+    const uint64_t segs = (norm_len + kGatherSegment - 1) / kGatherSegment;
+    const uint64_t ctas = std::min<uint64_t>(segs, static_cast<uint64_t>(sms) * 8);
+    normalize_gather_kernel<<<static_cast<unsigned>(ctas), 256, 0, st>>>(
         static_cast<const uint8_t*>(rb_dense.ptr), lo, d_ranges, d_off, n,
-        static_cast<uint8_t*>(rb_norm.ptr));
+        static_cast<uint8_t*>(rb_norm.ptr), norm_len);
     SBF_CUDA(cudaGetLastError());
     // The host layout vector must stay alive until the copies complete.
     SBF_CUDA(cudaStreamSynchronize(st));
