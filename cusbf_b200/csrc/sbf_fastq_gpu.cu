@@ -1,5 +1,5 @@
-// sbf_fastq_gpu.cu -- FASTQ parsing on the GPU for the FASTX insert/query
-// entry points.  The reference parses on the host (FastxReader,
+// sbf_fastq_gpu.cu -- FASTQ and FASTA parsing on the GPU for the FASTX
+// insert/query entry points.  The reference parses on the host (FastxReader,
 // include/cusbf/Fastx.hpp:297-462, detail/fastx_buffer_reader.hpp:90-169);
 // here a block of raw FASTQ text is uploaded as it is and
 //
@@ -11,6 +11,11 @@
 //   3. the sequence lines become the records of a ragged pass over the raw
 //      text (records in place, no copy), so headers, '+' lines, qualities
 //      and newlines are bytes outside every record.
+//
+// FASTA blocks use the same newline scan; each line's sequence bytes (none
+// for '>' headers) are scanned into offsets and copied into one compacted
+// buffer, header lines delimit records, and the block's last record is kept
+// for the next block unless the input ends.
 //
 // Blocks whose structure is anything else (wrapped lines, blank lines,
 // malformed records) are reported as irregular and the caller parses the
@@ -192,6 +197,76 @@ __global__ void fastq_record_counts_kernel(const uint8_t* t, const DevRange* seq
     }
 }
 
+// Bounds of line i without its '\n' and a trailing '\r', and whether it is a
+// FASTA header ('>' first).
+__device__ __forceinline__ bool fasta_line(const uint8_t* t, const uint64_t* line_end, uint64_t i,
+                                           uint64_t* a_out, uint64_t* b_out) {
+    const uint64_t a = i == 0 ? 0 : line_end[i - 1] + 1;
+    uint64_t b = line_end[i];
+    if (b > a && t[b - 1] == '\r') --b;
+    *a_out = a;
+    *b_out = b;
+    return b > a && t[a] == '>';
+}
+
+// FASTA, one thread per line: sequence bytes of the line (0 for headers and
+// '\r') and a header flag ('>' at the line start).
+__global__ void fasta_lines_kernel(const uint8_t* t, const uint64_t* line_end, uint64_t n,
+                                   uint64_t* len, uint64_t* hdr) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint64_t a, b;
+        const bool h = fasta_line(t, line_end, i, &a, &b);
+        hdr[i] = h ? 1 : 0;
+        len[i] = h ? 0 : b - a;
+    }
+}
+
+// One warp per line: copies sequence lines to their compacted offsets
+// (`off`: exclusive scan of the line lengths).
+__global__ void fasta_compact_kernel(const uint8_t* t, const uint64_t* line_end, uint64_t n,
+                                     const uint64_t* off, uint8_t* comp) {
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint64_t i = warp; i < n; i += warps) {
+        uint64_t a, b;
+        if (fasta_line(t, line_end, i, &a, &b)) continue;
+        for (uint64_t x = lane; a + x < b; x += 32) comp[off[i] + x] = t[a + x];
+    }
+}
+
+// One thread per line: header line i starts record hdr_scan[i] (headers
+// before it), whose sequence starts at off[i].  `last` receives the last
+// record's header line start and sequence start.
+__global__ void fasta_records_kernel(const uint8_t* t, const uint64_t* line_end, uint64_t n,
+                                     const uint64_t* off, const uint64_t* hdr_scan,
+                                     uint64_t n_rec, DevRange* seq, DevRange* hdr,
+                                     unsigned long long* last) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint64_t a, b;
+        if (!fasta_line(t, line_end, i, &a, &b)) continue;
+        const uint64_t r = hdr_scan[i];
+        hdr[r] = DevRange{a + 1, b - a - 1};
+        seq[r].offset = off[i];
+        if (r + 1 == n_rec) {
+            last[0] = a;
+            last[1] = off[i];
+            last[2] = i;
+        }
+    }
+}
+
+// Record lengths once every record start is known.
+__global__ void fasta_lengths_kernel(DevRange* seq, uint64_t n_rec, uint64_t total_seq) {
+    for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n_rec;
+         r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t end = r + 1 < n_rec ? seq[r + 1].offset : total_seq;
+        seq[r].bytes = end - seq[r].offset;
+    }
+}
+
 template <class T>
 int grow(DevBuf& b, uint64_t count) {
     return b.ensure(count * sizeof(T) + 64);
@@ -199,23 +274,23 @@ int grow(DevBuf& b, uint64_t count) {
 
 }  // namespace
 
-int FastqDevice::parse(sbf_filter* f, const uint8_t* h_text, uint64_t len, cudaStream_t st,
-                       FastqBlock* out) {
-    *out = FastqBlock{};
-    if (len == 0) return SBF_OK;
+int FastqDevice::scan_lines(sbf_filter* f, const uint8_t* h_text, uint64_t len, cudaStream_t st,
+                            uint64_t* n_lines_out) {
+    (void)f;
+    *n_lines_out = 0;
     const uint64_t tiles = (len + kTileBytes - 1) / kTileBytes;
     if (tiles > (uint64_t{1} << 20))
-        return set_error(SBF_ERR_INVALID_ARGUMENT, "FASTQ block too large for the device parser");
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "FASTX block too large for the device parser");
     int s;
     if ((s = text.ensure(len + 64)) != SBF_OK) return s;
     if ((s = grow<uint64_t>(tile_off, tiles + 2)) != SBF_OK) return s;
-    if ((s = ctl.ensure(64)) != SBF_OK) return s;
+    if ((s = ctl.ensure(128)) != SBF_OK) return s;
     auto* d_text = static_cast<uint8_t*>(text.ptr);
     auto* d_tiles = static_cast<uint64_t*>(tile_off.ptr);
-    auto* d_ctl = static_cast<unsigned long long*>(ctl.ptr);  // [0] lines, [1] flags, [2] bases
+    auto* d_ctl = static_cast<unsigned long long*>(ctl.ptr);
     cudaError_t e;
     if ((e = cudaMemcpyAsync(d_text, h_text, len, cudaMemcpyHostToDevice, st)) != cudaSuccess)
-        return cuda_fail(e, "cudaMemcpyAsync(fastq block)");
+        return cuda_fail(e, "cudaMemcpyAsync(fastx block)");
     if ((e = cudaMemsetAsync(d_ctl, 0, 64, st)) != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
     tile_newlines_kernel<<<static_cast<unsigned>(tiles), kScanThreads, 0, st>>>(d_text, len, d_tiles);
     scan_counts_kernel<<<1, 1024, 0, st>>>(d_tiles, tiles, reinterpret_cast<uint64_t*>(d_ctl));
@@ -224,16 +299,32 @@ int FastqDevice::parse(sbf_filter* f, const uint8_t* h_text, uint64_t len, cudaS
     if ((e = cudaMemcpyAsync(&n_lines, d_ctl, 8, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return cuda_fail(e, "cudaMemcpyAsync(lines)");
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    if (n_lines == 0) return SBF_OK;
+    if ((s = grow<uint64_t>(line_end, n_lines + 1)) != SBF_OK) return s;
+    newline_positions_kernel<<<static_cast<unsigned>(tiles), kScanThreads, 0, st>>>(
+        d_text, len, d_tiles, static_cast<uint64_t*>(line_end.ptr));
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "newline_positions_kernel");
+    *n_lines_out = n_lines;
+    return SBF_OK;
+}
+
+int FastqDevice::parse(sbf_filter* f, const uint8_t* h_text, uint64_t len, cudaStream_t st,
+                       FastqBlock* out) {
+    *out = FastqBlock{};
+    if (len == 0) return SBF_OK;
+    uint64_t n_lines = 0;
+    int s = scan_lines(f, h_text, len, st, &n_lines);
+    if (s != SBF_OK) return s;
     out->lines = n_lines;
     const uint64_t n_rec = n_lines / 4;
     out->records = n_rec;
     if (n_rec == 0) return SBF_OK;
-    if ((s = grow<uint64_t>(line_end, n_lines + 1)) != SBF_OK) return s;
     if ((s = grow<DevRange>(seq, n_rec)) != SBF_OK) return s;
     if ((s = grow<DevRange>(hdr, n_rec)) != SBF_OK) return s;
+    auto* d_text = static_cast<uint8_t*>(text.ptr);
     auto* d_le = static_cast<uint64_t*>(line_end.ptr);
-    newline_positions_kernel<<<static_cast<unsigned>(tiles), kScanThreads, 0, st>>>(d_text, len,
-                                                                                    d_tiles, d_le);
+    auto* d_ctl = static_cast<unsigned long long*>(ctl.ptr);  // [1] flags, [2] bases
+    cudaError_t e;
     const uint64_t threads = std::min<uint64_t>(n_rec, static_cast<uint64_t>(f->sms) * 2048);
     fastq_records_kernel<<<static_cast<unsigned>((threads + 255) / 256), 256, 0, st>>>(
         d_text, d_le, n_rec, static_cast<DevRange*>(seq.ptr), static_cast<DevRange*>(hdr.ptr),
@@ -251,6 +342,71 @@ int FastqDevice::parse(sbf_filter* f, const uint8_t* h_text, uint64_t len, cudaS
     out->bases = h[2];
     out->consumed = last_end + 1;
     out->d_text = d_text;
+    out->d_base = d_text;
+    out->base_len = out->consumed;
+    out->d_seq = static_cast<const DevRange*>(seq.ptr);
+    out->d_hdr = static_cast<const DevRange*>(hdr.ptr);
+    return SBF_OK;
+}
+
+int FastqDevice::parse_fasta(sbf_filter* f, const uint8_t* h_text, uint64_t len, bool eof,
+                             cudaStream_t st, FastqBlock* out) {
+    *out = FastqBlock{};
+    out->compacted = true;
+    if (len == 0) return SBF_OK;
+    uint64_t n_lines = 0;
+    int s = scan_lines(f, h_text, len, st, &n_lines);
+    if (s != SBF_OK) return s;
+    out->lines = n_lines;
+    if (n_lines == 0) return SBF_OK;
+    if ((s = grow<uint64_t>(line_len, n_lines + 1)) != SBF_OK) return s;
+    if ((s = grow<uint64_t>(line_hdr, n_lines + 1)) != SBF_OK) return s;
+    auto* d_text = static_cast<uint8_t*>(text.ptr);
+    auto* d_le = static_cast<uint64_t*>(line_end.ptr);
+    auto* d_len = static_cast<uint64_t*>(line_len.ptr);
+    auto* d_hdrf = static_cast<uint64_t*>(line_hdr.ptr);
+    auto* d_ctl = static_cast<unsigned long long*>(ctl.ptr);  // [3] seq total, [4] headers, [5..7] last header
+    cudaError_t e;
+    const unsigned lblocks =
+        static_cast<unsigned>(std::min<uint64_t>((n_lines + 255) / 256, static_cast<uint64_t>(f->sms) * 32));
+    fasta_lines_kernel<<<lblocks, 256, 0, st>>>(d_text, d_le, n_lines, d_len, d_hdrf);
+    scan_counts_kernel<<<1, 1024, 0, st>>>(d_len, n_lines, reinterpret_cast<uint64_t*>(d_ctl + 3));
+    scan_counts_kernel<<<1, 1024, 0, st>>>(d_hdrf, n_lines, reinterpret_cast<uint64_t*>(d_ctl + 4));
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "fasta line scan");
+    unsigned long long tot[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(tot, d_ctl + 3, 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "cudaMemcpyAsync(fasta totals)");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    const uint64_t total_seq = tot[0], n_rec = tot[1];
+    if (n_rec == 0) {
+        out->regular = false;  // no header among the complete lines
+        return SBF_OK;
+    }
+    if ((s = comp.ensure(total_seq + 64)) != SBF_OK) return s;
+    if ((s = grow<DevRange>(seq, n_rec)) != SBF_OK) return s;
+    if ((s = grow<DevRange>(hdr, n_rec)) != SBF_OK) return s;
+    auto* d_comp = static_cast<uint8_t*>(comp.ptr);
+    const uint64_t warps = std::min<uint64_t>(n_lines, static_cast<uint64_t>(f->sms) * 64);
+    fasta_compact_kernel<<<static_cast<unsigned>((warps * 32 + 255) / 256), 256, 0, st>>>(
+        d_text, d_le, n_lines, d_len, d_comp);
+    fasta_records_kernel<<<lblocks, 256, 0, st>>>(d_text, d_le, n_lines, d_len, d_hdrf, n_rec,
+                                                  static_cast<DevRange*>(seq.ptr),
+                                                  static_cast<DevRange*>(hdr.ptr), d_ctl + 5);
+    fasta_lengths_kernel<<<static_cast<unsigned>(std::min<uint64_t>((n_rec + 255) / 256, 4096)),
+                           256, 0, st>>>(static_cast<DevRange*>(seq.ptr), n_rec, total_seq);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "fasta records");
+    unsigned long long last[3] = {0, 0, 0};  // last header: line start, sequence start, line
+    if ((e = cudaMemcpyAsync(last, d_ctl + 5, 24, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "cudaMemcpyAsync(last header)");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    const uint64_t use = eof ? n_rec : n_rec - 1;
+    out->records = use;
+    out->lines = eof ? n_lines : last[2];  // lines of the records processed
+    out->consumed = eof ? len : last[0];
+    out->base_len = eof ? total_seq : last[1];
+    out->bases = out->base_len;
+    out->d_text = d_text;
+    out->d_base = d_comp;
     out->d_seq = static_cast<const DevRange*>(seq.ptr);
     out->d_hdr = static_cast<const DevRange*>(hdr.ptr);
     return SBF_OK;
@@ -265,21 +421,22 @@ int FastqDevice::run(sbf_filter* f, bool query, const FastqBlock& b, cudaStream_
     auto* d_counts = static_cast<unsigned long long*>(counts.ptr);
     cudaError_t e;
     if ((e = cudaMemsetAsync(d_counts, 0, 16, st)) != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-    // The records of this block end at b.consumed: the ragged pass covers
-    // exactly those bytes.
-    const uint64_t len = b.consumed;
+    // The records of this block end at b.base_len: the ragged pass covers
+    // exactly those bytes of d_base (the text for FASTQ, the compacted
+    // sequences for FASTA).
+    const uint64_t len = b.base_len;
     const uint64_t windows = f->kmers_of(len);
     uint8_t* d_hits = nullptr;
     if (query) {
         if ((s = out.ensure(windows + 64)) != SBF_OK) return s;
         d_hits = static_cast<uint8_t*>(out.ptr);
-        s = sbf_ragged_contains_async(f, reinterpret_cast<const char*>(b.d_text), len,
+        s = sbf_ragged_contains_async(f, reinterpret_cast<const char*>(b.d_base), len,
                                       reinterpret_cast<const sbf_record_range*>(b.d_seq),
                                       b.records, d_hits, windows,
                                       reinterpret_cast<uint64_t*>(d_counts),
                                       reinterpret_cast<sbf_stream_t>(st));
     } else {
-        s = sbf_ragged_insert_async(f, reinterpret_cast<const char*>(b.d_text), len,
+        s = sbf_ragged_insert_async(f, reinterpret_cast<const char*>(b.d_base), len,
                                     reinterpret_cast<const sbf_record_range*>(b.d_seq), b.records,
                                     reinterpret_cast<uint64_t*>(d_counts),
                                     reinterpret_cast<sbf_stream_t>(st));
@@ -295,7 +452,13 @@ int FastqDevice::run(sbf_filter* f, bool query, const FastqBlock& b, cudaStream_
         auto* d_pos = d_valid + b.records;
         const uint64_t warps = std::min<uint64_t>(b.records, static_cast<uint64_t>(f->sms) * 64);
         fastq_record_counts_kernel<<<static_cast<unsigned>((warps * 32 + 255) / 256), 256, 0, st>>>(
-            b.d_text, b.d_seq, b.records, f->k, d_hits, d_valid, d_pos);
+            b.d_base, b.d_seq, b.records, f->k, d_hits, d_valid, d_pos);
+        if (b.compacted) {
+            if ((s = h_comp.ensure(len + 64)) != SBF_OK) return s;
+            if (len && (e = cudaMemcpyAsync(h_comp.p, b.d_base, len, cudaMemcpyDeviceToHost, st)) !=
+                           cudaSuccess)
+                return cuda_fail(e, "cudaMemcpyAsync(fasta sequences)");
+        }
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "fastq_record_counts_kernel");
         h_seq.resize(b.records);
         h_hdr.resize(b.records);
@@ -346,6 +509,10 @@ void fastq_device_release(sbf_filter* f) {
 }
 
 void FastqDevice::release() {
+    line_len.release();
+    line_hdr.release();
+    comp.release();
+    h_comp.release();
     text.release();
     tile_off.release();
     line_end.release();

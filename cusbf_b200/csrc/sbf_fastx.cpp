@@ -356,11 +356,11 @@ uint64_t fastq_block_bytes() {
     return uint64_t{256} << 20;
 }
 
-// FASTQ input through the GPU parser in blocks of complete four-line
-// records; falls back to run_fastx_host for the rest of the input at the
-// first block that is not strictly four-line (or not FASTQ at all, or a
-// record longer than a block), so results and errors are always the host
-// parser's.
+// FASTQ and FASTA input through the GPU parsers in blocks of complete
+// records (FASTQ: strictly four-line records; FASTA: records end before the
+// next '>' header, and a record longer than the block grows it); falls back
+// to run_fastx_host for the rest of the input at the first block that is
+// anything else, so results and errors are always the host parser's.
 int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const char* source,
               double fill_fraction, sbf_stream_t stream, sbf_insert_report* irep,
               sbf_query_report* qrep, sbf_fastx_record_cb consume, void* cuser) {
@@ -379,7 +379,8 @@ int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const ch
                                      consume, cuser, 0, 0));
     if (!f->fastq) f->fastq = new FastqDevice();
     FastqDevice& dev = *f->fastq;
-    const uint64_t cap = fastq_block_bytes();
+    uint64_t cap = fastq_block_bytes();
+    const uint64_t kMaxBlockBytes = uint64_t{8} << 30;  // FASTA records up to this size
     PinnedBuf& buf = f->fastq_block;
     int s = buf.ensure(cap + 1);
     if (s != SBF_OK) return s;
@@ -404,18 +405,36 @@ int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const ch
                 len += static_cast<uint64_t>(n);
         }
         if (len == 0) break;
-        if (text[0] != '@') return fallback(len);  // FASTA, blank lines, or not FASTX
+        const bool fastq = text[0] == '@';
+        if (!fastq && text[0] != '>') return fallback(len);  // blank lines, or not FASTX
         uint64_t parse_len = len;
-        bool added_newline = false;
         if (eof && text[len - 1] != '\n') {
             text[len] = '\n';  // the last line ends at end of input
             parse_len = len + 1;
-            added_newline = true;
         }
         FastqBlock b;
-        if ((s = dev.parse(f, reinterpret_cast<const uint8_t*>(text), parse_len, st, &b)) != SBF_OK)
-            return s;
-        if (!b.regular || b.records == 0 || (eof && b.consumed < parse_len)) return fallback(len);
+        if (fastq) {
+            s = dev.parse(f, reinterpret_cast<const uint8_t*>(text), parse_len, st, &b);
+            if (s != SBF_OK) return s;
+            if (!b.regular || b.records == 0 || (eof && b.consumed < parse_len)) return fallback(len);
+        } else {
+            s = dev.parse_fasta(f, reinterpret_cast<const uint8_t*>(text), parse_len, eof, st, &b);
+            if (s != SBF_OK) return s;
+            if (!b.regular) return fallback(len);
+            if (b.records == 0) {
+                // One record longer than the block: grow the block and read on.
+                if (eof || cap >= kMaxBlockBytes) return fallback(len);
+                PinnedBuf bigger;
+                if ((s = bigger.ensure(2 * cap + 1)) != SBF_OK) return fallback(len);
+                std::memcpy(bigger.p, text, len);
+                buf.release();
+                buf = bigger;
+                bigger.p = nullptr;
+                text = static_cast<char*>(buf.p);
+                cap *= 2;
+                continue;
+            }
+        }
         uint64_t valid = 0, positive = 0;
         const bool views = query && consume;
         if ((s = dev.run(f, query, b, st, views, &valid, &positive)) != SBF_OK) return s;
@@ -430,12 +449,14 @@ int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const ch
             it.inserted_kmers += valid;
         }
         if (views) {
+            const char* seq_base =
+                b.compacted ? reinterpret_cast<const char*>(dev.comp_host()) : text;
             for (uint64_t r = 0; r < b.records; ++r) {
                 const DevRange sq = dev.h_seq[r], hd = dev.h_hdr[r];
                 sbf_fastx_record_view v{index_base + r,
                                         text + hd.offset,
                                         hd.bytes,
-                                        text + sq.offset,
+                                        seq_base + sq.offset,
                                         sq.bytes,
                                         sq.bytes,
                                         dev.h_valid[r],
@@ -447,9 +468,8 @@ int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const ch
             }
         }
         index_base += b.records;
-        line_base += 4 * b.records;
+        line_base += fastq ? 4 * b.records : b.lines;
         const uint64_t consumed = std::min<uint64_t>(b.consumed, len);
-        (void)added_newline;
         std::memmove(text, text + consumed, len - consumed);
         len -= consumed;
         if (eof && len == 0) break;
