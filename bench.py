@@ -589,12 +589,15 @@ def run_served(args, world: int, rank: int, local_rank: int) -> None:
     out_ring = torch.empty(out_ring_bytes, dtype=torch.uint8).pin_memory()
     out_np = out_ring.numpy()
     check_idx = set(range(0, n_req, max(1, n_req // 64)))
-    op_q = 2 if args.server_bits else 1
+    op_q = 3 if args.server_counts else 2 if args.server_bits else 1
 
-    def result_bytes(w):
-        return 4 * ((w + 31) // 32) if op_q == 2 else w
+    def result_len(nr):
+        """Result bytes of a query of nr reads: hit bytes, bit words, or
+        (valid, positive) uint64 pairs per read."""
+        w = nr * read_len - K + 1
+        return 16 * nr if op_q == 3 else 4 * ((w + 31) // 32) if op_q == 2 else w
 
-    check_out = {i: np.zeros(max(result_bytes(int(n_reads[i]) * read_len - K + 1), 1), np.uint8)
+    check_out = {i: np.zeros(max(result_len(int(n_reads[i])), 1), np.uint8)
                  for i in check_idx if not is_ins[i]}
     ins_range_t = torch.empty((n_req, 2), dtype=torch.int64).pin_memory()
     ins_range = ins_range_t.numpy().view(np.uint64)
@@ -616,7 +619,7 @@ def run_served(args, world: int, rank: int, local_rank: int) -> None:
                                arrival)
             else:
                 nr = int(n_reads[i])
-                w = result_bytes(nr * read_len - K + 1)
+                w = result_len(nr)
                 if i in check_out:
                     optr = check_out[i].ctypes.data
                 else:
@@ -702,7 +705,8 @@ def run_served(args, world: int, rank: int, local_rank: int) -> None:
         "data": "synthetic (seeded Poisson request stream over seeded reads and sequences)",
         "config": {"workload": f"served: {n_req:,} requests over {duration:.1f} s at "
                                f"{rate:.0f} req/s, filter of the 100 Mbp genome resident",
-                   "query_results": "bit-packed (op 2)" if op_q == 2 else "one byte per window",
+                   "query_results": {1: "one byte per window", 2: "bit-packed (op 2)",
+                                     3: "per-read (valid, positive) counts (op 3)"}[op_q],
                    "k": K, "s": S, "m": M, "hashes": H, "filter_bits": bits,
                    "staging_budget_bytes": 16 << 30, "offered_bytes": int(offered),
                    "offered_gb_per_s": offered / duration / 1e9,
@@ -737,6 +741,8 @@ def main() -> None:
     ap.add_argument("--no-serial", action="store_true", help="c5: skip the one-per-launch run")
     ap.add_argument("--server-bits", action="store_true",
                     help="c5: queries ask for bit-packed results")
+    ap.add_argument("--server-counts", action="store_true",
+                    help="c5: queries ask for per-read (valid, positive) counts only")
     ap.add_argument("--rate", type=float, default=0.0, help="c5: offered req/s (default 20k)")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip timing the reference GPU path")
@@ -1040,6 +1046,8 @@ def main() -> None:
         line["served"] = run_form(["--config", "c5", "--duration", "2.0"], summarize_served)
         line["served_bits"] = run_form(["--config", "c5", "--duration", "2.0", "--server-bits",
                                         "--no-serial"], summarize_served)
+        line["served_counts"] = run_form(["--config", "c5", "--duration", "2.0",
+                                          "--server-counts", "--no-serial"], summarize_served)
     print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -1080,6 +1088,7 @@ def summarize_ragged(d: dict) -> dict:
 def summarize_served(d: dict) -> dict:
     sv, one, pl = d["served"], d.get("one_request_per_launch") or {}, d["plain_per_record"]
     return {"metric": d["metric"], "workload": d["config"]["workload"],
+            "query_results": d["config"]["query_results"],
             "offered_gb_per_s": d["config"]["offered_gb_per_s"],
             "kmers_per_s": sv["kmers_per_s"], "requests_per_s": sv["requests_per_s"],
             "latency_ms": sv["latency_ms"], "mean_batch_requests": sv["mean_batch_requests"],

@@ -234,6 +234,8 @@ _sig("sbf_query_record_batch", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, C.POINTE
 _sig("sbf_contains_record_batch_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _vp)
 _sig("sbf_ragged_insert_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _vp)
 _sig("sbf_ragged_contains_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _vp, _vp)
+_sig("sbf_ragged_contains_counts_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, _vp, _vp,
+     _vp, _vp)
 _sig("sbf_ragged_insert", C.c_int, _vp, _vp, _u64, _vp, _u64, C.POINTER(RaggedTuning), _vp,
      C.POINTER(InsertReport))
 _sig("sbf_ragged_query", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, C.POINTER(RaggedTuning),
@@ -672,6 +674,22 @@ def _ragged_methods():
         _check(_lib.sbf_ragged_contains_async(self._h, p, n, rp, rn // 16, o, on, cp,
                                               _stream(stream)))
 
+    def ragged_contains_counts_async(self, d_seq, d_ranges, d_record_valid, d_record_positive,
+                                     d_out=None, d_counts=None, stream=None) -> None:
+        """Ragged query with per-record valid / positive window counts
+        computed in the query kernel (uint64 device arrays, one entry per
+        record, zeroed by the call); `d_out` (hit bytes) is optional."""
+        p, n = _dev_ptr(d_seq)
+        rp, rn = _dev_ptr(d_ranges)
+        vp, vn = _dev_ptr(d_record_valid)
+        pp, pn = _dev_ptr(d_record_positive)
+        if min(vn, pn) < (rn // 16) * 8:
+            raise ValueError("per-record count arrays need one uint64 per record")
+        o, on = _dev_ptr(d_out) if d_out is not None else (None, 0)
+        cp = _dev_ptr(d_counts)[0] if d_counts is not None else None
+        _check(_lib.sbf_ragged_contains_counts_async(self._h, p, n, rp, rn // 16, o, on, vp, pp,
+                                                     cp, _stream(stream)))
+
     def ragged_insert(self, seq, ranges, tuning=None, stream=None) -> InsertReport:
         b = _host_bytes(seq)
         r = _ranges(ranges)
@@ -710,8 +728,8 @@ def _ragged_methods():
         st = _lib.sbf_ragged_tuning_lookup(self._h, int(query), nbytes, n_records, C.byref(t))
         return t if st == OK else None
 
-    for f in (ragged_insert_async, ragged_contains_async, ragged_insert, ragged_query,
-              ragged_autotune, ragged_tuning_lookup):
+    for f in (ragged_insert_async, ragged_contains_async, ragged_contains_counts_async,
+              ragged_insert, ragged_query, ragged_autotune, ragged_tuning_lookup):
         setattr(Filter, f.__name__, f)
 
 
@@ -897,7 +915,7 @@ class Server:
     result equals one-request-at-a-time execution in arrival order.  While it
     runs, the filter must not be used directly."""
 
-    INSERT, QUERY, QUERY_BITS = 0, 1, 2
+    INSERT, QUERY, QUERY_BITS, QUERY_COUNTS = 0, 1, 2, 3
 
     def __init__(self, filt: "Filter", **config):
         self._filter = filt
@@ -927,8 +945,12 @@ class Server:
         if op != self.INSERT and o is None:
             span = max(int(r[-1, 0] + r[-1, 1]) - int(r[0, 0]), 0) if r.shape[0] else 0
             w = self._filter.kmer_count(span)
-            o = (np.zeros(max(w, 1), np.uint8) if op == self.QUERY
-                 else np.zeros(max((w + 31) // 32, 1), np.uint32))
+            if op == self.QUERY:
+                o = np.zeros(max(w, 1), np.uint8)
+            elif op == self.QUERY_COUNTS:
+                o = np.zeros((max(r.shape[0], 1), 2), np.uint64)
+            else:
+                o = np.zeros(max((w + 31) // 32, 1), np.uint32)
         t = self.submit_raw(op, _np_ptr(b), _np_ptr(r), r.shape[0],
                             _np_ptr(o) if o is not None else None,
                             o.nbytes if o is not None else 0, arrival)
@@ -943,7 +965,9 @@ class Server:
         return self.submit(self.INSERT, base, ranges, None, arrival)
 
     def wait(self, ticket: int, timeout: float = 0.0):
-        """Waits for a request; returns (info dict, query hits or None)."""
+        """Waits for a request; returns (info dict, result or None): hit
+        bytes (QUERY), bit words (QUERY_BITS), or an (n, 2) array of
+        per-record (valid, positive) windows (QUERY_COUNTS)."""
         info = ServerRequestInfo()
         st = _lib.sbf_server_wait(self._h, ticket, timeout, C.byref(info))
         with self._lock:
@@ -952,7 +976,12 @@ class Server:
         out = None
         if refs is not None and refs[2] is not None:
             o = refs[2]
-            out = o[:info.windows] if o.dtype == np.uint8 else o[:(info.windows + 31) // 32]
+            if o.dtype == np.uint8:
+                out = o[:info.windows]
+            elif o.dtype == np.uint64:
+                out = o.reshape(-1, 2)[:refs[1].shape[0]]
+            else:
+                out = o[:(info.windows + 31) // 32]
         return info.as_dict(), out
 
     def drain(self) -> None:

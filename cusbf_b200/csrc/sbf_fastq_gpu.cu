@@ -153,50 +153,6 @@ __global__ void fastq_records_kernel(const uint8_t* t, const uint64_t* line_end,
     if ((threadIdx.x & 31) == 0 && local) atomicAdd(bases, local);
 }
 
-__device__ __forceinline__ bool dna_byte(uint8_t b) {
-    const uint8_t u = b & 0xDFu;
-    return u == 'A' || u == 'C' || u == 'G' || u == 'T';
-}
-
-// Per-record valid and positive windows (one warp per record).
-__global__ void fastq_record_counts_kernel(const uint8_t* t, const DevRange* seq, uint64_t n,
-                                           uint32_t k, const uint8_t* hits,
-                                           unsigned long long* valid_out,
-                                           unsigned long long* pos_out) {
-    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31;
-    for (uint64_t r = warp; r < n; r += warps) {
-        const uint64_t off = seq[r].offset, size = seq[r].bytes;
-        unsigned long long valid = 0, pos = 0;
-        if (size >= k) {
-            const uint8_t* rec = t + off;
-            int64_t last_inv = -1;
-            for (uint64_t base = 0; base < size; base += 32) {
-                const uint64_t e = base + lane;
-                const bool in = e < size;
-                const bool inv = in && !dna_byte(rec[e]);
-                const uint32_t m = __ballot_sync(0xFFFFFFFFu, inv);
-                const uint32_t upto = m & (0xFFFFFFFFu >> (31 - lane));
-                const int64_t li = upto ? static_cast<int64_t>(base) + (31 - __clz(upto)) : last_inv;
-                const bool ok = in && e + 1 >= k && static_cast<int64_t>(e) - li >= k;
-                valid += __popc(__ballot_sync(0xFFFFFFFFu, ok));
-                if (m) last_inv = static_cast<int64_t>(base) + (31 - __clz(m));
-            }
-            const uint64_t windows = size - k + 1;
-            unsigned long long l = 0;
-            for (uint64_t p = lane; p < windows; p += 32) l += hits[off + p];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xFFFFFFFFu, l, o);
-            pos = l;
-        }
-        if (lane == 0) {
-            valid_out[r] = valid;
-            pos_out[r] = pos;
-        }
-    }
-}
-
 // Bounds of line i without its '\n' and a trailing '\r', and whether it is a
 // FASTA header ('>' first).
 __device__ __forceinline__ bool fasta_line(const uint8_t* t, const uint64_t* line_end, uint64_t i,
@@ -427,14 +383,29 @@ int FastqDevice::run(sbf_filter* f, bool query, const FastqBlock& b, cudaStream_
     const uint64_t len = b.base_len;
     const uint64_t windows = f->kmers_of(len);
     uint8_t* d_hits = nullptr;
+    const bool views = query && want_views;
+    unsigned long long *d_valid = nullptr, *d_pos = nullptr;
+    if (views) {
+        if ((s = rec_counts.ensure(b.records * 16 + 64)) != SBF_OK) return s;
+        d_valid = static_cast<unsigned long long*>(rec_counts.ptr);
+        d_pos = d_valid + b.records;
+    }
     if (query) {
         if ((s = out.ensure(windows + 64)) != SBF_OK) return s;
         d_hits = static_cast<uint8_t*>(out.ptr);
-        s = sbf_ragged_contains_async(f, reinterpret_cast<const char*>(b.d_base), len,
-                                      reinterpret_cast<const sbf_record_range*>(b.d_seq),
-                                      b.records, d_hits, windows,
-                                      reinterpret_cast<uint64_t*>(d_counts),
-                                      reinterpret_cast<sbf_stream_t>(st));
+        // With record views the per-record counts come from the query
+        // kernel's epilogue.
+        s = views ? sbf_ragged_contains_counts_async(
+                        f, reinterpret_cast<const char*>(b.d_base), len,
+                        reinterpret_cast<const sbf_record_range*>(b.d_seq), b.records, d_hits,
+                        windows, reinterpret_cast<uint64_t*>(d_valid),
+                        reinterpret_cast<uint64_t*>(d_pos), reinterpret_cast<uint64_t*>(d_counts),
+                        reinterpret_cast<sbf_stream_t>(st))
+                  : sbf_ragged_contains_async(f, reinterpret_cast<const char*>(b.d_base), len,
+                                              reinterpret_cast<const sbf_record_range*>(b.d_seq),
+                                              b.records, d_hits, windows,
+                                              reinterpret_cast<uint64_t*>(d_counts),
+                                              reinterpret_cast<sbf_stream_t>(st));
     } else {
         s = sbf_ragged_insert_async(f, reinterpret_cast<const char*>(b.d_base), len,
                                     reinterpret_cast<const sbf_record_range*>(b.d_seq), b.records,
@@ -445,21 +416,14 @@ int FastqDevice::run(sbf_filter* f, bool query, const FastqBlock& b, cudaStream_
     unsigned long long h[2] = {0, 0};
     if ((e = cudaMemcpyAsync(h, d_counts, 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return cuda_fail(e, "cudaMemcpyAsync(counts)");
-    if (query && want_views) {
-        // Per-record counts, the record table and the hits for the callbacks.
-        if ((s = rec_counts.ensure(b.records * 16 + 64)) != SBF_OK) return s;
-        auto* d_valid = static_cast<unsigned long long*>(rec_counts.ptr);
-        auto* d_pos = d_valid + b.records;
-        const uint64_t warps = std::min<uint64_t>(b.records, static_cast<uint64_t>(f->sms) * 64);
-        fastq_record_counts_kernel<<<static_cast<unsigned>((warps * 32 + 255) / 256), 256, 0, st>>>(
-            b.d_base, b.d_seq, b.records, f->k, d_hits, d_valid, d_pos);
+    if (views) {
+        // The record table, per-record counts and hits for the callbacks.
         if (b.compacted) {
             if ((s = h_comp.ensure(len + 64)) != SBF_OK) return s;
             if (len && (e = cudaMemcpyAsync(h_comp.p, b.d_base, len, cudaMemcpyDeviceToHost, st)) !=
                            cudaSuccess)
                 return cuda_fail(e, "cudaMemcpyAsync(fasta sequences)");
         }
-        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "fastq_record_counts_kernel");
         h_seq.resize(b.records);
         h_hdr.resize(b.records);
         h_valid.resize(b.records);

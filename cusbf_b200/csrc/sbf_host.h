@@ -86,9 +86,9 @@ struct sbf_filter {
     uint64_t kmers_of(uint64_t symbols) const;
     int stage_record_batch(const char* h_seq, uint64_t len, const sbf_record_range* r, uint64_t n,
                            cudaStream_t st, std::vector<uint64_t>& out_off, uint64_t& norm_len);
-    int record_stats(const sbf_record_range* r, uint64_t n, const uint8_t* d_hits,
-                     cudaStream_t st, std::vector<uint64_t>& valid,
-                     std::vector<uint64_t>& positive);
+    int record_pass(bool query, uint64_t n, uint64_t norm_len, uint8_t* d_hits, cudaStream_t st,
+                    std::vector<uint64_t>& valid, std::vector<uint64_t>& positive,
+                    uint64_t* total_valid);
     int launch(bool query, bool dense, const void* input, uint64_t input_bytes, uint64_t n_kmers,
                uint8_t* out, cudaStream_t st, uint32_t* out_bits = nullptr) const;
     int host_pipeline(bool query, bool dense, const void* h_in, uint64_t in_bytes,

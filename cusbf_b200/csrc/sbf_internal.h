@@ -48,6 +48,12 @@ struct TileParams {
     const uint32_t* tile_rec;      // per tile: first record whose end > tile start
     unsigned int* queue;           // work-queue counter, zero before the launch
     unsigned long long* counts;    // [0] valid windows, [1] positive windows
+    // Optional per-record tallies (zeroed before the launch): valid and
+    // positive windows of record r are added to rec_valid[r << rec_shift]
+    // and rec_pos[r << rec_shift] (rec_shift 1 interleaves the two arrays).
+    unsigned long long* rec_valid;
+    unsigned long long* rec_pos;
+    uint32_t rec_shift;
 };
 
 // Device error codes written to TileParams::err.

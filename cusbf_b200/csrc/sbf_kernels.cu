@@ -670,6 +670,75 @@ __device__ __forceinline__ uint32_t strip_in_record(const uint32_t* bk, uint32_t
     return vmask;
 }
 
+// Ragged launches with per-record tallies: adds the strip's valid windows
+// (vmask) and positive windows (hits) to the records they belong to.  Window
+// j belongs to the record containing byte x0 + j.  The strip's records are
+// found by one binary search (first record ending after its first valid
+// window) and a walk over the record ends; empty records are skipped by the
+// walk.  Across the warp, the record a strip starts in is usually the one the
+// previous strip ended in: a strip's last record is handed to the next lane
+// when it is that lane's first, and lanes holding the same record are summed
+// with one match + reduce, so a warp issues about one atomic pair per record
+// it touches (count_positive_kmers_per_record_kernel,
+// detail/count_positive_kmers.cuh:21-45, fused into the query epilogue).
+__device__ __forceinline__ void tally_records(const TileParams& p, uint32_t first, int64_t x0,
+                                              uint32_t vmask, uint32_t hits) {
+    constexpr uint32_t kNone = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t n = p.n_ranges;
+    uint32_t kf = kNone, vf = 0, kl = kNone, vl = 0;  // first / last record and (valid << 16 | pos)
+    auto add = [&](uint32_t r, uint32_t c) {
+        const uint64_t at = static_cast<uint64_t>(r) << p.rec_shift;
+        atomicAdd(p.rec_valid + at, static_cast<unsigned long long>(c >> 16));
+        if (c & 0xFFFFu) atomicAdd(p.rec_pos + at, static_cast<unsigned long long>(c & 0xFFFFu));
+    };
+    uint32_t v = vmask;
+    const uint32_t h = hits & vmask;
+    if (v) {
+        int j = __ffs(v) - 1;
+        // First record whose end exceeds x0 + j (records before `first` end
+        // before the tile).
+        uint64_t lo = first, hi = n;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (static_cast<int64_t>(p.ranges[mid].offset + p.ranges[mid].bytes) > x0 + j)
+                hi = mid;
+            else
+                lo = mid + 1;
+        }
+        uint64_t r = lo;
+        for (bool head = true; r < n; head = false) {
+            const int64_t lim = static_cast<int64_t>(p.ranges[r].offset + p.ranges[r].bytes) - x0;
+            const uint32_t seg = lim >= 32 ? v : (v & ((1u << lim) - 1u));
+            const uint32_t c = (static_cast<uint32_t>(__popc(seg)) << 16) |
+                               static_cast<uint32_t>(__popc(h & seg));
+            v &= ~seg;
+            if (head) {
+                kf = static_cast<uint32_t>(r);
+                vf = c;
+            } else if (v) {
+                add(static_cast<uint32_t>(r), c);  // a record inside the strip
+            } else {
+                kl = static_cast<uint32_t>(r);
+                vl = c;
+            }
+            if (!v) break;
+            j = __ffs(v) - 1;
+            do {
+                ++r;
+            } while (r < n && static_cast<int64_t>(p.ranges[r].offset + p.ranges[r].bytes) <= x0 + j);
+        }
+    }
+    const uint32_t prev_kl = __shfl_up_sync(0xFFFFFFFFu, kl, 1);
+    const uint32_t prev_vl = __shfl_up_sync(0xFFFFFFFFu, vl, 1);
+    const uint32_t next_kf = __shfl_down_sync(0xFFFFFFFFu, kf, 1);
+    if (lane > 0 && prev_kl != kNone && prev_kl == kf) vf += prev_vl;
+    if (kl != kNone && !(lane < 31 && next_kf == kl)) add(kl, vl);
+    const uint32_t grp = __match_any_sync(0xFFFFFFFFu, kf);
+    const uint32_t tot = __reduce_add_sync(grp, vf);
+    if (kf != kNone && lane == static_cast<uint32_t>(__ffs(grp) - 1)) add(kf, tot);
+}
+
 // Persistent tile kernel.  Plain launches walk tiles blockIdx.x + i * gridDim.x;
 // ragged launches take tiles from the device work-queue counter p.queue, so
 // tiles of uneven cost (records of any length, N runs) balance across CTAs.
@@ -765,11 +834,11 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
             vmask = strip_in_record<C>(bk, vmask);
             n_valid += __popc(vmask);
         }
+        uint32_t hits = 0;
         if constexpr (kQuery) {
-            const uint32_t hits =
-                query_strip<C>(c, vmask, p.shard_mask, p.words, slots + 4 * tid,
-                               reinterpret_cast<uint32_t*>(slots + kSlots * kThreads * 4) + tid,
-                               p.out, first_kmer, p.n_kmers);
+            hits = query_strip<C>(c, vmask, p.shard_mask, p.words, slots + 4 * tid,
+                                  reinterpret_cast<uint32_t*>(slots + kSlots * kThreads * 4) + tid,
+                                  p.out, first_kmer, p.n_kmers);
             if constexpr (kRagged) n_pos += __popc(hits & vmask);
             // Bit-packed mode (grid phase 0, so strips start at multiples of
             // 32 windows): one 32-bit word per strip, coalesced across the warp.
@@ -777,6 +846,9 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
                 p.out_bits[first_kmer >> 5] = hits;
         } else {
             if (vmask) insert_strip<C>(c, vmask, p.shard_mask, p.words, ring);
+        }
+        if constexpr (kRagged) {
+            if (p.rec_valid) tally_records(p, first_rec[it % 3], first_kmer, vmask, hits);
         }
     }
     if constexpr (!kQuery) flush_ring_drain();

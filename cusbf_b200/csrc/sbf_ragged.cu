@@ -486,20 +486,29 @@ static inline cudaStream_t S_(sbf_stream_t s) { return reinterpret_cast<cudaStre
 
 static int ragged_async(sbf_filter_t* f, bool query, const char* d_seq, uint64_t len,
                         const sbf_record_range* d_ranges, uint64_t n, uint8_t* d_out,
-                        uint64_t out_len, uint64_t* d_counts, sbf_stream_t stream) {
+                        uint64_t out_len, uint64_t* d_counts, sbf_stream_t stream,
+                        uint64_t* d_rec_valid = nullptr, uint64_t* d_rec_pos = nullptr) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
     if (n && !d_ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "ranges pointer is null");
     if (n > 0xFFFFFFFFull) return set_error(SBF_ERR_INVALID_ARGUMENT, "too many records");
+    const bool tally = d_rec_valid != nullptr;
+    if (tally && n && !d_rec_pos)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "per-record count arrays are null");
+    cudaStream_t st = S_(stream);
+    if (tally && n) {
+        SBF_CUDA(cudaMemsetAsync(d_rec_valid, 0, n * sizeof(uint64_t), st));
+        SBF_CUDA(cudaMemsetAsync(d_rec_pos, 0, n * sizeof(uint64_t), st));
+    }
     const uint64_t W = f->kmers_of(len);
     if (W == 0) return SBF_OK;
     if (!d_seq) return set_error(SBF_ERR_INVALID_ARGUMENT, "sequence pointer is null");
-    if (query && (!d_out || out_len < W))
+    // With per-record counts the hit bytes are optional.
+    if (query && (tally ? (d_out && out_len < W) : (!d_out || out_len < W)))
         return set_error(SBF_ERR_INVALID_ARGUMENT, "ragged query output span is too small");
     RaggedState* r = nullptr;
     SBF_TRY(ragged_state(f, &r));
-    cudaStream_t st = S_(stream);
     if (n == 0) {
-        if (query) SBF_CUDA(cudaMemsetAsync(d_out, 0, W, st));
+        if (query && d_out) SBF_CUDA(cudaMemsetAsync(d_out, 0, W, st));
         return SBF_OK;
     }
     TileParams p = ragged_params(f, query, reinterpret_cast<const uint8_t*>(d_seq), len,
@@ -507,6 +516,8 @@ static int ragged_async(sbf_filter_t* f, bool query, const char* d_seq, uint64_t
                                  r->d_ctl,
                                  d_counts ? reinterpret_cast<unsigned long long*>(d_counts)
                                           : ctl_counts(r));
+    p.rec_valid = reinterpret_cast<unsigned long long*>(d_rec_valid);
+    p.rec_pos = reinterpret_cast<unsigned long long*>(d_rec_pos);
     SBF_TRY(r->direct_tile_rec.ensure(p.n_tiles * 4 + 64));
     p.tile_rec = static_cast<const uint32_t*>(r->direct_tile_rec.ptr);
     return ragged_launch(f, query, p, 0, st);
@@ -524,6 +535,25 @@ extern "C" int sbf_ragged_contains_async(const sbf_filter_t* f, const char* d_se
                                          sbf_stream_t stream) {
     return ragged_async(const_cast<sbf_filter*>(f), true, d_seq, len, d_ranges, n, d_out, out_len,
                         d_counts, stream);
+}
+
+extern "C" int sbf_ragged_contains_counts_async(const sbf_filter_t* f, const char* d_seq,
+                                                uint64_t len, const sbf_record_range* d_ranges,
+                                                uint64_t n, uint8_t* d_out, uint64_t out_len,
+                                                uint64_t* d_record_valid,
+                                                uint64_t* d_record_positive, uint64_t* d_counts,
+                                                sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (n == 0) {
+        // No records: nothing to count; a given output span reads all 0.
+        return d_out ? ragged_async(const_cast<sbf_filter*>(f), true, d_seq, len, d_ranges, 0,
+                                    d_out, out_len, d_counts, stream)
+                     : SBF_OK;
+    }
+    if (!d_record_valid || !d_record_positive)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "per-record count arrays are null");
+    return ragged_async(const_cast<sbf_filter*>(f), true, d_seq, len, d_ranges, n, d_out, out_len,
+                        d_counts, stream, d_record_valid, d_record_positive);
 }
 
 extern "C" int sbf_ragged_insert(sbf_filter_t* f, const char* h_seq, uint64_t len,

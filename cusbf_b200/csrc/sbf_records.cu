@@ -30,7 +30,6 @@ using namespace sbf;
 namespace sbf {
 
 constexpr uint8_t kSeparator = 'N';
-constexpr uint64_t kStatSegment = 1u << 16;  // bytes of a record per stats work item
 
 // ---------------------------------------------------------------------------
 // Host layout
@@ -108,68 +107,6 @@ __global__ void normalize_gather_kernel(const uint8_t* dense, uint64_t dense_bas
     }
 }
 
-// Per-record statistics over segments of at most kStatSegment window starts:
-// valid windows (K consecutive A/C/G/T bytes) and, when `hits` is given,
-// positive windows.  One warp per segment; counters are accumulated with
-// atomics because long records span several segments.
-struct StatSegment {
-    uint64_t record;
-    uint64_t begin;  // first window start of the segment (record-relative)
-    uint64_t end;    // one past the last window start
-};
-
-__device__ __forceinline__ bool dna_valid(uint8_t b) {
-    const uint8_t u = b & 0xDFu;
-    return u == 'A' || u == 'C' || u == 'G' || u == 'T';
-}
-
-__global__ void record_stats_kernel(const uint8_t* norm, const uint64_t* out_off,
-                                    const sbf_record_range* ranges, const StatSegment* segs,
-                                    uint64_t n_segs, uint32_t k, const uint8_t* hits,
-                                    unsigned long long* valid_out,
-                                    unsigned long long* positive_out) {
-    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31;
-    for (uint64_t s = warp; s < n_segs; s += warps) {
-        const StatSegment sg = segs[s];
-        const uint8_t* rec = norm + out_off[sg.record];
-        const uint64_t size = ranges[sg.record].sequence_bytes;
-        // A window starting at p is valid iff bytes [p, p+k) are all valid.
-        // Scan window ends e in [begin+k-1, end+k-1) tracking the position of
-        // the last invalid byte, starting k-1 bytes early so the first window
-        // sees its whole span.
-        const uint64_t scan0 = sg.begin;
-        const uint64_t scan1 = sg.end + k - 1;  // <= size
-        int64_t last_inv = static_cast<int64_t>(scan0) - 1;  // nothing invalid before scan0 matters
-        unsigned long long valid = 0, pos = 0;
-        for (uint64_t base = scan0; base < scan1; base += 32) {
-            const uint64_t e = base + lane;
-            const bool in = e < scan1;
-            const bool inv = in && !dna_valid(rec[e]);
-            const uint32_t m = __ballot_sync(0xFFFFFFFFu, inv);
-            const uint32_t upto = m & (0xFFFFFFFFu >> (31 - lane));
-            const int64_t li = upto ? static_cast<int64_t>(base) + (31 - __clz(upto)) : last_inv;
-            const bool window_valid = in && e >= scan0 + k - 1 && (static_cast<int64_t>(e) - li) >= k;
-            valid += __popc(__ballot_sync(0xFFFFFFFFu, window_valid));
-            if (m) last_inv = static_cast<int64_t>(base) + (31 - __clz(m));
-        }
-        (void)size;
-        if (hits) {
-            const uint8_t* h = hits + out_off[sg.record];
-            unsigned long long local = 0;
-            for (uint64_t p = sg.begin + lane; p < sg.end; p += 32) local += h[p];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xFFFFFFFFu, local, o);
-            pos = local;
-        }
-        if (lane == 0) {
-            if (valid) atomicAdd(valid_out + sg.record, valid);
-            if (hits && pos) atomicAdd(positive_out + sg.record, pos);
-        }
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Device staging of a host record batch
 // ---------------------------------------------------------------------------
@@ -227,12 +164,18 @@ int sbf_filter::stage_record_batch(const char* h_seq, uint64_t len, const sbf_re
     const uint64_t span = hi - lo;
     SBF_TRY(rb_dense.ensure(span + 16));
     SBF_TRY(rb_norm.ensure(norm_len + 16));
-    SBF_TRY(rb_meta.ensure(n * (sizeof(sbf_record_range) + sizeof(uint64_t)) + 64));
+    SBF_TRY(rb_meta.ensure(n * (2 * sizeof(sbf_record_range) + sizeof(uint64_t)) + 64));
     auto* d_ranges = static_cast<sbf_record_range*>(rb_meta.ptr);
     auto* d_off = reinterpret_cast<uint64_t*>(d_ranges + n);
+    // The records' places in the normalised buffer: the ranges of the
+    // ragged pass that inserts or queries it.
+    std::vector<sbf_record_range> norm(n);
+    for (uint64_t i = 0; i < n; ++i) norm[i] = sbf_record_range{out_off[i], r[i].sequence_bytes};
     SBF_CUDA(cudaMemcpyAsync(rb_dense.ptr, h_seq + lo, span, cudaMemcpyHostToDevice, st));
     SBF_CUDA(cudaMemcpyAsync(d_ranges, r, n * sizeof(sbf_record_range), cudaMemcpyHostToDevice, st));
     SBF_CUDA(cudaMemcpyAsync(d_off, out_off.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    SBF_CUDA(cudaMemcpyAsync(d_off + n, norm.data(), n * sizeof(sbf_record_range),
+                             cudaMemcpyHostToDevice, st));
     const uint64_t segs = (norm_len + kGatherSegment - 1) / kGatherSegment;
     const uint64_t ctas = std::min<uint64_t>(segs, static_cast<uint64_t>(sms) * 8);
     normalize_gather_kernel<<<static_cast<unsigned>(ctas), 256, 0, st>>>(
@@ -244,40 +187,40 @@ int sbf_filter::stage_record_batch(const char* h_seq, uint64_t len, const sbf_re
     return SBF_OK;
 }
 
-// Per-record valid (and, with hits, positive) counts into host vectors.
-int sbf_filter::record_stats(const sbf_record_range* r, uint64_t n, const uint8_t* d_hits,
-                             cudaStream_t st, std::vector<uint64_t>& valid,
-                             std::vector<uint64_t>& positive) {
+// One ragged pass over the staged normalised batch: inserts or queries it
+// and returns per-record valid (and, for queries, positive) windows, counted
+// in the kernel's epilogue.  d_hits (query, optional) receives the hit bytes
+// in the normalised layout.
+int sbf_filter::record_pass(bool query, uint64_t n, uint64_t norm_len, uint8_t* d_hits,
+                            cudaStream_t st, std::vector<uint64_t>& valid,
+                            std::vector<uint64_t>& positive, uint64_t* total_valid) {
     valid.assign(n, 0);
     positive.assign(n, 0);
-    std::vector<StatSegment> segs;
-    segs.reserve(n);
-    for (uint64_t i = 0; i < n; ++i) {
-        const uint64_t size = r[i].sequence_bytes;
-        if (size < k) continue;
-        const uint64_t windows = size - k + 1;
-        for (uint64_t b = 0; b < windows; b += kStatSegment)
-            segs.push_back(StatSegment{i, b, std::min<uint64_t>(windows, b + kStatSegment)});
-    }
-    if (segs.empty()) return SBF_OK;
-    SBF_TRY(rb_stats.ensure(segs.size() * sizeof(StatSegment) + 2 * n * 8 + 64));
-    auto* d_segs = static_cast<StatSegment*>(rb_stats.ptr);
-    auto* d_valid = reinterpret_cast<unsigned long long*>(d_segs + segs.size());
+    *total_valid = 0;
+    const uint64_t windows = kmers_of(norm_len);
+    if (n == 0 || windows == 0) return SBF_OK;
+    SBF_TRY(rb_stats.ensure((2 * n + 2) * sizeof(uint64_t) + 64));
+    auto* d_counts = static_cast<uint64_t*>(rb_stats.ptr);
+    auto* d_valid = d_counts + 2;
     auto* d_pos = d_valid + n;
-    SBF_CUDA(cudaMemcpyAsync(d_segs, segs.data(), segs.size() * sizeof(StatSegment),
-                             cudaMemcpyHostToDevice, st));
-    SBF_CUDA(cudaMemsetAsync(d_valid, 0, 2 * n * 8, st));
-    const auto* d_ranges = static_cast<const sbf_record_range*>(rb_meta.ptr);
-    const auto* d_off = reinterpret_cast<const uint64_t*>(d_ranges + n);
-    const uint64_t warps = std::min<uint64_t>(segs.size(), static_cast<uint64_t>(sms) * 64);
-    record_stats_kernel<<<static_cast<unsigned>((warps * 32 + 255) / 256), 256, 0, st>>>(
-        static_cast<const uint8_t*>(rb_norm.ptr), d_off, d_ranges, d_segs, segs.size(), k,
-        d_hits, d_valid, d_pos);
-    SBF_CUDA(cudaGetLastError());
-    SBF_CUDA(cudaMemcpyAsync(valid.data(), d_valid, n * 8, cudaMemcpyDeviceToHost, st));
-    if (d_hits)
+    const auto* d_norm = reinterpret_cast<const sbf_record_range*>(
+        reinterpret_cast<const uint64_t*>(static_cast<const sbf_record_range*>(rb_meta.ptr) + n) + n);
+    const char* seq = static_cast<const char*>(rb_norm.ptr);
+    SBF_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(uint64_t), st));
+    unsigned long long tot[2] = {0, 0};
+    if (query) {
+        SBF_TRY(sbf_ragged_contains_counts_async(this, seq, norm_len, d_norm, n, d_hits, windows,
+                                                 d_valid, d_pos, d_counts,
+                                                 reinterpret_cast<sbf_stream_t>(st)));
+        SBF_CUDA(cudaMemcpyAsync(valid.data(), d_valid, n * 8, cudaMemcpyDeviceToHost, st));
         SBF_CUDA(cudaMemcpyAsync(positive.data(), d_pos, n * 8, cudaMemcpyDeviceToHost, st));
+    } else {
+        SBF_TRY(sbf_ragged_insert_async(this, seq, norm_len, d_norm, n, d_counts,
+                                        reinterpret_cast<sbf_stream_t>(st)));
+    }
+    SBF_CUDA(cudaMemcpyAsync(tot, d_counts, sizeof(tot), cudaMemcpyDeviceToHost, st));
     SBF_CUDA(cudaStreamSynchronize(st));
+    *total_valid = tot[0];
     return SBF_OK;
 }
 
@@ -404,12 +347,9 @@ extern "C" int sbf_insert_record_batch(sbf_filter_t* f, const char* h_seq, uint6
     SBF_TRY(f->stage_record_batch(h_seq, len, ranges, n, st, off, norm_len));
     sbf_insert_report rep{n, 0, 0};
     for (uint64_t i = 0; i < n; ++i) rep.indexed_bases += ranges[i].sequence_bytes;
-    const uint64_t windows = f->kmers_of(norm_len);
-    if (windows) {
-        SBF_TRY(f->launch(false, false, f->rb_norm.ptr, norm_len, windows, nullptr, st));
+    if (f->kmers_of(norm_len)) {
         std::vector<uint64_t> valid, pos;
-        SBF_TRY(f->record_stats(ranges, n, nullptr, st, valid, pos));
-        for (uint64_t v : valid) rep.inserted_kmers += v;
+        SBF_TRY(f->record_pass(false, n, norm_len, nullptr, st, valid, pos, &rep.inserted_kmers));
         SBF_TRY(f->check_device_error(st));
     }
     if (report) *report = rep;
@@ -433,13 +373,18 @@ extern "C" int sbf_query_record_batch(const sbf_filter_t* cf, const char* h_seq,
     std::vector<uint64_t> valid(n, 0), pos(n, 0);
     std::vector<uint8_t> hits;
     if (windows) {
-        SBF_TRY(f->rb_hits.ensure(windows + 64));
-        auto* d_hits = static_cast<uint8_t*>(f->rb_hits.ptr);
-        SBF_TRY(f->launch(true, false, f->rb_norm.ptr, norm_len, windows, d_hits, st));
-        SBF_TRY(f->record_stats(ranges, n, d_hits, st, valid, pos));
+        // Hit bytes are written only when a consumer reads them.
+        uint8_t* d_hits = nullptr;
+        if (consume) {
+            SBF_TRY(f->rb_hits.ensure(windows + 64));
+            d_hits = static_cast<uint8_t*>(f->rb_hits.ptr);
+        }
+        uint64_t total = 0;
+        SBF_TRY(f->record_pass(true, n, norm_len, d_hits, st, valid, pos, &total));
         if (consume) {
             hits.resize(windows);
             SBF_CUDA(cudaMemcpyAsync(hits.data(), d_hits, windows, cudaMemcpyDeviceToHost, st));
+            SBF_CUDA(cudaStreamSynchronize(st));
         }
         SBF_TRY(f->check_device_error(st));
     }

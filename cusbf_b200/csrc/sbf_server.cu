@@ -54,12 +54,22 @@ constexpr uint64_t kDirectBytes = 256 << 10;  // pinned spans at least this size
 uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
 // Operations: 0 insert, 1 query (one byte per window), 2 query with
-// bit-packed results.  Bit-packed requests start at multiples of 32 bytes
-// of the batch, so each request's bits start on a word boundary.
-constexpr int kOpInsert = 0, kOpQuery = 1, kOpQueryBits = 2;
+// bit-packed results, 3 query returning per-record counts only (two uint64
+// per record: valid windows, positive windows; computed in the query
+// kernel's epilogue, no hit bytes written).  Bit-packed requests start at
+// multiples of 32 bytes of the batch, so each request's bits start on a word
+// boundary.
+constexpr int kOpInsert = 0, kOpQuery = 1, kOpQueryBits = 2, kOpQueryCounts = 3;
 uint64_t pad_of(int op) { return op == kOpQueryBits ? 32 : 16; }
-uint64_t result_bytes(int op, uint64_t windows) {
-    return op == kOpQueryBits ? (windows + 31) / 32 * 4 : op == kOpQuery ? windows : 0;
+uint64_t result_bytes(int op, uint64_t windows, uint64_t records) {
+    return op == kOpQueryBits     ? (windows + 31) / 32 * 4
+           : op == kOpQuery       ? windows
+           : op == kOpQueryCounts ? records * 16
+                                  : 0;
+}
+// Device bytes of a batch's result region.
+uint64_t out_region(int op, uint64_t seq_bytes, uint64_t records) {
+    return op == kOpInsert ? 0 : align_up(op == kOpQueryCounts ? records * 16 : seq_bytes, kAlign);
 }
 
 // FIFO ring allocator: regions are released in allocation order.  The
@@ -121,7 +131,8 @@ struct SrvRequest {
 struct SrvBatch {
     int op = 0;
     std::vector<SrvRequest*> reqs;
-    std::vector<uint64_t> req_off;
+    std::vector<uint64_t> req_off;  // each request's first byte in the batch
+    std::vector<uint64_t> req_rec;  // each request's first record in the batch
     uint64_t seq_bytes = 0, n_ranges = 0;
     uint64_t dev_off = 0, dev_bytes = 0, pin_off = 0, pin_bytes = 0;
     bool complete = false;
@@ -273,7 +284,7 @@ void Server::run() {
             ++take;
         }
         const uint64_t n_tiles = seq / kTileKmers + 2;
-        const uint64_t dev_bytes = align_up(seq, kAlign) + (b->op ? align_up(seq, kAlign) : 0) +
+        const uint64_t dev_bytes = align_up(seq, kAlign) + out_region(b->op, seq, nr) +
                                    align_up(nr * sizeof(DevRange), kAlign) +
                                    align_up(n_tiles * 4, kAlign) +
                                    align_up(take * sizeof(FixEntry), kAlign);
@@ -357,11 +368,12 @@ void Server::run() {
 int Server::launch(SrvBatch* b) {
     const bool query = b->op != kOpInsert;
     const bool bits = b->op == kOpQueryBits;
+    const bool tally = b->op == kOpQueryCounts;
     uint8_t* dbase = d_ring + b->dev_off;
     uint8_t* d_seq = dbase;
     uint8_t* d_out = query ? dbase + align_up(b->seq_bytes, kAlign) : nullptr;
     auto* d_rng = reinterpret_cast<DevRange*>(dbase + align_up(b->seq_bytes, kAlign) +
-                                              (query ? align_up(b->seq_bytes, kAlign) : 0));
+                                              out_region(b->op, b->seq_bytes, b->n_ranges));
     auto* d_tile = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(d_rng) +
                                                align_up(b->n_ranges * sizeof(DevRange), kAlign));
     auto* d_fix = reinterpret_cast<FixEntry*>(
@@ -385,11 +397,13 @@ int Server::launch(SrvBatch* b) {
     };
     cudaError_t e;
     b->req_off.resize(b->reqs.size());
+    b->req_rec.resize(b->reqs.size());
     for (size_t i = 0; i < b->reqs.size(); ++i) {
         SrvRequest* r = b->reqs[i];
         const uint64_t span = r->hi - r->lo;
         const uint64_t padded = align_up(span, pad_of(r->op));
         b->req_off[i] = o;
+        b->req_rec[i] = k;
         if (r->n) {
             // One bulk copy of the client's ranges; offsets are rebased on the GPU.
             std::memcpy(h_rng + k, r->ranges, r->n * sizeof(DevRange));
@@ -432,15 +446,23 @@ int Server::launch(SrvBatch* b) {
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "rebase_ranges_kernel");
     }
     if (k) {
-        const TileParams p =
-            ragged_params(f, query, d_seq, b->seq_bytes, d_rng, k, d_tile, d_out, d_ctl,
-                          reinterpret_cast<unsigned long long*>(d_ctl + 2) + (query ? 2 : 0),
+        TileParams p =
+            ragged_params(f, query, d_seq, b->seq_bytes, d_rng, k, d_tile, tally ? nullptr : d_out,
+                          d_ctl, reinterpret_cast<unsigned long long*>(d_ctl + 2) + (query ? 2 : 0),
                           bits);
+        if (tally) {
+            // (valid, positive) pairs per record, accumulated by the kernel.
+            if ((e = cudaMemsetAsync(d_out, 0, k * 16, comp)) != cudaSuccess)
+                return cuda_fail(e, "cudaMemsetAsync");
+            p.rec_valid = reinterpret_cast<unsigned long long*>(d_out);
+            p.rec_pos = p.rec_valid + 1;
+            p.rec_shift = 1;
+        }
         const int rc = cfg.use_graph
                            ? ragged_graph_launch(f, graph[query ? 1 : 0], query, p, 0, comp)
                            : ragged_launch(f, query, p, 0, comp);
         if (rc != SBF_OK) return rc;
-    } else if (query && b->seq_bytes) {
+    } else if (query && !tally && b->seq_bytes) {
         if ((e = cudaMemsetAsync(d_out, 0, b->seq_bytes, comp)) != cudaSuccess)
             return cuda_fail(e, "cudaMemsetAsync");
     }
@@ -454,9 +476,9 @@ int Server::launch(SrvBatch* b) {
         return cuda_fail(e, "cudaStreamWaitEvent");
     for (size_t i = 0; i < b->reqs.size(); ++i) {
         SrvRequest* r = b->reqs[i];
-        if (r->windows == 0) continue;
-        const uint64_t src = bits ? b->req_off[i] / 8 : b->req_off[i];
-        if ((e = cudaMemcpyAsync(r->out, d_out + src, result_bytes(b->op, r->windows),
+        if (tally ? r->n == 0 : r->windows == 0) continue;
+        const uint64_t src = tally ? b->req_rec[i] * 16 : bits ? b->req_off[i] / 8 : b->req_off[i];
+        if ((e = cudaMemcpyAsync(r->out, d_out + src, result_bytes(b->op, r->windows, r->n),
                                  cudaMemcpyDeviceToHost, down)) != cudaSuccess)
             return cuda_fail(e, "cudaMemcpyAsync(hits)");
     }
@@ -545,9 +567,10 @@ extern "C" int sbf_server_submit(sbf_server_t* h, int op, const char* base,
                                  uint64_t out_len, double arrival, uint64_t* ticket) {
     if (!h || !ticket) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     Server& s = h->s;
-    if (op != kOpInsert && op != kOpQuery && op != kOpQueryBits)
+    if (op != kOpInsert && op != kOpQuery && op != kOpQueryBits && op != kOpQueryCounts)
         return set_error(SBF_ERR_INVALID_ARGUMENT,
-                         "op must be 0 (insert), 1 (query) or 2 (query, bit-packed)");
+                         "op must be 0 (insert), 1 (query), 2 (query, bit-packed) or 3 (query, "
+                         "per-record counts)");
     if (n && (!ranges || !base)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     auto r = std::make_unique<SrvRequest>();
     r->op = op;
@@ -565,7 +588,8 @@ extern "C" int sbf_server_submit(sbf_server_t* h, int op, const char* base,
     }
     const uint64_t span = r->hi - r->lo;
     r->windows = span >= s.f->k ? span - s.f->k + 1 : 0;
-    if (op != kOpInsert && r->windows && (!out || out_len < result_bytes(op, r->windows)))
+    const bool has_result = op == kOpQueryCounts ? n > 0 : (op != kOpInsert && r->windows > 0);
+    if (has_result && (!out || out_len < result_bytes(op, r->windows, n)))
         return set_error(SBF_ERR_INVALID_ARGUMENT, "query output span is too small");
     if (align_up(span, pad_of(op)) > s.cfg.max_batch_bytes || n * sizeof(DevRange) > s.cfg.max_batch_bytes)
         return set_error(SBF_ERR_INVALID_ARGUMENT,

@@ -338,6 +338,18 @@ int sbf_ragged_insert_async(sbf_filter_t* filter, const char* d_seq, uint64_t le
 int sbf_ragged_contains_async(const sbf_filter_t* filter, const char* d_seq, uint64_t len,
                               const sbf_record_range* d_ranges, uint64_t n, uint8_t* d_out,
                               uint64_t out_len, uint64_t* d_counts, sbf_stream_t stream);
+/* The device-resident ragged query with per-record counts computed in the
+ * query kernel's epilogue (the reference computes them in a second pass:
+ * count_positive_kmers_per_record, detail/count_positive_kmers.cuh:21-45,
+ * called from filter.cuh:1055).  d_record_valid[r] and d_record_positive[r]
+ * (device, n x uint64, zeroed here) receive record r's valid and positive
+ * windows.  d_out is optional: NULL computes the counts without writing any
+ * hit bytes; otherwise it is filled as by sbf_ragged_contains_async. */
+int sbf_ragged_contains_counts_async(const sbf_filter_t* filter, const char* d_seq, uint64_t len,
+                                     const sbf_record_range* d_ranges, uint64_t n,
+                                     uint8_t* d_out, uint64_t out_len, uint64_t* d_record_valid,
+                                     uint64_t* d_record_positive, uint64_t* d_counts,
+                                     sbf_stream_t stream);
 /* Host batches through the chunked pipeline (ranges validated as for
  * record batches).  `tuning` NULL uses the tuning table entry for the
  * batch's shape when there is one, else defaults.  Synchronous. */
@@ -413,7 +425,9 @@ void sbf_server_destroy(sbf_server_t* server);
 double sbf_server_now(void);
 /* Queues a request: op 0 = insert, 1 = query, 2 = query with bit-packed
  * results (out[] as 32-bit words, bit i % 32 of word i / 32 for window i;
- * out_len >= 4 * ceil((span - k + 1) / 32)).  Records are (offset, bytes)
+ * out_len >= 4 * ceil((span - k + 1) / 32)), 3 = query returning only
+ * per-record counts (out[] as 2n uint64: record r's valid windows at 2r,
+ * positive windows at 2r + 1; out_len >= 16 n).  Records are (offset, bytes)
  * ranges into `base`, ordered and non-overlapping; the request's span is
  * [ranges[0].offset, end of ranges[n-1]).  A query writes one byte per
  * window of the span to out[0 .. span - k] (out_len >= span - k + 1): the

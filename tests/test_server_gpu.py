@@ -239,3 +239,49 @@ def test_bit_packed_requests_match_bytes(sbf, cuda):
             np.testing.assert_array_equal(hits, b.view(np.uint32))
     srv.close()
     np.testing.assert_array_equal(f.words_host(), want_words)
+
+
+_VALID = np.zeros(256, bool)
+_VALID[np.frombuffer(b"ACGTacgt", np.uint8)] = True
+
+
+def _record_counts(base, ranges, span_hits, k=31):
+    """Per-record (valid, positive) windows from a request's byte results."""
+    lo = int(ranges[0, 0])
+    out = np.zeros((ranges.shape[0], 2), np.uint64)
+    for i, (off, ln) in enumerate(ranges.astype(np.int64)):
+        if ln < k:
+            continue
+        bad = np.concatenate([[0], np.cumsum(~_VALID[base[off:off + ln]])])
+        out[i, 0] = int(((bad[k:] - bad[:-k]) == 0).sum())
+        out[i, 1] = int(span_hits[off - lo:off - lo + ln - k + 1].sum())
+    return out
+
+
+@pytest.mark.parametrize("cfg", [dict(), dict(use_graph=1, max_inflight=2)],
+                         ids=["default", "graph"])
+def test_count_requests_match_bytes(sbf, cuda, cfg):
+    """Op 3 returns each record's valid and positive windows (counted in the
+    query kernel's epilogue), interleaved with byte and bit-packed queries
+    and inserts, equal to the counts of the serial byte results."""
+    rng = np.random.default_rng(37)
+    genome = random_dna(rng, 300_000)
+    reqs = _make_requests(rng, genome, 150)
+    bits = 1 << 22
+    want, want_words = _serial(sbf, genome, reqs, bits)
+    f = sbf.Filter(bits, **K31)
+    f.insert_sequence(genome)
+    srv = sbf.Server(f, staging_bytes=1 << 28, pinned_bytes=1 << 26, **cfg)
+    ops = [op if op == 0 else (1, 2, 3)[i % 3] for i, (op, _, _) in enumerate(reqs)]
+    tickets = [srv.submit(op, base, ranges) for op, (_, base, ranges) in zip(ops, reqs)]
+    n_counts = 0
+    for op, t, w, (_, base, ranges) in zip(ops, tickets, want, reqs):
+        _, res = srv.wait(t, timeout=60.0)
+        if op == 1:
+            np.testing.assert_array_equal(res, w)
+        elif op == 3:
+            np.testing.assert_array_equal(res, _record_counts(base, ranges, w))
+            n_counts += 1
+    srv.close()
+    assert n_counts > 20
+    np.testing.assert_array_equal(f.words_host(), want_words)
