@@ -217,6 +217,9 @@ _sig("sbf_contains_sequence", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp)
 _sig("sbf_dense_packed_word_count", _u64, _u64)
 _sig("sbf_pack_dense_device", C.c_int, _vp, _u64, _vp, _vp)
 _sig("sbf_pack_dense_host", C.c_int, _vp, _u64, _vp)
+_sig("sbf_dense_packed_word_count_for", _u64, C.c_int, _u64)
+_sig("sbf_pack_dense_device_for", C.c_int, C.c_int, _vp, _u64, _vp, _vp)
+_sig("sbf_pack_dense_host_for", C.c_int, C.c_int, _vp, _u64, _vp)
 _sig("sbf_insert_dense_packed_async", C.c_int, _vp, _vp, _u64, _u64, _vp, C.POINTER(_u64))
 _sig("sbf_insert_dense_packed", C.c_int, _vp, _vp, _u64, _u64, _vp, C.POINTER(_u64))
 _sig("sbf_contains_dense_packed_async", C.c_int, _vp, _vp, _u64, _u64, _vp, _u64, _vp)
@@ -483,8 +486,9 @@ class Filter:
 
     # -- dense packed input -------------------------------------------------
     @staticmethod
-    def dense_packed_word_count(num_symbols: int) -> int:
-        return _lib.sbf_dense_packed_word_count(num_symbols)
+    def dense_packed_word_count(num_symbols: int, alphabet: int = ALPHABET_DNA) -> int:
+        """Words of `num_symbols` dense symbols (64 / symbolBits per word)."""
+        return _lib.sbf_dense_packed_word_count_for(alphabet, num_symbols)
 
     def insert_dense_packed_async(self, d_words, num_symbols: int, stream=None) -> int:
         p, nb = _dev_ptr(d_words)
@@ -508,7 +512,7 @@ class Filter:
 
     def contains_dense_packed(self, words, num_symbols: int, d_out=None, stream=None):
         w = np.ascontiguousarray(words, dtype=np.uint64)
-        n = self.kmer_count(num_symbols)
+        n = max(num_symbols - self.config.k + 1, 0)
         if d_out is not None:
             o, on = _dev_ptr(d_out)
             _check(_lib.sbf_contains_dense_packed_to_device(self._h, _np_ptr(w), w.size,
@@ -884,20 +888,29 @@ def _fastx_methods():
 _fastx_methods()
 
 
-def pack_dense_sequence(seq) -> np.ndarray:
-    """Host dense packing (include/cusbf/dense_packed.hpp:36-50), DNA."""
+_SYMBOL_WIDTH = {ALPHABET_DNA: 1, ALPHABET_PROTEIN: 1, ALPHABET_DNA_TRIPLET: 3}
+
+
+def pack_dense_sequence(seq, alphabet: int = ALPHABET_DNA) -> np.ndarray:
+    """Host dense packing (include/cusbf/dense_packed.hpp:36-50): one symbol
+    per symbolWidth input bytes, 64 / symbolBits symbols per word."""
     b = _host_bytes(seq)
-    n_words = _lib.sbf_dense_packed_word_count(b.size)
+    n_sym = b.size // _SYMBOL_WIDTH[alphabet]
+    n_words = _lib.sbf_dense_packed_word_count_for(alphabet, n_sym)
     out = np.zeros(max(n_words, 1), dtype=np.uint64)
-    _check(_lib.sbf_pack_dense_host(_np_ptr(b), b.size, _np_ptr(out)))
+    _check(_lib.sbf_pack_dense_host_for(alphabet, _np_ptr(b), n_sym, _np_ptr(out)))
     return out[:n_words]
 
 
-def pack_dense_sequence_device(d_seq, num_symbols: int, d_words, stream=None) -> None:
+def pack_dense_sequence_device(d_seq, num_symbols: int, d_words, stream=None,
+                               alphabet: int = ALPHABET_DNA) -> None:
     """Device dense packing (include/cusbf/dense_packed.hpp:58-74)."""
     p, _ = _dev_ptr(d_seq)
     w, _ = _dev_ptr(d_words)
-    _check(_lib.sbf_pack_dense_device(p, num_symbols, w, _stream(stream)))
+    if alphabet == ALPHABET_DNA:
+        _check(_lib.sbf_pack_dense_device(p, num_symbols, w, _stream(stream)))
+    else:
+        _check(_lib.sbf_pack_dense_device_for(alphabet, p, num_symbols, w, _stream(stream)))
 
 
 __all__ = [

@@ -140,6 +140,14 @@ uint64_t sbf_filter::kmers_of(uint64_t symbols) const {
     return symbols < k ? 0 : symbols - k + 1;
 }
 
+int sbf_filter::require_byte_symbols(const char* what) const {
+    if (width == 1) return SBF_OK;
+    return set_error(SBF_ERR_INVALID_ARGUMENT,
+                     "%s needs a one-byte alphabet; DNA triplets are supported by the sequence and "
+                     "dense-packed entry points",
+                     what);
+}
+
 int sbf_filter::launch(bool query, bool dense, const void* input, uint64_t input_bytes,
                        uint64_t n_kmers, uint8_t* out, cudaStream_t st,
                        uint32_t* out_bits) const {
@@ -165,6 +173,7 @@ int sbf_filter::launch(bool query, bool dense, const void* input, uint64_t input
     p.out_bits = out_bits;
     p.n_tiles = (n_kmers + static_cast<uint64_t>(phase) + kTileKmers - 1) / kTileKmers;
     p.err = d_err;
+    p.gen = gen;
     const int which = (query ? 1 : 0) + (dense ? 2 : 0);
     void (*fn)(TileParams) = which == 0   ? ks->insert_bytes
                              : which == 1 ? ks->query_bytes
@@ -205,10 +214,14 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
     // 32 symbols per 8-byte word, so chunks are cut at word boundaries.
     const uint64_t chunk_target = host_chunk_bytes();
     uint64_t chunk_kmers;
+    const uint64_t per_word = dense_per_word();
     if (dense) {
-        chunk_kmers = std::max<uint64_t>((chunk_target * 4) / 32 * 32, 1024);
+        // About chunk_target packed bytes, a whole number of words.
+        const uint64_t syms = chunk_target / 8 * per_word;
+        chunk_kmers = std::max<uint64_t>(syms / per_word * per_word, 1024 / per_word * per_word);
     } else {
-        chunk_kmers = bits ? std::max<uint64_t>(chunk_target / 32 * 32, 1024) : chunk_target;
+        const uint64_t t = chunk_target / width;
+        chunk_kmers = bits ? std::max<uint64_t>(t / 32 * 32, 1024) : t;
     }
     const uint64_t n_chunks = (n_kmers + chunk_kmers - 1) / chunk_kmers;
     auto chunk_span = [&](uint64_t c, uint64_t& first_byte, uint64_t& bytes, uint64_t& kmers,
@@ -217,16 +230,17 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
         kmers = std::min<uint64_t>(chunk_kmers, n_kmers - w0);
         const uint64_t syms = kmers + k - 1;
         if (dense) {
-            first_byte = (w0 / 32) * 8;
-            sym_offset = w0 % 32;  // always 0: chunk_kmers is a multiple of 32
-            bytes = std::min<uint64_t>(((sym_offset + syms + 31) / 32) * 8, in_bytes - first_byte);
+            first_byte = (w0 / per_word) * 8;
+            sym_offset = w0 % per_word;  // always 0: chunk_kmers is a multiple of per_word
+            bytes = std::min<uint64_t>(dense_words(sym_offset + syms) * 8, in_bytes - first_byte);
         } else {
-            first_byte = w0;
+            first_byte = w0 * width;
             sym_offset = 0;
-            bytes = syms;
+            bytes = syms * width;
         }
     };
-    const uint64_t max_in = dense ? ((chunk_kmers + k - 1 + 31) / 32) * 8 + 8 : chunk_kmers + k;
+    const uint64_t max_in =
+        dense ? dense_words(chunk_kmers + k - 1) * 8 + 8 : (chunk_kmers + k) * width;
     const bool in_pinned = is_pinned(h_in);
     if (bits) out_host = reinterpret_cast<uint8_t*>(bits_host);
     // Output bytes of a chunk of `kmers` windows, and the chunk's output offset.
@@ -311,16 +325,33 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
                                  int alphabet, uint64_t requested_bits, sbf_filter_t** out) {
     if (!out) return set_error(SBF_ERR_INVALID_ARGUMENT, "output handle pointer is null");
     *out = nullptr;
-    if (alphabet != SBF_ALPHABET_DNA)
+    // Symbol geometry of the alphabet (Alphabet.cuh; Config::symbolBits is
+    // bit_width(symbolCount - 1), config.cuh:45-60).
+    uint32_t bits = 0, width = 0;
+    switch (alphabet) {
+        case SBF_ALPHABET_DNA: bits = 2; width = 1; break;
+        case SBF_ALPHABET_PROTEIN: bits = 5; width = 1; break;
+        case SBF_ALPHABET_DNA_TRIPLET: bits = 6; width = 3; break;
+        default:
+            return set_error(SBF_ERR_INVALID_ARGUMENT, "unknown alphabet %d", alphabet);
+    }
+    // The reference's Config static_asserts (config.cuh:76-118).
+    if (k == 0 || k * bits > 64)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "k=%u does not fit one packed 64-bit k-mer", k);
+    if (m == 0 || m > k || s == 0 || s > k)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "need 0 < m <= k and 0 < s <= k (k=%u s=%u m=%u)",
+                         k, s, m);
+    if (hashes < 4 || hashes > 16 || hashes % 4 != 0)
         return set_error(SBF_ERR_INVALID_ARGUMENT,
-                         "alphabet %d is not implemented by the GPU engine (DNA only)", alphabet);
-    const KernelSet* ks = find_kernels(static_cast<int>(k), static_cast<int>(s),
-                                       static_cast<int>(m), static_cast<int>(hashes));
-    if (!ks)
-        return set_error(SBF_ERR_INVALID_ARGUMENT,
-                         "configuration k=%u s=%u m=%u hashes=%u is not compiled into this "
-                         "library",
-                         k, s, m, hashes);
+                         "hash count %u must be 4, 8, 12 or 16 (a multiple of the 4 shard words)",
+                         hashes);
+    // Specialised tile kernels for the compiled DNA configurations; the
+    // runtime-parameterised kernels for everything else.
+    const KernelSet* ks = alphabet == SBF_ALPHABET_DNA
+                              ? find_kernels(static_cast<int>(k), static_cast<int>(s),
+                                             static_cast<int>(m), static_cast<int>(hashes))
+                              : nullptr;
+    if (!ks) ks = generic_kernels();
     uint64_t blocks = requested_bits / 256 + (requested_bits % 256 != 0);
     if (blocks < 1) blocks = 1;
     uint64_t shards = 1;
@@ -331,6 +362,9 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
     f->s = s;
     f->m = m;
     f->h = hashes;
+    f->alphabet = alphabet;
+    f->width = width;
+    f->gen = GenericCfg{k, s, m, hashes, bits, width, static_cast<uint32_t>(alphabet)};
     f->num_shards = shards;
     f->filter_bits = shards * 256;
     int rc = SBF_OK;
@@ -436,7 +470,7 @@ extern "C" int sbf_filter_words(const sbf_filter_t* f, uint64_t** d_words, uint6
 }
 
 extern "C" uint64_t sbf_filter_kmer_count(const sbf_filter_t* f, uint64_t bytes) {
-    return f ? f->kmers_of(bytes) : 0;
+    return f ? f->kmers_of_bytes(bytes) : 0;
 }
 
 extern "C" int sbf_filter_load_factor(sbf_filter_t* f, sbf_stream_t stream, double* out) {
@@ -455,7 +489,7 @@ extern "C" int sbf_filter_load_factor(sbf_filter_t* f, sbf_stream_t stream, doub
 extern "C" int sbf_insert_sequence_async(sbf_filter_t* f, const char* d_seq, uint64_t bytes,
                                          sbf_stream_t stream, uint64_t* kmers_out) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    const uint64_t n = f->kmers_of(bytes);
+    const uint64_t n = f->kmers_of_bytes(bytes);
     if (kmers_out) *kmers_out = n;
     if (n == 0) return SBF_OK;
     if (!d_seq) return set_error(SBF_ERR_INVALID_ARGUMENT, "sequence pointer is null");
@@ -465,7 +499,7 @@ extern "C" int sbf_insert_sequence_async(sbf_filter_t* f, const char* d_seq, uin
 extern "C" int sbf_insert_sequence(sbf_filter_t* f, const char* h_seq, uint64_t bytes,
                                    sbf_stream_t stream, uint64_t* kmers_out) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    const uint64_t n = f->kmers_of(bytes);
+    const uint64_t n = f->kmers_of_bytes(bytes);
     if (kmers_out) *kmers_out = n;
     if (n == 0) return SBF_OK;
     if (!h_seq) return set_error(SBF_ERR_INVALID_ARGUMENT, "sequence pointer is null");
@@ -476,7 +510,7 @@ extern "C" int sbf_contains_sequence_async(const sbf_filter_t* f, const char* d_
                                            uint64_t bytes, uint8_t* d_out, uint64_t out_len,
                                            sbf_stream_t stream) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    const uint64_t n = f->kmers_of(bytes);
+    const uint64_t n = f->kmers_of_bytes(bytes);
     if (n == 0) return SBF_OK;
     if (!d_seq || !d_out) return set_error(SBF_ERR_INVALID_ARGUMENT, "null device pointer");
     if (out_len < n)
@@ -490,7 +524,7 @@ extern "C" int sbf_contains_sequence_to_device(const sbf_filter_t* f, const char
                                                uint64_t bytes, uint8_t* d_out, uint64_t out_len,
                                                sbf_stream_t stream) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    const uint64_t n = f->kmers_of(bytes);
+    const uint64_t n = f->kmers_of_bytes(bytes);
     if (n == 0) return SBF_OK;
     if (!h_seq || !d_out) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     if (out_len < n) return set_error(SBF_ERR_INVALID_ARGUMENT, "query output span is too small");
@@ -501,7 +535,7 @@ extern "C" int sbf_contains_sequence_to_device(const sbf_filter_t* f, const char
 extern "C" int sbf_contains_sequence(const sbf_filter_t* f, const char* h_seq, uint64_t bytes,
                                      uint8_t* h_out, uint64_t out_len, sbf_stream_t stream) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    const uint64_t n = f->kmers_of(bytes);
+    const uint64_t n = f->kmers_of_bytes(bytes);
     if (n == 0) return SBF_OK;
     if (!h_seq || !h_out) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     if (out_len < n) return set_error(SBF_ERR_INVALID_ARGUMENT, "query output span is too small");
@@ -515,7 +549,7 @@ extern "C" int sbf_contains_sequence_bits_async(const sbf_filter_t* f, const cha
                                                 uint64_t bytes, uint32_t* d_bits,
                                                 uint64_t n_words, sbf_stream_t stream) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    const uint64_t n = f->kmers_of(bytes);
+    const uint64_t n = f->kmers_of_bytes(bytes);
     if (n == 0) return SBF_OK;
     if (!d_seq || !d_bits) return set_error(SBF_ERR_INVALID_ARGUMENT, "null device pointer");
     if (reinterpret_cast<uintptr_t>(d_bits) & 3u)
@@ -531,7 +565,7 @@ extern "C" int sbf_contains_sequence_bits(const sbf_filter_t* f, const char* h_s
                                           uint64_t bytes, uint32_t* h_bits, uint64_t n_words,
                                           sbf_stream_t stream) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    const uint64_t n = f->kmers_of(bytes);
+    const uint64_t n = f->kmers_of_bytes(bytes);
     if (n == 0) return SBF_OK;
     if (!h_seq || !h_bits) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     if (n_words < (n + 31) / 32)
@@ -574,7 +608,7 @@ static int check_dense(const sbf_filter_t* f, const void* words, uint64_t n_word
                        uint64_t num_symbols) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
     if (!words) return set_error(SBF_ERR_INVALID_ARGUMENT, "dense word pointer is null");
-    if (n_words < (num_symbols + 31) / 32)
+    if (n_words < f->dense_words(num_symbols))
         return set_error(SBF_ERR_INVALID_ARGUMENT, "dense packed span is too small for num_symbols");
     return SBF_OK;
 }
@@ -587,7 +621,7 @@ extern "C" int sbf_insert_dense_packed_async(sbf_filter_t* f, const uint64_t* d_
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
     if (n == 0) return SBF_OK;
     SBF_TRY(check_dense(f, d_words, n_words, num_symbols));
-    return f->launch(false, true, d_words, ((num_symbols + 31) / 32) * 8, n, nullptr, S(stream));
+    return f->launch(false, true, d_words, f->dense_words(num_symbols) * 8, n, nullptr, S(stream));
 }
 
 extern "C" int sbf_insert_dense_packed(sbf_filter_t* f, const uint64_t* h_words,
@@ -598,7 +632,7 @@ extern "C" int sbf_insert_dense_packed(sbf_filter_t* f, const uint64_t* h_words,
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
     if (n == 0) return SBF_OK;
     SBF_TRY(check_dense(f, h_words, n_words, num_symbols));
-    return f->host_pipeline(false, true, h_words, ((num_symbols + 31) / 32) * 8, n, nullptr,
+    return f->host_pipeline(false, true, h_words, f->dense_words(num_symbols) * 8, n, nullptr,
                             nullptr, S(stream));
 }
 
@@ -612,7 +646,7 @@ extern "C" int sbf_contains_dense_packed_async(const sbf_filter_t* f, const uint
     SBF_TRY(check_dense(f, d_words, n_words, num_symbols));
     if (!d_out || out_len < n)
         return set_error(SBF_ERR_INVALID_ARGUMENT, "dense packed query output span is too small");
-    return f->launch(true, true, d_words, ((num_symbols + 31) / 32) * 8, n, d_out, S(stream));
+    return f->launch(true, true, d_words, f->dense_words(num_symbols) * 8, n, d_out, S(stream));
 }
 
 extern "C" int sbf_contains_dense_packed_to_device(const sbf_filter_t* f, const uint64_t* h_words,
@@ -626,7 +660,7 @@ extern "C" int sbf_contains_dense_packed_to_device(const sbf_filter_t* f, const 
     if (!d_out || out_len < n)
         return set_error(SBF_ERR_INVALID_ARGUMENT, "dense packed query output span is too small");
     return const_cast<sbf_filter*>(f)->host_pipeline(true, true, h_words,
-                                                     ((num_symbols + 31) / 32) * 8, n, nullptr,
+                                                     f->dense_words(num_symbols) * 8, n, nullptr,
                                                      d_out, S(stream));
 }
 
@@ -640,6 +674,6 @@ extern "C" int sbf_contains_dense_packed(const sbf_filter_t* f, const uint64_t* 
     if (!h_out || out_len < n)
         return set_error(SBF_ERR_INVALID_ARGUMENT, "dense packed query output span is too small");
     return const_cast<sbf_filter*>(f)->host_pipeline(true, true, h_words,
-                                                     ((num_symbols + 31) / 32) * 8, n, h_out,
+                                                     f->dense_words(num_symbols) * 8, n, h_out,
                                                      nullptr, S(stream));
 }

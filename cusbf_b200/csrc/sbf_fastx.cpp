@@ -366,6 +366,7 @@ int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const ch
               sbf_query_report* qrep, sbf_fastx_record_cb consume, void* cuser) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
     if (!read) return set_error(SBF_ERR_INVALID_ARGUMENT, "read callback is null");
+    if (const int bs = f->require_byte_symbols("FASTA/FASTQ input"); bs != SBF_OK) return bs;
     sbf_insert_report it{0, 0, 0};
     sbf_query_report qt{0, 0, 0, 0};
     auto finish = [&](int s) -> int {

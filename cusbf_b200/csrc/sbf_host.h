@@ -56,6 +56,9 @@ struct FastqDevice;
 struct sbf_filter {
     const sbf::KernelSet* ks = nullptr;
     uint32_t k = 0, s = 0, m = 0, h = 0;
+    int alphabet = 0;
+    uint32_t width = 1;  // input bytes per symbol (3 for DNA triplets)
+    sbf::GenericCfg gen{};
     uint64_t num_shards = 0;
     uint64_t filter_bits = 0;
     uint64_t* d_words = nullptr;
@@ -84,6 +87,16 @@ struct sbf_filter {
     sbf::DevBuf rb_dense, rb_norm, rb_meta, rb_hits, rb_stats;
 
     uint64_t kmers_of(uint64_t symbols) const;
+    // Windows of a byte sequence (symbols = bytes / width).
+    uint64_t kmers_of_bytes(uint64_t bytes) const { return kmers_of(bytes / width); }
+    // Dense packing: 64 / bits symbols per 64-bit word (32 for DNA).
+    uint64_t dense_per_word() const { return 64u / gen.bits; }
+    uint64_t dense_words(uint64_t symbols) const {
+        return (symbols + dense_per_word() - 1) / dense_per_word();
+    }
+    // Record-level paths (ragged batches, record batches, FASTX, the server)
+    // work on one-byte symbols only; SBF_OK or an invalid-argument error.
+    int require_byte_symbols(const char* what) const;
     int stage_record_batch(const char* h_seq, uint64_t len, const sbf_record_range* r, uint64_t n,
                            cudaStream_t st, std::vector<uint64_t>& out_off, uint64_t& norm_len);
     int record_pass(bool query, uint64_t n, uint64_t norm_len, uint8_t* d_hits, cudaStream_t st,

@@ -27,6 +27,15 @@ struct DevRange {
     uint64_t bytes;
 };
 
+// Configuration of the runtime-parameterised kernels (sbf_generic.cu), used
+// for every configuration and alphabet that has no specialised kernel.
+struct GenericCfg {
+    uint32_t k, s, m, h;
+    uint32_t bits;      // bits per packed symbol
+    uint32_t width;     // input bytes per symbol
+    uint32_t alphabet;  // SBF_ALPHABET_*
+};
+
 // One launch of a tile kernel.  Grid position g of tile n is
 // g = n * kTileKmers + (0 .. kTileKmers-1); it holds window (k-mer)
 // i = g + sym_base, and symbol i is the first base of that window.
@@ -54,6 +63,7 @@ struct TileParams {
     unsigned long long* rec_valid;
     unsigned long long* rec_pos;
     uint32_t rec_shift;
+    GenericCfg gen;  // read by the generic kernels only
 };
 
 // Device error codes written to TileParams::err.
@@ -62,7 +72,8 @@ enum : int {
     kDevErrStageTimeout = 1,  // a bulk-copy wait ran out of its time bound
 };
 
-// Function table for one compiled configuration <K,S,M,H>.
+// Function table for one compiled configuration <K,S,M,H> (k = s = m = h = 0
+// for the generic table, whose kernels read TileParams::gen).
 struct KernelSet {
     int k, s, m, h;
     void (*insert_bytes)(TileParams);
@@ -76,6 +87,8 @@ struct KernelSet {
 // Returns the kernel table for a configuration, or nullptr when it is not
 // compiled into this library.
 const KernelSet* find_kernels(int k, int s, int m, int h);
+// The runtime-parameterised kernels (sbf_generic.cu).
+const KernelSet* generic_kernels();
 
 // Auxiliary kernels (sbf_kernels.cu).
 cudaError_t launch_pack_dense(const uint8_t* seq, uint64_t num_symbols, uint64_t* words,

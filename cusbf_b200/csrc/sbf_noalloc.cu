@@ -124,6 +124,9 @@ extern "C" int sbf_record_batch_counts_noalloc(const sbf_filter_t* f, const char
                                                uint64_t* valid_out, uint64_t* positive_out) {
     using namespace sbf;
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (f->alphabet != SBF_ALPHABET_DNA)
+        return set_error(SBF_ERR_INVALID_ARGUMENT,
+                         "sbf_record_batch_counts_noalloc counts DNA windows only");
     if (n && (!ranges || !valid_out || !positive_out))
         return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     if (n > kNoAllocMaxRecords)

@@ -193,6 +193,7 @@ TileParams ragged_params(const sbf_filter* f, bool query, const uint8_t* d_seq,
     p.tile_rec = d_tile_rec;
     p.queue = queue;
     p.counts = counts;
+    p.gen = f->gen;
     return p;
 }
 
@@ -489,6 +490,7 @@ static int ragged_async(sbf_filter_t* f, bool query, const char* d_seq, uint64_t
                         uint64_t out_len, uint64_t* d_counts, sbf_stream_t stream,
                         uint64_t* d_rec_valid = nullptr, uint64_t* d_rec_pos = nullptr) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    SBF_TRY(f->require_byte_symbols("ragged batches"));
     if (n && !d_ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "ranges pointer is null");
     if (n > 0xFFFFFFFFull) return set_error(SBF_ERR_INVALID_ARGUMENT, "too many records");
     const bool tally = d_rec_valid != nullptr;
@@ -561,6 +563,7 @@ extern "C" int sbf_ragged_insert(sbf_filter_t* f, const char* h_seq, uint64_t le
                                  const sbf_ragged_tuning* tuning, sbf_stream_t stream,
                                  sbf_insert_report* report) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    SBF_TRY(f->require_byte_symbols("ragged batches"));
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     SBF_TRY(validate_ranges(len, ranges, n));
     sbf_ragged_tuning t{};
@@ -582,6 +585,7 @@ extern "C" int sbf_ragged_query(const sbf_filter_t* cf, const char* h_seq, uint6
                                 sbf_stream_t stream, sbf_query_report* report) {
     auto* f = const_cast<sbf_filter*>(cf);
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    SBF_TRY(f->require_byte_symbols("ragged batches"));
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     SBF_TRY(validate_ranges(len, ranges, n));
     const uint64_t W = f->kmers_of(len);
@@ -618,6 +622,7 @@ extern "C" int sbf_ragged_autotune(sbf_filter_t* f, int query, const char* h_seq
                                    uint64_t sample_bytes, sbf_stream_t stream,
                                    sbf_ragged_tuning* chosen) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    SBF_TRY(f->require_byte_symbols("ragged batches"));
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     SBF_TRY(validate_ranges(len, ranges, n));
     if (sample_bytes == 0) sample_bytes = uint64_t{256} << 20;

@@ -312,10 +312,10 @@ extern "C" int sbf_insert_record_batch_async(sbf_filter_t* f, const char* d_seq,
     if (n && !ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "ranges pointer is null");
     SBF_TRY(validate_ranges(len, ranges, n));
     uint64_t total = 0;
-    for (uint64_t i = 0; i < n; ++i) total += f->kmers_of(ranges[i].sequence_bytes);
+    for (uint64_t i = 0; i < n; ++i) total += f->kmers_of_bytes(ranges[i].sequence_bytes);
     if (kmers_out) *kmers_out = total;
     if (total == 0) return SBF_OK;
-    return f->launch(false, false, d_seq, len, f->kmers_of(len), nullptr, S(stream));
+    return f->launch(false, false, d_seq, len, f->kmers_of_bytes(len), nullptr, S(stream));
 }
 
 extern "C" int sbf_contains_record_batch_async(const sbf_filter_t* f, const char* d_seq,
@@ -325,7 +325,7 @@ extern "C" int sbf_contains_record_batch_async(const sbf_filter_t* f, const char
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
     if (n && !ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "ranges pointer is null");
     SBF_TRY(validate_ranges(len, ranges, n));
-    const uint64_t total = f->kmers_of(len);
+    const uint64_t total = f->kmers_of_bytes(len);
     if (total == 0) return SBF_OK;
     if (!d_out || out_len < total)
         return set_error(SBF_ERR_INVALID_ARGUMENT, "record batch query output span is too small");
@@ -340,6 +340,7 @@ extern "C" int sbf_insert_record_batch(sbf_filter_t* f, const char* h_seq, uint6
                                        const sbf_record_range* ranges, uint64_t n,
                                        sbf_stream_t stream, sbf_insert_report* report) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    SBF_TRY(f->require_byte_symbols("host record batches"));
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     cudaStream_t st = S(stream);
     std::vector<uint64_t> off;
@@ -362,6 +363,7 @@ extern "C" int sbf_query_record_batch(const sbf_filter_t* cf, const char* h_seq,
                                       sbf_record_query_cb consume, void* user) {
     auto* f = const_cast<sbf_filter*>(cf);
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    SBF_TRY(f->require_byte_symbols("host record batches"));
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     cudaStream_t st = S(stream);
     std::vector<uint64_t> off;

@@ -498,6 +498,7 @@ extern "C" int sbf_server_create(sbf_filter_t* f, const sbf_server_config* confi
                                  sbf_server_t** out) {
     if (!f || !out) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     *out = nullptr;
+    if (const int bs = f->require_byte_symbols("the request server"); bs != SBF_OK) return bs;
     sbf_server_config c{};
     if (config) c = *config;
     if (c.staging_bytes == 0) c.staging_bytes = uint64_t{16} << 30;

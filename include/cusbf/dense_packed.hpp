@@ -1,7 +1,7 @@
-// dense_packed.hpp -- 2-bit dense packing (drop-in for the reference's
-// include/cusbf/dense_packed.hpp:20-74): 32 symbols per uint64_t word,
-// symbol t at bits [2(t%32), 2(t%32)+2) of word t/32, invalid bytes stored as
-// their low two code bits.
+// dense_packed.hpp -- dense packing (drop-in for the reference's
+// include/cusbf/dense_packed.hpp:20-74): 64 / symbolBits symbols per uint64_t
+// word (32 for DNA), symbol t at bits [b(t%per), b(t%per)+b) of word t/per,
+// invalid symbols stored as their low symbolBits bits.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -29,10 +29,12 @@ template <typename Config>
 
 template <typename Config>
 [[nodiscard]] std::vector<uint64_t> pack_dense_sequence(std::string_view sequence) {
-    static_assert(Config::symbolBits == 2 && Config::symbolWidth == 1,
-                  "the B200 engine packs the 2-bit DNA alphabet");
-    std::vector<uint64_t> words(dense_packed_word_count<Config>(sequence.size()), 0);
-    if (!sequence.empty()) sbf_pack_dense_host(sequence.data(), sequence.size(), words.data());
+    const uint64_t num_symbols = sequence.size() / Config::symbolWidth;
+    std::vector<uint64_t> words(dense_packed_word_count<Config>(num_symbols), 0);
+    if (num_symbols == 0) return words;
+    const int s = sbf_pack_dense_host_for(detail::alphabet_id<typename Config::Alphabet>(),
+                                          sequence.data(), num_symbols, words.data());
+    if (s != SBF_OK) throw std::runtime_error(detail::status_error(s).message());
     return words;
 }
 
@@ -40,8 +42,9 @@ template <typename Config>
 inline void pack_dense_sequence_device(const char* d_sequence, uint64_t num_symbols,
                                        uint64_t* d_words, cudaStream_t stream = {}) {
     if (num_symbols == 0) return;
-    const int s = sbf_pack_dense_device(d_sequence, num_symbols, d_words,
-                                        reinterpret_cast<sbf_stream_t>(stream));
+    const int s = sbf_pack_dense_device_for(detail::alphabet_id<typename Config::Alphabet>(),
+                                            d_sequence, num_symbols, d_words,
+                                            reinterpret_cast<sbf_stream_t>(stream));
     if (s != SBF_OK) throw std::runtime_error(detail::status_error(s).message());
 }
 

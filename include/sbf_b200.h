@@ -222,6 +222,14 @@ int sbf_pack_dense_device(const char* d_seq, uint64_t num_symbols, uint64_t* d_w
                           sbf_stream_t stream);
 /* pack_dense_sequence (dense_packed.hpp:36-50), on the host. */
 int sbf_pack_dense_host(const char* h_seq, uint64_t num_symbols, uint64_t* h_words);
+/* The same three for any alphabet (SBF_ALPHABET_*): 64 / bits symbols per
+ * word (32 DNA, 12 protein, 10 DNA triplets); num_symbols symbols of
+ * symbolWidth input bytes each (3 for DNA triplets). */
+uint64_t sbf_dense_packed_word_count_for(int alphabet, uint64_t num_symbols);
+int sbf_pack_dense_host_for(int alphabet, const char* h_seq, uint64_t num_symbols,
+                            uint64_t* h_words);
+int sbf_pack_dense_device_for(int alphabet, const char* d_seq, uint64_t num_symbols,
+                              uint64_t* d_words, sbf_stream_t stream);
 int sbf_insert_dense_packed_async(sbf_filter_t* filter, const uint64_t* d_words,
                                   uint64_t n_words, uint64_t num_symbols, sbf_stream_t stream,
                                   uint64_t* kmers_out);

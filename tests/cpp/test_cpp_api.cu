@@ -153,6 +153,25 @@ int main() {
         CHECK(f.num_shards() == (1u << 12) && f.filter_bits() == (1u << 20));
         CHECK(f.ref().num_blocks() == f.num_shards());
     }
+    {  // other alphabets and configurations run on the generic kernels
+        using P = cusbf::Config<5, 4, 3, 4, 256, cusbf::ProteinAlphabet>;
+        cusbf::filter<P> p(1 << 14);
+        const std::string prot = "MKTAYIAKQRQISFVKSHFSRQ";
+        CHECK(CUSBF_UNWRAP(p.insert_sequence(prot)) == prot.size() - 4);
+        const auto hits = CUSBF_UNWRAP(p.contains_sequence(prot + "*WWWWW"));
+        CHECK(hits.size() == prot.size() + 6 - 4);
+        for (size_t i = 0; i < hits.size(); ++i)
+            CHECK(hits[i] == (i < prot.size() - 4 ? 1 : i <= prot.size() ? 0 : hits[i]));
+        using T = cusbf::Config<3, 2, 2, 4, 256, cusbf::DnaTripletAlphabet>;
+        cusbf::filter<T> t(1 << 14);
+        CHECK(CUSBF_UNWRAP(t.insert_sequence(std::string("ACGTTGCAAGGC"))) == 2);
+        CHECK(all_ones(CUSBF_UNWRAP(t.contains_sequence(std::string("ACGTTGCAAGGC")))));
+        using D = cusbf::Config<25, 22, 13, 8>;
+        cusbf::filter<D> d(1 << 16);
+        const std::string dna(200, 'C');
+        CHECK(CUSBF_UNWRAP(d.insert_sequence(dna)) == 200 - 24);
+        CHECK(all_ones(CUSBF_UNWRAP(d.contains_sequence(dna))));
+    }
     std::printf("cpp api checks: %s\n", failures ? "FAILED" : "ok");
     return failures ? 1 : 0;
 }

@@ -263,8 +263,10 @@ def test_reference_known_answers(sbf, cuda):
 
 
 def test_errors(sbf, cuda):
+    # The reference's Config rules: a DNA k-mer fits 64 bits (k <= 32), and
+    # a 31-symbol protein k-mer (5 bits a symbol) does not.
     with pytest.raises(sbf.SbfError) as e:
-        sbf.Filter(1 << 10, k=17, s=9, m=5, hashes=4)
+        sbf.Filter(1 << 10, k=33, s=9, m=5, hashes=4)
     assert e.value.category == "invalid_argument"
     with pytest.raises(sbf.SbfError) as e:
         sbf.Filter(1 << 10, alphabet=2)
