@@ -880,7 +880,7 @@ def main() -> None:
     positives = int(d_out.sum(dtype=torch.int64).item())
 
     # End-to-end through the host API with pinned buffers.
-    e2e = e2e_bits = None
+    e2e = e2e_bits = e2e_dense = None
     if not args.no_e2e:
         h_genome = torch.from_numpy(joined).pin_memory()
         h_query = torch.empty(d_query.numel(), dtype=torch.uint8).pin_memory()
@@ -941,7 +941,47 @@ def main() -> None:
                     "d2h_bytes_per_step": int(4 * n_words), "ms_per_step": b_ms,
                     "api": "sbf_insert_sequence + sbf_contains_sequence_bits (host buffers, "
                            "pinned; one result bit per window)"}
-        del h_bits, bnp
+
+        # The same step with 2-bit dense-packed input (the reference's dense
+        # wire format, packed by the client before the step) and bit-packed
+        # results: a quarter byte in and an eighth of a byte out per window.
+        n_gs, n_qs = d_genome.numel(), d_query.numel()
+        d_gw = torch.empty(sbf.Filter.dense_packed_word_count(n_gs), dtype=torch.int64, device=dev)
+        d_qw = torch.empty(sbf.Filter.dense_packed_word_count(n_qs), dtype=torch.int64, device=dev)
+        sbf.pack_dense_sequence_device(d_genome, n_gs, d_gw, stream)
+        sbf.pack_dense_sequence_device(d_query, n_qs, d_qw, stream)
+        h_gw = torch.empty(d_gw.numel(), dtype=torch.int64).pin_memory()
+        h_qw = torch.empty(d_qw.numel(), dtype=torch.int64).pin_memory()
+        torch.cuda.synchronize(dev)
+        h_gw.copy_(d_gw)
+        h_qw.copy_(d_qw)
+        del d_gw, d_qw
+        gw_np, qw_np = h_gw.numpy().view(np.uint64), h_qw.numpy().view(np.uint64)
+        n_dense_windows = (n_gs - K + 1) + (n_qs - K + 1)
+
+        def e2e_dense_step():
+            f.clear(stream)
+            torch.cuda.synchronize(dev)
+            w0 = time.perf_counter()
+            f.insert_dense_packed(gw_np, n_gs, stream)
+            sbf._check(sbf._lib.sbf_contains_dense_packed_bits(
+                f.handle, qw_np.ctypes.data, qw_np.size, n_qs, bnp.ctypes.data, n_words,
+                stream.cuda_stream))
+            return (time.perf_counter() - w0) * 1e3
+
+        e2e_dense_step()
+        d_ms = float(np.mean([e2e_dense_step() for _ in range(max(1, args.e2e_steps))]))
+        (d_ms,) = max_over_ranks([d_ms], dist, dev)
+        e2e_dense = {"value": world * n_dense_windows / (d_ms / 1e3), "unit": "k-mers/s",
+                     "h2d_bytes_per_step": int(gw_np.nbytes + qw_np.nbytes),
+                     "d2h_bytes_per_step": int(4 * n_words), "ms_per_step": d_ms,
+                     "windows_per_step": int(n_dense_windows),
+                     "api": "sbf_insert_dense_packed + sbf_contains_dense_packed_bits (host "
+                            "buffers, pinned; 2-bit input, one result bit per window)",
+                     "note": "dense packing stores N as a base (the reference's "
+                             "pack_dense_sequence does the same), so every window is valid and "
+                             "hit counts differ from the byte path on windows with N"}
+        del h_bits, bnp, h_gw, h_qw, gw_np, qw_np
 
     if rank != 0:
         if dist:
@@ -1029,6 +1069,7 @@ def main() -> None:
         "cpu_baseline": cpu,
         "e2e": e2e,
         "e2e_bits": e2e_bits,
+        "e2e_dense": e2e_dense,
         "gpu_launches": 2 * args.steps,
         "clocks": clock_info,
     }

@@ -218,6 +218,8 @@ _sig("sbf_dense_packed_word_count", _u64, _u64)
 _sig("sbf_pack_dense_device", C.c_int, _vp, _u64, _vp, _vp)
 _sig("sbf_pack_dense_host", C.c_int, _vp, _u64, _vp)
 _sig("sbf_dense_packed_word_count_for", _u64, C.c_int, _u64)
+_sig("sbf_contains_dense_packed_bits_async", C.c_int, _vp, _vp, _u64, _u64, _vp, _u64, _vp)
+_sig("sbf_contains_dense_packed_bits", C.c_int, _vp, _vp, _u64, _u64, _vp, _u64, _vp)
 _sig("sbf_pack_dense_device_for", C.c_int, C.c_int, _vp, _u64, _vp, _vp)
 _sig("sbf_pack_dense_host_for", C.c_int, C.c_int, _vp, _u64, _vp)
 _sig("sbf_insert_dense_packed_async", C.c_int, _vp, _vp, _u64, _u64, _vp, C.POINTER(_u64))
@@ -230,6 +232,11 @@ _sig("sbf_normalized_batch_bytes", _u64, _vp, _u64)
 _sig("sbf_normalize_record_batch", C.c_int, _u32, _vp, _u64, _vp, _u64, _vp, _u64,
      C.POINTER(_u64), _vp)
 _sig("sbf_query_layout", C.c_int, _u32, _vp, _u64, _vp, C.POINTER(_u64))
+_sig("sbf_validate_record_batch_for", C.c_int, C.c_int, _u64, _vp, _u64)
+_sig("sbf_normalized_batch_bytes_for", _u64, C.c_int, _vp, _u64)
+_sig("sbf_normalize_record_batch_for", C.c_int, C.c_int, _u32, _vp, _u64, _vp, _u64, _vp, _u64,
+     C.POINTER(_u64), _vp)
+_sig("sbf_query_layout_for", C.c_int, C.c_int, _u32, _vp, _u64, _vp, C.POINTER(_u64))
 _sig("sbf_insert_record_batch", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, C.POINTER(InsertReport))
 _sig("sbf_insert_record_batch_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, C.POINTER(_u64))
 _sig("sbf_query_record_batch", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, C.POINTER(QueryReport),
@@ -339,17 +346,17 @@ def records_from_ranges(seq, ranges):
     return [b[int(o):int(o) + int(n)] for o, n in _ranges(ranges)]
 
 
-def validate_record_batch(nbytes: int, ranges) -> None:
+def validate_record_batch(nbytes: int, ranges, alphabet: int = ALPHABET_DNA) -> None:
     r = _ranges(ranges)
-    _check(_lib.sbf_validate_record_batch(nbytes, _np_ptr(r), r.shape[0]))
+    _check(_lib.sbf_validate_record_batch_for(alphabet, nbytes, _np_ptr(r), r.shape[0]))
 
 
-def normalized_batch_bytes(ranges) -> int:
+def normalized_batch_bytes(ranges, alphabet: int = ALPHABET_DNA) -> int:
     r = _ranges(ranges)
-    return _lib.sbf_normalized_batch_bytes(_np_ptr(r), r.shape[0])
+    return _lib.sbf_normalized_batch_bytes_for(alphabet, _np_ptr(r), r.shape[0])
 
 
-def normalize_record_batch(k: int, seq, ranges):
+def normalize_record_batch(k: int, seq, ranges, alphabet: int = ALPHABET_DNA):
     """normalize_record_batch (normalized_record_batch.hpp:289-316): the
     separator-joined sequence and one NormalizedRecord per record."""
     b = _host_bytes(seq)
@@ -357,21 +364,21 @@ def normalize_record_batch(k: int, seq, ranges):
     n = r.shape[0]
     total = _u64()
     recs = (NormalizedRecord * max(n, 1))()
-    _check(_lib.sbf_normalize_record_batch(k, _np_ptr(b), b.size, _np_ptr(r), n, None, 0,
-                                           C.byref(total), None))
+    _check(_lib.sbf_normalize_record_batch_for(alphabet, k, _np_ptr(b), b.size, _np_ptr(r), n,
+                                               None, 0, C.byref(total), None))
     out = np.zeros(max(total.value, 1), dtype=np.uint8)
-    _check(_lib.sbf_normalize_record_batch(k, _np_ptr(b), b.size, _np_ptr(r), n, _np_ptr(out),
-                                           out.size, C.byref(total), recs))
+    _check(_lib.sbf_normalize_record_batch_for(alphabet, k, _np_ptr(b), b.size, _np_ptr(r), n,
+                                               _np_ptr(out), out.size, C.byref(total), recs))
     return out[:total.value], list(recs)[:n]
 
 
-def query_layout(k: int, records):
+def query_layout(k: int, records, alphabet: int = ALPHABET_DNA):
     """QueryLayout::build (query_layout.cuh:42-72): (layout records, total hits)."""
     n = len(records)
     arr = (NormalizedRecord * max(n, 1))(*records)
     out = (QueryLayoutRecord * max(n, 1))()
     total = _u64()
-    _check(_lib.sbf_query_layout(k, arr, n, out, C.byref(total)))
+    _check(_lib.sbf_query_layout_for(alphabet, k, arr, n, out, C.byref(total)))
     return list(out)[:n], total.value
 
 
@@ -509,6 +516,26 @@ class Filter:
         o, on = _dev_ptr(d_out)
         _check(_lib.sbf_contains_dense_packed_async(self._h, p, nb // 8, num_symbols, o, on,
                                                     _stream(stream)))
+
+    def contains_dense_packed_bits_async(self, d_words, num_symbols: int, d_bits,
+                                         stream=None) -> None:
+        """Dense input, one result bit per window (bit i % 32 of word i / 32)."""
+        p, nb = _dev_ptr(d_words)
+        o, on = _dev_ptr(d_bits)
+        _check(_lib.sbf_contains_dense_packed_bits_async(self._h, p, nb // 8, num_symbols, o,
+                                                         on // 4, _stream(stream)))
+
+    def contains_dense_packed_bits(self, words, num_symbols: int, out=None, stream=None):
+        """Host dense words -> uint32 result words (one bit per window)."""
+        w = np.ascontiguousarray(words, dtype=np.uint64)
+        n = max(num_symbols - self.config.k + 1, 0)
+        nw = (n + 31) // 32
+        if out is None:
+            out = np.zeros(max(nw, 1), np.uint32)
+        o = out.numpy() if hasattr(out, "numpy") else out
+        _check(_lib.sbf_contains_dense_packed_bits(self._h, _np_ptr(w), w.size, num_symbols,
+                                                   _np_ptr(o), o.nbytes // 4, _stream(stream)))
+        return o[:nw]
 
     def contains_dense_packed(self, words, num_symbols: int, d_out=None, stream=None):
         w = np.ascontiguousarray(words, dtype=np.uint64)

@@ -216,9 +216,11 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
     uint64_t chunk_kmers;
     const uint64_t per_word = dense_per_word();
     if (dense) {
-        // About chunk_target packed bytes, a whole number of words.
+        // About chunk_target packed bytes, a whole number of words (and of
+        // 32-window result words in bit-packed mode).
+        const uint64_t unit = bits ? per_word * 32 : per_word;
         const uint64_t syms = chunk_target / 8 * per_word;
-        chunk_kmers = std::max<uint64_t>(syms / per_word * per_word, 1024 / per_word * per_word);
+        chunk_kmers = std::max<uint64_t>(syms / unit * unit, unit);
     } else {
         const uint64_t t = chunk_target / width;
         chunk_kmers = bits ? std::max<uint64_t>(t / 32 * 32, 1024) : t;
@@ -576,6 +578,15 @@ extern "C" int sbf_contains_sequence_bits(const sbf_filter_t* f, const char* h_s
 
 // ---- dense input --------------------------------------------------------------
 
+extern "C" int sbf_contains_dense_packed_bits_async(const sbf_filter_t* f, const uint64_t* d_words,
+                                                    uint64_t n_words, uint64_t num_symbols,
+                                                    uint32_t* d_bits, uint64_t n_bit_words,
+                                                    sbf_stream_t stream);
+extern "C" int sbf_contains_dense_packed_bits(const sbf_filter_t* f, const uint64_t* h_words,
+                                              uint64_t n_words, uint64_t num_symbols,
+                                              uint32_t* h_bits, uint64_t n_bit_words,
+                                              sbf_stream_t stream);
+
 extern "C" uint64_t sbf_dense_packed_word_count(uint64_t num_symbols) {
     return (num_symbols + 31) / 32;
 }
@@ -676,4 +687,37 @@ extern "C" int sbf_contains_dense_packed(const sbf_filter_t* f, const uint64_t* 
     return const_cast<sbf_filter*>(f)->host_pipeline(true, true, h_words,
                                                      f->dense_words(num_symbols) * 8, n, h_out,
                                                      nullptr, S(stream));
+}
+
+// ---- dense input, bit-packed results (no reference counterpart) ----------------
+
+extern "C" int sbf_contains_dense_packed_bits_async(const sbf_filter_t* f, const uint64_t* d_words,
+                                                    uint64_t n_words, uint64_t num_symbols,
+                                                    uint32_t* d_bits, uint64_t n_bit_words,
+                                                    sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    const uint64_t n = f->kmers_of(num_symbols);
+    if (n == 0) return SBF_OK;
+    SBF_TRY(check_dense(f, d_words, n_words, num_symbols));
+    if (!d_bits || (reinterpret_cast<uintptr_t>(d_bits) & 3u))
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "bit output must be a 4-byte aligned pointer");
+    if (n_bit_words < (n + 31) / 32)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "bit output span is too small");
+    return f->launch(true, true, d_words, f->dense_words(num_symbols) * 8, n, nullptr, S(stream),
+                     d_bits);
+}
+
+extern "C" int sbf_contains_dense_packed_bits(const sbf_filter_t* f, const uint64_t* h_words,
+                                              uint64_t n_words, uint64_t num_symbols,
+                                              uint32_t* h_bits, uint64_t n_bit_words,
+                                              sbf_stream_t stream) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    const uint64_t n = f->kmers_of(num_symbols);
+    if (n == 0) return SBF_OK;
+    SBF_TRY(check_dense(f, h_words, n_words, num_symbols));
+    if (!h_bits || n_bit_words < (n + 31) / 32)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "bit output span is too small");
+    return const_cast<sbf_filter*>(f)->host_pipeline(true, true, h_words,
+                                                     f->dense_words(num_symbols) * 8, n, nullptr,
+                                                     nullptr, S(stream), h_bits);
 }

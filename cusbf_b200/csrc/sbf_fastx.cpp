@@ -226,12 +226,13 @@ size_t host_chunk_limit() {
 
 // Whether the chunk's estimated staging reaches the budget
 // (fastx_chunk_reached_staging_budget, detail/fastx_chunk.cuh:110-127).
-bool should_flush(bool query, size_t budget, uint64_t raw, uint64_t records, uint32_t k) {
+bool should_flush(bool query, size_t budget, uint64_t raw, uint64_t records, uint32_t k,
+                  uint32_t width) {
     if (raw == 0) return false;
     if (budget == 0) return true;
-    const uint64_t norm = raw + records * 2;
+    const uint64_t norm = raw + records * 2 * width;
     uint64_t staging = norm;
-    if (query) staging += norm < k ? 0 : norm - k + 1;
+    if (query) staging += norm / width < k ? 0 : norm / width - k + 1;
     return staging >= budget || raw >= host_chunk_limit();
 }
 
@@ -287,9 +288,9 @@ int run_fastx_host(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, con
         if (query) {
             sbf_query_report r{};
             QueryCtx ctx{&chunk, consume, cuser};
-            const int s = sbf_query_record_batch(f, chunk.seq.data(), chunk.seq.size(),
-                                                 chunk.ranges.data(), chunk.ranges.size(), stream,
-                                                 &r, consume ? chunk_record_cb : nullptr, &ctx);
+            const int s = query_record_batch_impl(f, chunk.seq.data(), chunk.seq.size(),
+                                                  chunk.ranges.data(), chunk.ranges.size(), stream,
+                                                  &r, consume ? chunk_record_cb : nullptr, &ctx);
             if (s != SBF_OK) return s;
             qt.records_queried += r.records_queried;
             qt.queried_bases += r.queried_bases;
@@ -297,9 +298,9 @@ int run_fastx_host(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, con
             qt.positive_kmers += r.positive_kmers;
         } else {
             sbf_insert_report r{};
-            const int s = sbf_insert_record_batch(f, chunk.seq.data(), chunk.seq.size(),
-                                                  chunk.ranges.data(), chunk.ranges.size(),
-                                                  stream, &r);
+            const int s = insert_record_batch_impl(f, chunk.seq.data(), chunk.seq.size(),
+                                                   chunk.ranges.data(), chunk.ranges.size(),
+                                                   stream, &r);
             if (s != SBF_OK) return s;
             it.records_indexed += r.records_indexed;
             it.indexed_bases += r.indexed_bases;
@@ -317,7 +318,7 @@ int run_fastx_host(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, con
         chunk.seq += seq;
         if (query && consume) chunk.headers.push_back(header);
         ++next_index;
-        if (should_flush(query, budget, chunk.seq.size(), chunk.ranges.size(), f->k)) {
+        if (should_flush(query, budget, chunk.seq.size(), chunk.ranges.size(), f->k, f->width)) {
             const int s = flush();
             if (s != SBF_OK) return s;
         }
@@ -366,7 +367,6 @@ int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const ch
               sbf_query_report* qrep, sbf_fastx_record_cb consume, void* cuser) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
     if (!read) return set_error(SBF_ERR_INVALID_ARGUMENT, "read callback is null");
-    if (const int bs = f->require_byte_symbols("FASTA/FASTQ input"); bs != SBF_OK) return bs;
     sbf_insert_report it{0, 0, 0};
     sbf_query_report qt{0, 0, 0, 0};
     auto finish = [&](int s) -> int {
@@ -375,7 +375,10 @@ int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const ch
         if (qrep) *qrep = qt;
         return SBF_OK;
     };
-    if (!device_fastq_enabled())
+    // The GPU parsers feed a ragged pass over the raw text, whose symbol grid
+    // is the buffer's: multi-byte symbols (DNA triplets) need each record
+    // padded to a symbol boundary, which the host path's normalisation does.
+    if (!device_fastq_enabled() || f->width != 1)
         return finish(run_fastx_host(f, query, read, ruser, source, fill_fraction, stream, it, qt,
                                      consume, cuser, 0, 0));
     if (!f->fastq) f->fastq = new FastqDevice();

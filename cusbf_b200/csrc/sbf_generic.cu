@@ -121,13 +121,14 @@ __global__ void __launch_bounds__(kThreads) generic_kernel(TileParams p) {
             if (!kDense && e == kInvalid) last_inv = static_cast<int64_t>(t);
             km = ((km << c.bits) | (e & sym_mask)) & km_mask;
         }
-        // Ragged: the record holding the current window's first byte.
+        // Ragged: the record holding the current window's first byte
+        // (window w covers bytes [w * width, (w + k) * width)).
         uint64_t r = 0;
         if constexpr (kRagged) {
             uint64_t lo = 0, hi = p.n_ranges;
             while (lo < hi) {
                 const uint64_t mid = (lo + hi) >> 1;
-                if (p.ranges[mid].offset + p.ranges[mid].bytes > w0)
+                if (p.ranges[mid].offset + p.ranges[mid].bytes > w0 * c.width)
                     hi = mid;
                 else
                     lo = mid + 1;
@@ -164,9 +165,10 @@ __global__ void __launch_bounds__(kThreads) generic_kernel(TileParams p) {
             km = ((km << c.bits) | (e & sym_mask)) & km_mask;
             bool valid = last_inv < static_cast<int64_t>(w);
             if constexpr (kRagged) {
-                while (r < p.n_ranges && p.ranges[r].offset + p.ranges[r].bytes <= w) ++r;
-                valid = valid && r < p.n_ranges && p.ranges[r].offset <= w &&
-                        w + c.k <= p.ranges[r].offset + p.ranges[r].bytes;
+                const uint64_t b0 = w * c.width;
+                while (r < p.n_ranges && p.ranges[r].offset + p.ranges[r].bytes <= b0) ++r;
+                valid = valid && r < p.n_ranges && p.ranges[r].offset <= b0 &&
+                        (w + c.k) * c.width <= p.ranges[r].offset + p.ranges[r].bytes;
             }
             bool hit = false;
             if (valid) {

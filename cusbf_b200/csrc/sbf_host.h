@@ -13,6 +13,9 @@
 namespace sbf {
 
 int set_error(int status, const char* fmt, ...);
+// Bits per packed symbol and input bytes per symbol of an alphabet
+// (SBF_ALPHABET_*); false for an unknown alphabet (sbf_generic.cu).
+bool alphabet_geometry(int alphabet, uint32_t* bits, uint32_t* width);
 void set_error_location(const char* file, uint32_t line, uint32_t col);
 int cuda_fail(cudaError_t e, const char* what);
 bool is_pinned(const void* p);
@@ -94,8 +97,8 @@ struct sbf_filter {
     uint64_t dense_words(uint64_t symbols) const {
         return (symbols + dense_per_word() - 1) / dense_per_word();
     }
-    // Record-level paths (ragged batches, record batches, FASTX, the server)
-    // work on one-byte symbols only; SBF_OK or an invalid-argument error.
+    // The ragged host pipeline and the server work on one-byte symbols only;
+    // SBF_OK or an invalid-argument error.
     int require_byte_symbols(const char* what) const;
     int stage_record_batch(const char* h_seq, uint64_t len, const sbf_record_range* r, uint64_t n,
                            cudaStream_t st, std::vector<uint64_t>& out_off, uint64_t& norm_len);
@@ -113,4 +116,13 @@ struct sbf_filter {
 namespace sbf {
 void ragged_release(sbf_filter* f);
 void fastq_device_release(sbf_filter* f);
+// Host record batches without the symbol-alignment check of the public entry
+// points (FASTX chunks hold records of any length; normalisation pads each
+// to a symbol boundary).
+int insert_record_batch_impl(sbf_filter* f, const char* h_seq, uint64_t len,
+                             const sbf_record_range* ranges, uint64_t n, sbf_stream_t stream,
+                             sbf_insert_report* report);
+int query_record_batch_impl(sbf_filter* f, const char* h_seq, uint64_t len,
+                            const sbf_record_range* ranges, uint64_t n, sbf_stream_t stream,
+                            sbf_query_report* report, sbf_record_query_cb consume, void* user);
 }  // namespace sbf

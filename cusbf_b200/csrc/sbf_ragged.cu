@@ -173,7 +173,7 @@ TileParams ragged_params(const sbf_filter* f, bool query, const uint8_t* d_seq,
     TileParams p{};
     p.input = d_seq;
     p.input_bytes = len;
-    p.n_kmers = f->kmers_of(len);
+    p.n_kmers = f->kmers_of_bytes(len);
     int64_t phase = 0;
     if (query && out_bits)
         phase = 0;  // strips start at multiples of 32 windows
@@ -490,7 +490,6 @@ static int ragged_async(sbf_filter_t* f, bool query, const char* d_seq, uint64_t
                         uint64_t out_len, uint64_t* d_counts, sbf_stream_t stream,
                         uint64_t* d_rec_valid = nullptr, uint64_t* d_rec_pos = nullptr) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    SBF_TRY(f->require_byte_symbols("ragged batches"));
     if (n && !d_ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "ranges pointer is null");
     if (n > 0xFFFFFFFFull) return set_error(SBF_ERR_INVALID_ARGUMENT, "too many records");
     const bool tally = d_rec_valid != nullptr;
@@ -501,7 +500,7 @@ static int ragged_async(sbf_filter_t* f, bool query, const char* d_seq, uint64_t
         SBF_CUDA(cudaMemsetAsync(d_rec_valid, 0, n * sizeof(uint64_t), st));
         SBF_CUDA(cudaMemsetAsync(d_rec_pos, 0, n * sizeof(uint64_t), st));
     }
-    const uint64_t W = f->kmers_of(len);
+    const uint64_t W = f->kmers_of_bytes(len);
     if (W == 0) return SBF_OK;
     if (!d_seq) return set_error(SBF_ERR_INVALID_ARGUMENT, "sequence pointer is null");
     // With per-record counts the hit bytes are optional.
@@ -563,7 +562,7 @@ extern "C" int sbf_ragged_insert(sbf_filter_t* f, const char* h_seq, uint64_t le
                                  const sbf_ragged_tuning* tuning, sbf_stream_t stream,
                                  sbf_insert_report* report) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    SBF_TRY(f->require_byte_symbols("ragged batches"));
+    SBF_TRY(f->require_byte_symbols("the ragged host pipeline"));
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     SBF_TRY(validate_ranges(len, ranges, n));
     sbf_ragged_tuning t{};
@@ -585,7 +584,7 @@ extern "C" int sbf_ragged_query(const sbf_filter_t* cf, const char* h_seq, uint6
                                 sbf_stream_t stream, sbf_query_report* report) {
     auto* f = const_cast<sbf_filter*>(cf);
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    SBF_TRY(f->require_byte_symbols("ragged batches"));
+    SBF_TRY(f->require_byte_symbols("the ragged host pipeline"));
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     SBF_TRY(validate_ranges(len, ranges, n));
     const uint64_t W = f->kmers_of(len);
@@ -622,7 +621,7 @@ extern "C" int sbf_ragged_autotune(sbf_filter_t* f, int query, const char* h_seq
                                    uint64_t sample_bytes, sbf_stream_t stream,
                                    sbf_ragged_tuning* chosen) {
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    SBF_TRY(f->require_byte_symbols("ragged batches"));
+    SBF_TRY(f->require_byte_symbols("the ragged host pipeline"));
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     SBF_TRY(validate_ranges(len, ranges, n));
     if (sample_bytes == 0) sample_bytes = uint64_t{256} << 20;

@@ -29,7 +29,21 @@ using namespace sbf;
 
 namespace sbf {
 
-constexpr uint8_t kSeparator = 'N';
+// Separator byte between normalised records (Alphabet::separator: '*' for
+// proteins, 'N' for DNA and DNA triplets).
+uint8_t separator_of(int alphabet) { return alphabet == SBF_ALPHABET_PROTEIN ? '*' : 'N'; }
+
+// Whether the symbol at p encodes as valid (Alphabet::encode != invalidSymbol).
+bool symbol_valid(int alphabet, const char* p) {
+    auto dna = [](char c) {
+        const uint8_t u = static_cast<uint8_t>(c) & 0xDFu;
+        return u == 'A' || u == 'C' || u == 'G' || u == 'T';
+    };
+    if (alphabet == SBF_ALPHABET_PROTEIN)
+        return static_cast<uint8_t>((static_cast<uint8_t>(p[0]) & 0xDFu) - 'A') < 26;
+    if (alphabet == SBF_ALPHABET_DNA_TRIPLET) return dna(p[0]) && dna(p[1]) && dna(p[2]);
+    return dna(p[0]);
+}
 
 // ---------------------------------------------------------------------------
 // Host layout
@@ -49,13 +63,27 @@ int validate_ranges(uint64_t len, const sbf_record_range* r, uint64_t n) {
     return SBF_OK;
 }
 
-// Normalised offsets: out_off[i] = (bytes of records before i) + (separators
-// before i); a separator precedes record i exactly when some earlier record
-// is non-empty.  Returns the normalised length.
-uint64_t normalized_offsets(const sbf_record_range* r, uint64_t n, uint64_t* out_off) {
+// Record batches of multi-byte symbols must start and end on symbol
+// boundaries (filter.cuh:865-873, normalized_record_batch.hpp:137-145).
+int validate_alignment(uint32_t width, const sbf_record_range* r, uint64_t n) {
+    if (width <= 1) return SBF_OK;
+    for (uint64_t i = 0; i < n; ++i)
+        if (r[i].sequence_offset % width != 0 || r[i].sequence_bytes % width != 0)
+            return set_error(SBF_ERR_INVALID_ARGUMENT,
+                             "record batch ranges must align to the configured alphabet symbol "
+                             "width");
+    return SBF_OK;
+}
+
+// Normalised offsets (write_record_boundary, normalized_record_batch.hpp:
+// 209-232): before every record that follows non-empty content, the length
+// is padded to a symbol boundary and one separator symbol (`width` bytes) is
+// added.  Returns the normalised length.
+uint64_t normalized_offsets(const sbf_record_range* r, uint64_t n, uint64_t* out_off,
+                            uint32_t width) {
     uint64_t pos = 0;
     for (uint64_t i = 0; i < n; ++i) {
-        if (pos != 0) pos += 1;
+        if (pos != 0) pos += (width - pos % width) % width + width;
         out_off[i] = pos;
         pos += r[i].sequence_bytes;
     }
@@ -76,12 +104,13 @@ constexpr uint64_t kGatherSegment = 1u << 16;
 
 __global__ void normalize_gather_kernel(const uint8_t* dense, uint64_t dense_base,
                                         const sbf_record_range* ranges, const uint64_t* out_off,
-                                        uint64_t n, uint8_t* out, uint64_t norm_len) {
+                                        uint64_t n, uint8_t* out, uint64_t norm_len,
+                                        uint8_t separator) {
     __shared__ uint64_t first;
     for (uint64_t seg = blockIdx.x; seg * kGatherSegment < norm_len; seg += gridDim.x) {
         const uint64_t s0 = seg * kGatherSegment;
         const uint64_t s1 = s0 + kGatherSegment < norm_len ? s0 + kGatherSegment : norm_len;
-        for (uint64_t x = s0 + threadIdx.x; x < s1; x += blockDim.x) out[x] = kSeparator;
+        for (uint64_t x = s0 + threadIdx.x; x < s1; x += blockDim.x) out[x] = separator;
         if (threadIdx.x == 0) {
             // First record whose normalised end is past the segment start.
             uint64_t lo = 0, hi = n;
@@ -156,7 +185,7 @@ int sbf_filter::stage_record_batch(const char* h_seq, uint64_t len, const sbf_re
                                    uint64_t& norm_len) {
     SBF_TRY(validate_ranges(len, r, n));
     out_off.resize(n);
-    norm_len = normalized_offsets(r, n, out_off.data());
+    norm_len = normalized_offsets(r, n, out_off.data(), width);
     if (n == 0 || norm_len == 0) return SBF_OK;
     // The dense span covering every record.
     uint64_t lo = r[0].sequence_offset, hi = 0;
@@ -180,7 +209,7 @@ int sbf_filter::stage_record_batch(const char* h_seq, uint64_t len, const sbf_re
     const uint64_t ctas = std::min<uint64_t>(segs, static_cast<uint64_t>(sms) * 8);
     normalize_gather_kernel<<<static_cast<unsigned>(ctas), 256, 0, st>>>(
         static_cast<const uint8_t*>(rb_dense.ptr), lo, d_ranges, d_off, n,
-        static_cast<uint8_t*>(rb_norm.ptr), norm_len);
+        static_cast<uint8_t*>(rb_norm.ptr), norm_len, separator_of(alphabet));
     SBF_CUDA(cudaGetLastError());
     // The host layout vector must stay alive until the copies complete.
     SBF_CUDA(cudaStreamSynchronize(st));
@@ -197,7 +226,7 @@ int sbf_filter::record_pass(bool query, uint64_t n, uint64_t norm_len, uint8_t* 
     valid.assign(n, 0);
     positive.assign(n, 0);
     *total_valid = 0;
-    const uint64_t windows = kmers_of(norm_len);
+    const uint64_t windows = kmers_of_bytes(norm_len);
     if (n == 0 || windows == 0) return SBF_OK;
     SBF_TRY(rb_stats.ensure((2 * n + 2) * sizeof(uint64_t) + 64));
     auto* d_counts = static_cast<uint64_t*>(rb_stats.ptr);
@@ -234,47 +263,73 @@ extern "C" int sbf_validate_record_batch(uint64_t len, const sbf_record_range* r
     return validate_ranges(len, ranges, n);
 }
 
-extern "C" uint64_t sbf_normalized_batch_bytes(const sbf_record_range* ranges, uint64_t n) {
+extern "C" int sbf_validate_record_batch_for(int alphabet, uint64_t len,
+                                             const sbf_record_range* ranges, uint64_t n) {
+    uint32_t bits = 0, width = 0;
+    if (!alphabet_geometry(alphabet, &bits, &width))
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "unknown alphabet %d", alphabet);
+    if (n && !ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "ranges pointer is null");
+    SBF_TRY(validate_ranges(len, ranges, n));
+    return validate_alignment(width, ranges, n);
+}
+
+// estimate_normalized_batch_bytes (normalized_record_batch.hpp:185-200).
+extern "C" uint64_t sbf_normalized_batch_bytes_for(int alphabet, const sbf_record_range* ranges,
+                                                   uint64_t n) {
+    uint32_t bits = 0, width = 0;
+    if (!alphabet_geometry(alphabet, &bits, &width)) return 0;
     uint64_t size = 0;
     for (uint64_t i = 0; i < n; ++i) {
-        if (i != 0 || size != 0) size += 1;
+        if (i != 0 || size != 0) size += (width - size % width) % width + width;
         size += ranges[i].sequence_bytes;
     }
     return size;
 }
 
-extern "C" int sbf_normalize_record_batch(uint32_t k, const char* h_seq, uint64_t len,
-                                          const sbf_record_range* ranges, uint64_t n, char* out,
-                                          uint64_t out_cap, uint64_t* out_len,
-                                          sbf_normalized_record* records_out) {
+extern "C" uint64_t sbf_normalized_batch_bytes(const sbf_record_range* ranges, uint64_t n) {
+    return sbf_normalized_batch_bytes_for(SBF_ALPHABET_DNA, ranges, n);
+}
+
+// normalize_record_batch (normalized_record_batch.hpp:235-276) for any
+// alphabet: records at their normalised offsets, separator symbols between
+// them, and each record's valid windows (valid_record_kmer_count, :88-110).
+extern "C" int sbf_normalize_record_batch_for(int alphabet, uint32_t k, const char* h_seq,
+                                              uint64_t len, const sbf_record_range* ranges,
+                                              uint64_t n, char* out, uint64_t out_cap,
+                                              uint64_t* out_len,
+                                              sbf_normalized_record* records_out) {
+    uint32_t bits = 0, width = 0;
+    if (!alphabet_geometry(alphabet, &bits, &width))
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "unknown alphabet %d", alphabet);
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     SBF_TRY(validate_ranges(len, ranges, n));
+    SBF_TRY(validate_alignment(width, ranges, n));
     std::vector<uint64_t> off(n);
-    const uint64_t total = normalized_offsets(ranges, n, off.data());
+    const uint64_t total = normalized_offsets(ranges, n, off.data(), width);
     if (out_len) *out_len = total;
     if (out && out_cap < total)
         return set_error(SBF_ERR_INVALID_ARGUMENT, "normalised output buffer is too small");
+    const char sep = static_cast<char>(separator_of(alphabet));
+    uint64_t written = 0;
     for (uint64_t i = 0; i < n; ++i) {
         const char* src = h_seq + ranges[i].sequence_offset;
         const uint64_t size = ranges[i].sequence_bytes;
         if (out) {
-            if (off[i] != 0) out[off[i] - 1] = static_cast<char>(kSeparator);
+            std::memset(out + written, sep, off[i] - written);
             std::memcpy(out + off[i], src, size);
+            written = off[i] + size;
         }
         if (records_out) {
-            // valid_record_kmer_count (normalized_record_batch.hpp:88-110).
+            const uint64_t syms = size / width;
             uint64_t valid = 0;
-            if (size >= k) {
+            if (syms >= k) {
                 uint64_t invalid = 0;
-                auto bad = [&](uint64_t p) {
-                    const uint8_t u = static_cast<uint8_t>(src[p]) & 0xDFu;
-                    return !(u == 'A' || u == 'C' || u == 'G' || u == 'T');
-                };
-                for (uint64_t p = 0; p < k; ++p) invalid += bad(p);
+                auto bad = [&](uint64_t t) { return !symbol_valid(alphabet, src + t * width); };
+                for (uint64_t t = 0; t < k; ++t) invalid += bad(t);
                 valid = invalid == 0;
-                for (uint64_t s = 1; s + k <= size; ++s) {
-                    invalid -= bad(s - 1);
-                    invalid += bad(s + k - 1);
+                for (uint64_t t = 1; t + k <= syms; ++t) {
+                    invalid -= bad(t - 1);
+                    invalid += bad(t + k - 1);
                     valid += invalid == 0;
                 }
             }
@@ -284,20 +339,39 @@ extern "C" int sbf_normalize_record_batch(uint32_t k, const char* h_seq, uint64_
     return SBF_OK;
 }
 
-extern "C" int sbf_query_layout(uint32_t k, const sbf_normalized_record* records, uint64_t n,
-                                sbf_query_layout_record* out, uint64_t* total_hits) {
+extern "C" int sbf_normalize_record_batch(uint32_t k, const char* h_seq, uint64_t len,
+                                          const sbf_record_range* ranges, uint64_t n, char* out,
+                                          uint64_t out_cap, uint64_t* out_len,
+                                          sbf_normalized_record* records_out) {
+    return sbf_normalize_record_batch_for(SBF_ALPHABET_DNA, k, h_seq, len, ranges, n, out, out_cap,
+                                          out_len, records_out);
+}
+
+// QueryLayout::build (detail/query_layout.cuh:42-72): hit offsets are
+// normalised symbol positions.
+extern "C" int sbf_query_layout_for(int alphabet, uint32_t k,
+                                    const sbf_normalized_record* records, uint64_t n,
+                                    sbf_query_layout_record* out, uint64_t* total_hits) {
+    uint32_t bits = 0, width = 0;
+    if (!alphabet_geometry(alphabet, &bits, &width))
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "unknown alphabet %d", alphabet);
     if (n && (!records || !out)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    auto kmers = [&](uint64_t bytes) { return bytes / width < k ? 0 : bytes / width - k + 1; };
     uint64_t logical = 0;
     for (uint64_t i = 0; i < n; ++i) {
-        if (logical != 0) logical += 1;
+        if (logical != 0) logical += (width - logical % width) % width + width;
         const uint64_t size = records[i].size;
         out[i] = sbf_query_layout_record{records[i].record_index, records[i].input_offset, size,
-                                         records[i].valid_kmers, logical,
-                                         size < k ? 0 : size - k + 1};
+                                         records[i].valid_kmers, logical / width, kmers(size)};
         logical += size;
     }
-    if (total_hits) *total_hits = logical < k ? 0 : logical - k + 1;
+    if (total_hits) *total_hits = kmers(logical);
     return SBF_OK;
+}
+
+extern "C" int sbf_query_layout(uint32_t k, const sbf_normalized_record* records, uint64_t n,
+                                sbf_query_layout_record* out, uint64_t* total_hits) {
+    return sbf_query_layout_for(SBF_ALPHABET_DNA, k, records, n, out, total_hits);
 }
 
 // ---------------------------------------------------------------------------
@@ -311,6 +385,7 @@ extern "C" int sbf_insert_record_batch_async(sbf_filter_t* f, const char* d_seq,
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
     if (n && !ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "ranges pointer is null");
     SBF_TRY(validate_ranges(len, ranges, n));
+    SBF_TRY(validate_alignment(f->width, ranges, n));
     uint64_t total = 0;
     for (uint64_t i = 0; i < n; ++i) total += f->kmers_of_bytes(ranges[i].sequence_bytes);
     if (kmers_out) *kmers_out = total;
@@ -325,6 +400,7 @@ extern "C" int sbf_contains_record_batch_async(const sbf_filter_t* f, const char
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
     if (n && !ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "ranges pointer is null");
     SBF_TRY(validate_ranges(len, ranges, n));
+    SBF_TRY(validate_alignment(f->width, ranges, n));
     const uint64_t total = f->kmers_of_bytes(len);
     if (total == 0) return SBF_OK;
     if (!d_out || out_len < total)
@@ -336,11 +412,9 @@ extern "C" int sbf_contains_record_batch_async(const sbf_filter_t* f, const char
 // C ABI: host record batches
 // ---------------------------------------------------------------------------
 
-extern "C" int sbf_insert_record_batch(sbf_filter_t* f, const char* h_seq, uint64_t len,
-                                       const sbf_record_range* ranges, uint64_t n,
-                                       sbf_stream_t stream, sbf_insert_report* report) {
-    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    SBF_TRY(f->require_byte_symbols("host record batches"));
+int sbf::insert_record_batch_impl(sbf_filter* f, const char* h_seq, uint64_t len,
+                                  const sbf_record_range* ranges, uint64_t n, sbf_stream_t stream,
+                                  sbf_insert_report* report) {
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     cudaStream_t st = S(stream);
     std::vector<uint64_t> off;
@@ -348,7 +422,7 @@ extern "C" int sbf_insert_record_batch(sbf_filter_t* f, const char* h_seq, uint6
     SBF_TRY(f->stage_record_batch(h_seq, len, ranges, n, st, off, norm_len));
     sbf_insert_report rep{n, 0, 0};
     for (uint64_t i = 0; i < n; ++i) rep.indexed_bases += ranges[i].sequence_bytes;
-    if (f->kmers_of(norm_len)) {
+    if (f->kmers_of_bytes(norm_len)) {
         std::vector<uint64_t> valid, pos;
         SBF_TRY(f->record_pass(false, n, norm_len, nullptr, st, valid, pos, &rep.inserted_kmers));
         SBF_TRY(f->check_device_error(st));
@@ -357,13 +431,10 @@ extern "C" int sbf_insert_record_batch(sbf_filter_t* f, const char* h_seq, uint6
     return SBF_OK;
 }
 
-extern "C" int sbf_query_record_batch(const sbf_filter_t* cf, const char* h_seq, uint64_t len,
-                                      const sbf_record_range* ranges, uint64_t n,
-                                      sbf_stream_t stream, sbf_query_report* report,
-                                      sbf_record_query_cb consume, void* user) {
-    auto* f = const_cast<sbf_filter*>(cf);
-    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
-    SBF_TRY(f->require_byte_symbols("host record batches"));
+int sbf::query_record_batch_impl(sbf_filter* f, const char* h_seq, uint64_t len,
+                                 const sbf_record_range* ranges, uint64_t n, sbf_stream_t stream,
+                                 sbf_query_report* report, sbf_record_query_cb consume,
+                                 void* user) {
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     cudaStream_t st = S(stream);
     std::vector<uint64_t> off;
@@ -371,7 +442,7 @@ extern "C" int sbf_query_record_batch(const sbf_filter_t* cf, const char* h_seq,
     SBF_TRY(f->stage_record_batch(h_seq, len, ranges, n, st, off, norm_len));
     sbf_query_report rep{n, 0, 0, 0};
     for (uint64_t i = 0; i < n; ++i) rep.queried_bases += ranges[i].sequence_bytes;
-    const uint64_t windows = f->kmers_of(norm_len);
+    const uint64_t windows = f->kmers_of_bytes(norm_len);
     std::vector<uint64_t> valid(n, 0), pos(n, 0);
     std::vector<uint8_t> hits;
     if (windows) {
@@ -397,14 +468,14 @@ extern "C" int sbf_query_record_batch(const sbf_filter_t* cf, const char* h_seq,
     if (consume) {
         for (uint64_t i = 0; i < n; ++i) {
             const uint64_t size = ranges[i].sequence_bytes;
-            const uint64_t hc = f->kmers_of(size);
+            const uint64_t hc = f->kmers_of_bytes(size);
             sbf_record_view v{i,
                               h_seq + ranges[i].sequence_offset,
                               size,
                               size,
                               valid[i],
                               pos[i],
-                              hc ? hits.data() + off[i] : nullptr,
+                              hc ? hits.data() + off[i] / f->width : nullptr,
                               hc};
             if (consume(user, &v) != 0)
                 return set_error(SBF_ERR_ABORTED, "record consumer aborted the query");
@@ -412,4 +483,24 @@ extern "C" int sbf_query_record_batch(const sbf_filter_t* cf, const char* h_seq,
     }
     if (report) *report = rep;
     return SBF_OK;
+}
+
+extern "C" int sbf_insert_record_batch(sbf_filter_t* f, const char* h_seq, uint64_t len,
+                                       const sbf_record_range* ranges, uint64_t n,
+                                       sbf_stream_t stream, sbf_insert_report* report) {
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (n && !ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    SBF_TRY(validate_alignment(f->width, ranges, n));
+    return insert_record_batch_impl(f, h_seq, len, ranges, n, stream, report);
+}
+
+extern "C" int sbf_query_record_batch(const sbf_filter_t* cf, const char* h_seq, uint64_t len,
+                                      const sbf_record_range* ranges, uint64_t n,
+                                      sbf_stream_t stream, sbf_query_report* report,
+                                      sbf_record_query_cb consume, void* user) {
+    auto* f = const_cast<sbf_filter*>(cf);
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    if (n && !ranges) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    SBF_TRY(validate_alignment(f->width, ranges, n));
+    return query_record_batch_impl(f, h_seq, len, ranges, n, stream, report, consume, user);
 }

@@ -35,11 +35,11 @@ class QueryLayout {
     [[nodiscard]] static QueryLayout build(std::span<const NormalizedRecord> records) {
         QueryLayout layout;
         layout.records_.resize(records.size());
-        sbf_query_layout(Config::k,
-                         reinterpret_cast<const sbf_normalized_record*>(records.data()),
-                         records.size(),
-                         reinterpret_cast<sbf_query_layout_record*>(layout.records_.data()),
-                         &layout.total_hit_count_);
+        sbf_query_layout_for(detail::alphabet_id<typename Config::Alphabet>(), Config::k,
+                             reinterpret_cast<const sbf_normalized_record*>(records.data()),
+                             records.size(),
+                             reinterpret_cast<sbf_query_layout_record*>(layout.records_.data()),
+                             &layout.total_hit_count_);
         return layout;
     }
 

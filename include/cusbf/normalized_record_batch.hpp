@@ -25,18 +25,20 @@ template <typename Config>
 [[nodiscard]] Result<void> normalize_record_batch_into(RecordBatchView batch,
                                                        std::string& sequence_out,
                                                        std::vector<NormalizedRecord>& records_out) {
-    static_assert(Config::symbolWidth == 1, "the B200 engine implements one-byte symbols");
+    constexpr int alphabet = detail::alphabet_id<typename Config::Alphabet>();
     const auto* r = reinterpret_cast<const sbf_record_range*>(batch.records.data());
     const uint64_t n = batch.records.size();
     uint64_t total = 0;
-    int s = sbf_normalize_record_batch(Config::k, batch.sequence.data(), batch.sequence.size(), r,
-                                       n, nullptr, 0, &total, nullptr);
+    int s = sbf_normalize_record_batch_for(alphabet, Config::k, batch.sequence.data(),
+                                           batch.sequence.size(), r, n, nullptr, 0, &total,
+                                           nullptr);
     if (s != SBF_OK) return Err(detail::status_error(s));
     sequence_out.resize(total);
     records_out.resize(n);
-    s = sbf_normalize_record_batch(Config::k, batch.sequence.data(), batch.sequence.size(), r, n,
-                                   sequence_out.data(), total, &total,
-                                   reinterpret_cast<sbf_normalized_record*>(records_out.data()));
+    s = sbf_normalize_record_batch_for(
+        alphabet, Config::k, batch.sequence.data(), batch.sequence.size(), r, n,
+        sequence_out.data(), total, &total,
+        reinterpret_cast<sbf_normalized_record*>(records_out.data()));
     if (s != SBF_OK) return Err(detail::status_error(s));
     return {};
 }

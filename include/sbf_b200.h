@@ -244,6 +244,15 @@ int sbf_contains_dense_packed_to_device(const sbf_filter_t* filter, const uint64
 int sbf_contains_dense_packed(const sbf_filter_t* filter, const uint64_t* h_words,
                               uint64_t n_words, uint64_t num_symbols, uint8_t* h_out,
                               uint64_t out_len, sbf_stream_t stream);
+/* Dense input with bit-packed results (no reference counterpart): bit i % 32
+ * of word i / 32 is window i's result; with 2-bit input this moves a quarter
+ * byte in and an eighth of a byte out per window.  d_bits 4-byte aligned. */
+int sbf_contains_dense_packed_bits_async(const sbf_filter_t* filter, const uint64_t* d_words,
+                                         uint64_t n_words, uint64_t num_symbols, uint32_t* d_bits,
+                                         uint64_t n_bit_words, sbf_stream_t stream);
+int sbf_contains_dense_packed_bits(const sbf_filter_t* filter, const uint64_t* h_words,
+                                   uint64_t n_words, uint64_t num_symbols, uint32_t* h_bits,
+                                   uint64_t n_bit_words, sbf_stream_t stream);
 
 /* ---- record batches (filter.cuh:338-400, :549-622) ----------------- */
 
@@ -262,6 +271,20 @@ int sbf_normalize_record_batch(uint32_t k, const char* h_seq, uint64_t len,
 /* QueryLayout::build (include/cusbf/detail/query_layout.cuh:42-72). */
 int sbf_query_layout(uint32_t k, const sbf_normalized_record* records, uint64_t n,
                      sbf_query_layout_record* out, uint64_t* total_hits);
+/* The four above for any alphabet (SBF_ALPHABET_*): the DNA-triplet alphabet
+ * needs record ranges aligned to its 3-byte symbols; records are joined by
+ * one separator symbol (symbolWidth bytes of 'N', or '*' for proteins) after
+ * padding to a symbol boundary, valid windows are counted over symbols, and
+ * hit offsets are normalised symbol positions. */
+int sbf_validate_record_batch_for(int alphabet, uint64_t len, const sbf_record_range* ranges,
+                                  uint64_t n);
+uint64_t sbf_normalized_batch_bytes_for(int alphabet, const sbf_record_range* ranges, uint64_t n);
+int sbf_normalize_record_batch_for(int alphabet, uint32_t k, const char* h_seq, uint64_t len,
+                                   const sbf_record_range* ranges, uint64_t n, char* out,
+                                   uint64_t out_cap, uint64_t* out_len,
+                                   sbf_normalized_record* records_out);
+int sbf_query_layout_for(int alphabet, uint32_t k, const sbf_normalized_record* records,
+                         uint64_t n, sbf_query_layout_record* out, uint64_t* total_hits);
 
 /* insert_record_batch (filter.cuh:338-364): host records, separators injected
  * on the device; synchronises. */

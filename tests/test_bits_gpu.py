@@ -64,3 +64,33 @@ def test_bits_errors(sbf, cuda):
     raw = torch.zeros(200, dtype=torch.uint8, device="cuda")
     with pytest.raises(sbf.SbfError):
         f.contains_sequence_bits_async(q, (raw.data_ptr() + 1, 196))  # misaligned
+
+
+@pytest.mark.parametrize("cfg", [K31, dict(k=12, s=10, m=6, hashes=8, alphabet=2)],
+                         ids=["k31", "protein12"])
+@pytest.mark.parametrize("chunk", [None, "4096"])
+def test_dense_bits_match_dense_bytes(sbf, cuda, monkeypatch, cfg, chunk):
+    """Dense-packed input with bit-packed results (host pipeline and device
+    entry point) equals the dense byte results."""
+    torch = cuda
+    if chunk:
+        monkeypatch.setenv("SBF_HOST_CHUNK_BYTES", chunk)
+    rng = np.random.default_rng(len(cfg) + (chunk is None))
+    alphabet = cfg.get("alphabet", 0)
+    if alphabet == 2:
+        a = np.frombuffer(b"ACDEFGHIKLMNPQRSTVWY", np.uint8)
+        seq = a[rng.integers(0, a.size, 700_001)]
+    else:
+        seq = random_dna(rng, 700_001)
+    f = sbf.Filter(1 << 22, **cfg)
+    packed = sbf.pack_dense_sequence(seq, alphabet=alphabet)
+    f.insert_dense_packed(packed[: packed.size // 3], (packed.size // 3) * (64 // (5 if alphabet else 2)))
+    want = f.contains_dense_packed(packed, seq.size)
+    assert want.any() and not want.all()
+    got = f.contains_dense_packed_bits(packed, seq.size)
+    np.testing.assert_array_equal(got, _pack(want))
+    d_words = torch.from_numpy(packed.view(np.int64).copy()).cuda()
+    d_bits = torch.full((got.size + 3,), -1, dtype=torch.int32, device="cuda")
+    f.contains_dense_packed_bits_async(d_words, seq.size, d_bits[:got.size])
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d_bits[:got.size].cpu().numpy().view(np.uint32), got)

@@ -170,18 +170,117 @@ def test_record_paths_match_oracle(sbf, cuda, oracle_mod, cfg):
     assert fq.positive_kmers == int(posv.sum()) and fq.queried_kmers == int(valid.sum())
 
 
-def test_triplets_reject_record_paths(sbf, cuda):
-    f = sbf.Filter(1 << 14, k=3, s=2, m=2, hashes=4, alphabet=TRIPLET)
-    seq = np.frombuffer(b"ACGTACGTACGTACGTACGT" * 10, np.uint8)
+PROT = dict(k=5, s=4, m=3, hashes=4, alphabet=PROTEIN)   # ProteinTestConfig
+TRIP = dict(k=3, s=2, m=2, hashes=4, alphabet=TRIPLET)   # TripletTestConfig
+
+
+def test_reference_alphabet_known_answers(sbf, cuda):
+    """The reference's alphabet tests (tests/test_bloom_filter.cu:73-90,
+    243-338 of tdortman/cuSBF), restated."""
+    f = sbf.Filter(1 << 14, **PROT)
+    s = b"ACDEFGHIKLMNPQRSTVWYACDEF"
+    packed = sbf.pack_dense_sequence(s, alphabet=PROTEIN)
+    assert f.insert_dense_packed(packed, len(s)) == len(s) - 4
+    hits = f.contains_dense_packed(packed, len(s))
+    assert hits.size == len(s) - 4 and hits.all()
+    np.testing.assert_array_equal(hits, f.contains_sequence(s))
+    f = sbf.Filter(1 << 12, **PROT)
+    s = b"ABCDEFGHIJKLMNOPQRSTUVWXYZ"
+    assert f.insert_sequence(s) == len(s) - 4 and f.contains_sequence(s).all()
+    f = sbf.Filter(1 << 12, **PROT)
+    f.insert_sequence(s.lower())
+    assert f.contains_sequence(s).all() and f.contains_sequence(s.lower()).all()
+    f = sbf.Filter(1 << 12, **PROT)
+    s = b"ACDE*ACDEFGHI"
+    assert f.insert_sequence(s) == 9
+    assert list(f.contains_sequence(s)) == [0, 0, 0, 0, 0, 1, 1, 1, 1]
+    f = sbf.Filter(1 << 12, **TRIP)
+    s = b"ACGTACGTTAAACCCGGGTTT"
+    assert f.insert_sequence(s) == len(s) // 3 - 2 and f.contains_sequence(s).all()
+    f = sbf.Filter(1 << 12, **TRIP)
+    f.insert_sequence(s.lower())
+    assert f.contains_sequence(s).all() and f.contains_sequence(s.lower()).all()
+    f = sbf.Filter(1 << 12, **TRIP)
+    s = b"ACGTACNNNGGGTTTAAA"
+    assert f.insert_sequence(s) == 4
+    assert list(f.contains_sequence(s)) == [0, 0, 0, 1]
+    f = sbf.Filter(1 << 12, **TRIP)
+    s = b"ACGTACGTTAAACCCGGGTTTAA"
+    assert f.insert_sequence(s) == 5
+    hits = f.contains_sequence(s)
+    assert hits.size == 5 and hits.all()
+
+
+def test_triplet_record_paths_match_oracle(sbf, cuda, oracle_mod):
+    """Triplet record batches (ranges on symbol boundaries) and FASTA records
+    of any length (each padded to a symbol boundary by normalisation)."""
+    torch = cuda
+    cfg = dict(k=6, s=5, m=3, hashes=8, alphabet=TRIPLET)
+    rng = np.random.default_rng(41)
+    o = oracle_mod.Oracle(**cfg)
+    parts, ranges, pos = [], [], 0
+    for i in range(200):
+        n = 3 * int(rng.integers(0, 60))
+        g = 3 * int(rng.integers(0, 3))
+        parts.append(random_dna(rng, g + n, b"ACGTACGTACGTN"))
+        ranges.append((pos + g, n))
+        pos += g + n
+    seq = np.concatenate(parts)
+    bits = 1 << 16
+    f = sbf.Filter(bits, **cfg)
+    ins = f.insert_record_batch(seq, ranges[::2])
+    w = o.new_words(bits)
+    for off, n in ranges[::2]:
+        o.insert(w, seq[off:off + n])
+    np.testing.assert_array_equal(f.words_host(), w)
+    recs = []
+    rep = f.query_record_batch(seq, ranges, consume=recs.append)
+    total = 0
+    for (off, n), r in zip(ranges, recs):
+        want = o.contains(w, seq[off:off + n])
+        np.testing.assert_array_equal(r["hits"], want)
+        assert r["positive_kmers"] == int(want.sum())
+        total += int(want.sum())
+    assert rep.positive_kmers == total
+    assert ins.inserted_kmers == sum(int(o.window_shards(seq[a:a + n], 4)[1].sum())
+                                     for a, n in ranges[::2])
+    # the device record batch over the normalised sequence
+    norm, nrecs = sbf.normalize_record_batch(cfg["k"], seq, ranges, alphabet=TRIPLET)
+    layout, n_hits = sbf.query_layout(cfg["k"], nrecs, alphabet=TRIPLET)
+    d_norm = torch.from_numpy(norm.copy()).cuda()
+    d_out = torch.zeros(n_hits, dtype=torch.uint8, device="cuda")
+    nranges = [(lr.hit_offset * 3, lr.size) for lr in layout]
+    f.contains_record_batch_async(d_norm, nranges, d_out)
+    torch.cuda.synchronize()
+    h = d_out.cpu().numpy()
+    for lr, r in zip(layout, recs):
+        np.testing.assert_array_equal(h[lr.hit_offset:lr.hit_offset + lr.hit_count], r["hits"])
+    # FASTA records of unaligned lengths: trailing partial symbols ignored
+    fasta = b"".join(b">r%d\n" % i + random_dna(rng, int(rng.integers(0, 200))).tobytes() + b"\n"
+                     for i in range(100))
+    g = sbf.Filter(bits, **cfg)
+    frep = g.insert_fastx(fasta)
+    w2 = o.new_words(bits)
+    lines = fasta.split(b"\n")
+    want_kmers = 0
+    for ln in lines[1::2]:
+        a = np.frombuffer(ln, np.uint8)
+        if a.size:
+            o.insert(w2, a)
+            want_kmers += int(o.window_shards(a, 4)[1].sum())
+    np.testing.assert_array_equal(g.words_host(), w2)
+    assert frep.records_indexed == 100 and frep.inserted_kmers == want_kmers
+
+
+def test_triplets_reject_pipeline_paths(sbf, cuda):
+    f = sbf.Filter(1 << 14, **TRIP)
+    seq = np.frombuffer(b"ACGTACGTACGTACGTACGT" * 9, np.uint8)
     with pytest.raises(sbf.SbfError):
         f.ragged_insert(seq, [(0, 60)])
     with pytest.raises(sbf.SbfError):
-        f.query_record_batch(seq, [(0, 60)])
-    with pytest.raises(sbf.SbfError):
-        f.query_fastx(b">a\nACGTACGTACGT\n")
-    with pytest.raises(sbf.SbfError):
         sbf.Server(f)
-    # the sequence paths still work
+    with pytest.raises(sbf.SbfError):
+        f.query_record_batch(seq, [(1, 60)])  # not on a symbol boundary
     assert f.insert_sequence(seq) == seq.size // 3 - 2
 
 

@@ -42,3 +42,33 @@ def test_invalid_configs_rejected(sbf, cfg):
     with pytest.raises(sbf.SbfError) as ei:
         sbf.Filter(1 << 16, **cfg)
     assert ei.value.status == sbf.ERR_INVALID_ARGUMENT
+
+
+def test_normalize_protein_and_triplets(sbf):
+    # write_record_boundary (normalized_record_batch.hpp:209-232): one
+    # separator symbol between records -- '*' for proteins, "NNN" for triplets.
+    seq, recs = sbf.normalize_record_batch(3, "ACDEFGHI", [(0, 4), (4, 4)], alphabet=PROTEIN)
+    assert seq.tobytes() == b"ACDE*FGHI"
+    assert [r.valid_kmers for r in recs] == [2, 2]
+    seq, recs = sbf.normalize_record_batch(2, "ACGTACGGGTTT", [(0, 6), (6, 6)],
+                                           alphabet=TRIPLET)
+    assert seq.tobytes() == b"ACGTACNNNGGGTTT"
+    assert [r.valid_kmers for r in recs] == [1, 1]
+    assert sbf.normalized_batch_bytes([(0, 6), (6, 6)], alphabet=TRIPLET) == 15
+    layout, total = sbf.query_layout(2, recs, alphabet=TRIPLET)
+    assert (layout[0].hit_offset, layout[1].hit_offset) == (0, 3)
+    assert (layout[0].hit_count, layout[1].hit_count, total) == (1, 1, 4)
+    # an invalid triplet in a record (any of its three bytes) resets windows
+    _, recs = sbf.normalize_record_batch(2, "ACGACGNGG", [(0, 9)], alphabet=TRIPLET)
+    assert recs[0].valid_kmers == 1
+    _, recs = sbf.normalize_record_batch(2, "ACGNACGGG", [(0, 9)], alphabet=TRIPLET)
+    assert recs[0].valid_kmers == 0
+
+
+def test_triplet_ranges_must_align(sbf):
+    # filter.cuh:865-873
+    with pytest.raises(sbf.SbfError):
+        sbf.validate_record_batch(12, [(0, 4), (6, 6)], alphabet=TRIPLET)
+    with pytest.raises(sbf.SbfError):
+        sbf.normalize_record_batch(2, "ACGTACGTACGT", [(1, 6)], alphabet=TRIPLET)
+    sbf.validate_record_batch(12, [(0, 6), (6, 6)], alphabet=TRIPLET)
