@@ -590,6 +590,22 @@ def run_served(args, world: int, rank: int, local_rank: int) -> None:
     out_np = out_ring.numpy()
     check_idx = set(range(0, n_req, max(1, n_req // 64)))
     op_q = 3 if args.server_counts else 2 if args.server_bits else 1
+    # Dense wire format: request bodies are 2-bit packed words (packed once,
+    # as a client would store them); ranges count symbols.
+    dense_flag = 0x10 if args.server_dense else 0
+    q_body, i_body = pool_np, ins_np
+    if dense_flag:
+        def packed_pinned(host_u8):
+            d = torch.from_numpy(host_u8).to(dev)
+            d_w = torch.empty(sbf.Filter.dense_packed_word_count(d.numel()), dtype=torch.int64,
+                              device=dev)
+            sbf.pack_dense_sequence_device(d, d.numel(), d_w)
+            h = torch.empty(d_w.numel(), dtype=torch.int64).pin_memory()
+            torch.cuda.synchronize(dev)
+            h.copy_(d_w)
+            return h
+        q_words, i_words = packed_pinned(pool_np), packed_pinned(ins_np)
+        q_body, i_body = q_words.numpy(), i_words.numpy()
 
     def result_len(nr):
         """Result bytes of a query of nr reads: hit bytes, bit words, or
@@ -615,7 +631,8 @@ def run_served(args, world: int, rank: int, local_rank: int) -> None:
             while sbf.Server.now() < arrival:
                 pass
             if is_ins[i]:
-                srv.submit_raw(0, ins_np.ctypes.data, ins_range.ctypes.data + 16 * i, 1, None, 0,
+                srv.submit_raw(dense_flag, i_body.ctypes.data, ins_range.ctypes.data + 16 * i, 1,
+                               None, 0,
                                arrival)
             else:
                 nr = int(n_reads[i])
@@ -630,7 +647,7 @@ def run_served(args, world: int, rank: int, local_rank: int) -> None:
                         srv.wait(ring_live.pop(0)[0])
                     optr = out_np.ctypes.data + lo
                     ring_pos = hi
-                t = srv.submit_raw(op_q, pool_np.ctypes.data,
+                t = srv.submit_raw(op_q | dense_flag, q_body.ctypes.data,
                                    rng_np.ctypes.data + 16 * int(first[i]), nr, optr, w, arrival)
                 if i not in check_out:
                     ring_live.append((t, lo, hi))
@@ -707,9 +724,12 @@ def run_served(args, world: int, rank: int, local_rank: int) -> None:
                                f"{rate:.0f} req/s, filter of the 100 Mbp genome resident",
                    "query_results": {1: "one byte per window", 2: "bit-packed (op 2)",
                                      3: "per-read (valid, positive) counts (op 3)"}[op_q],
+                   "request_bodies": ("2-bit dense-packed words (op | 0x10; N packs as G)"
+                                      if dense_flag else "ASCII bytes"),
                    "k": K, "s": S, "m": M, "hashes": H, "filter_bits": bits,
                    "staging_budget_bytes": 16 << 30, "offered_bytes": int(offered),
                    "offered_gb_per_s": offered / duration / 1e9,
+                   "wire_gb_per_s": offered / duration / 1e9 / (4 if dense_flag else 1),
                    "read_pool": f"{pool_reads:,} reads of 150 bp (half sampled with 1% "
                                 "substitutions, half random); requests are pool slices",
                    "l2": "inputs larger than L2 (no flush needed)"},
@@ -743,6 +763,8 @@ def main() -> None:
                     help="c5: queries ask for bit-packed results")
     ap.add_argument("--server-counts", action="store_true",
                     help="c5: queries ask for per-read (valid, positive) counts only")
+    ap.add_argument("--server-dense", action="store_true",
+                    help="c5: request bodies are 2-bit dense-packed words")
     ap.add_argument("--rate", type=float, default=0.0, help="c5: offered req/s (default 20k)")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="reference arm: skip timing the reference GPU path")
@@ -1089,6 +1111,9 @@ def main() -> None:
                                         "--no-serial"], summarize_served)
         line["served_counts"] = run_form(["--config", "c5", "--duration", "2.0",
                                           "--server-counts", "--no-serial"], summarize_served)
+        line["served_dense_bits"] = run_form(["--config", "c5", "--duration", "2.0",
+                                              "--server-dense", "--server-bits", "--no-serial"],
+                                             summarize_served)
     print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -1130,6 +1155,7 @@ def summarize_served(d: dict) -> dict:
     sv, one, pl = d["served"], d.get("one_request_per_launch") or {}, d["plain_per_record"]
     return {"metric": d["metric"], "workload": d["config"]["workload"],
             "query_results": d["config"]["query_results"],
+            "request_bodies": d["config"].get("request_bodies"),
             "offered_gb_per_s": d["config"]["offered_gb_per_s"],
             "kmers_per_s": sv["kmers_per_s"], "requests_per_s": sv["requests_per_s"],
             "latency_ms": sv["latency_ms"], "mean_batch_requests": sv["mean_batch_requests"],

@@ -956,6 +956,9 @@ class Server:
     runs, the filter must not be used directly."""
 
     INSERT, QUERY, QUERY_BITS, QUERY_COUNTS = 0, 1, 2, 3
+    # Flag for any op: `base` holds 2-bit dense-packed DNA words (32 symbols
+    # per uint64) and `ranges` count symbols.
+    DENSE = 0x10
 
     def __init__(self, filt: "Filter", **config):
         self._filter = filt
@@ -982,12 +985,13 @@ class Server:
         b = _host_bytes(base)
         r = _ranges(ranges)
         o = out
-        if op != self.INSERT and o is None:
+        bop = op & 0xF
+        if bop != self.INSERT and o is None:
             span = max(int(r[-1, 0] + r[-1, 1]) - int(r[0, 0]), 0) if r.shape[0] else 0
-            w = self._filter.kmer_count(span)
-            if op == self.QUERY:
+            w = max(span - self._filter.config.k + 1, 0)
+            if bop == self.QUERY:
                 o = np.zeros(max(w, 1), np.uint8)
-            elif op == self.QUERY_COUNTS:
+            elif bop == self.QUERY_COUNTS:
                 o = np.zeros((max(r.shape[0], 1), 2), np.uint64)
             else:
                 o = np.zeros(max((w + 31) // 32, 1), np.uint32)

@@ -181,7 +181,7 @@ int sbf_filter::launch(bool query, bool dense, const void* input, uint64_t input
                                           : ks->query_dense;
     const uint64_t resident = static_cast<uint64_t>(sms) * static_cast<uint64_t>(occupancy[which]);
     const uint64_t grid = std::min<uint64_t>(p.n_tiles, std::max<uint64_t>(resident, 1));
-    fn<<<static_cast<unsigned>(grid), kThreads, query ? kQuerySlotBytes : kInsertSlotBytes, st>>>(p);
+    fn<<<static_cast<unsigned>(grid), kThreads, ks->smem(query), st>>>(p);
     SBF_CUDA(cudaGetLastError());
     ++launches;
     return SBF_OK;
@@ -379,7 +379,7 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
                                       ks->query_dense, ks->insert_ragged, ks->query_ragged};
         for (int i = 0; i < 6 && rc == SBF_OK; ++i) {
             // Query kernels: shard slots; insert kernels: flush staging ring.
-            const int dyn = (i & 1) ? kQuerySlotBytes : kInsertSlotBytes;
+            const int dyn = ks->smem((i & 1) != 0);
             if (dyn) {
                 e = cudaFuncSetAttribute(reinterpret_cast<const void*>(fns[i]),
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);

@@ -16,7 +16,7 @@
 // its bytes lie inside one record.
 //
 // The kernels take the same TileParams and launch shape as the tile kernels
-// (the dynamic shared memory they are given is not used), so every caller --
+// (with no dynamic shared memory, so more CTAs fit an SM), so every caller --
 // plain launches, host pipelines, ragged batches, the server -- runs them
 // unchanged.
 #include <cuda_runtime.h>
@@ -241,6 +241,8 @@ const KernelSet kGeneric = {
     generic_kernel<true, true, false>,
     generic_kernel<false, false, true>,
     generic_kernel<true, false, true>,
+    0,
+    0,
 };
 
 // Dense packing for any alphabet (pack_dense_sequence_kernel,

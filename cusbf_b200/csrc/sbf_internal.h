@@ -82,6 +82,11 @@ struct KernelSet {
     void (*query_dense)(TileParams);
     void (*insert_ragged)(TileParams);
     void (*query_ragged)(TileParams);
+    // Dynamic shared memory of the insert and query kernels: the tile
+    // kernels' flush ring and shard slots; none for the generic kernels.
+    int smem_insert = kInsertSlotBytes;
+    int smem_query = kQuerySlotBytes;
+    int smem(bool query) const { return query ? smem_query : smem_insert; }
 };
 
 // Returns the kernel table for a configuration, or nullptr when it is not

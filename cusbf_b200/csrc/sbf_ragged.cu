@@ -212,8 +212,7 @@ int ragged_launch(sbf_filter* f, bool query, const TileParams& p, uint32_t ctas,
                                  const_cast<uint32_t*>(p.tile_rec), st));
     SBF_CUDA(cudaMemsetAsync(p.queue, 0, sizeof(unsigned int), st));
     void (*fn)(TileParams) = query ? f->ks->query_ragged : f->ks->insert_ragged;
-    fn<<<ragged_grid(f, query, p.n_tiles, ctas), kThreads,
-         query ? kQuerySlotBytes : kInsertSlotBytes, st>>>(p);
+    fn<<<ragged_grid(f, query, p.n_tiles, ctas), kThreads, f->ks->smem(query), st>>>(p);
     SBF_CUDA(cudaGetLastError());
     f->launches += 2;
     return SBF_OK;
@@ -241,7 +240,7 @@ int ragged_graph_launch(sbf_filter* f, RaggedGraph& g, bool query, const TilePar
     tk.func = reinterpret_cast<void*>(query ? f->ks->query_ragged : f->ks->insert_ragged);
     tk.gridDim = dim3(ragged_grid(f, query, p.n_tiles, ctas));
     tk.blockDim = dim3(kThreads);
-    tk.sharedMemBytes = query ? kQuerySlotBytes : kInsertSlotBytes;
+    tk.sharedMemBytes = f->ks->smem(query);
     tk.kernelParams = tile_args;
     if (!g.exec) {
         SBF_CUDA(cudaGraphCreate(&g.graph, 0));

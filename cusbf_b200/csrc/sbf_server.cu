@@ -60,8 +60,16 @@ uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 // multiples of 32 bytes of the batch, so each request's bits start on a word
 // boundary.
 constexpr int kOpInsert = 0, kOpQuery = 1, kOpQueryBits = 2, kOpQueryCounts = 3;
-uint64_t pad_of(int op) { return op == kOpQueryBits ? 32 : 16; }
+// Flag on any operation: the request body is 2-bit dense-packed DNA (32
+// symbols per little-endian uint64, the reference's dense format,
+// dense_packed.hpp:36-50) and its ranges count symbols.  The batch is
+// unpacked to bytes on the GPU, so a quarter of the bytes cross PCIe.
+constexpr int kOpDense = 0x10;
+int base_op(int op) { return op & 0xF; }
+bool is_dense(int op) { return (op & kOpDense) != 0; }
+uint64_t pad_of(int op) { return base_op(op) == kOpQueryBits ? 32 : 16; }
 uint64_t result_bytes(int op, uint64_t windows, uint64_t records) {
+    op = base_op(op);
     return op == kOpQueryBits     ? (windows + 31) / 32 * 4
            : op == kOpQuery       ? windows
            : op == kOpQueryCounts ? records * 16
@@ -69,8 +77,11 @@ uint64_t result_bytes(int op, uint64_t windows, uint64_t records) {
 }
 // Device bytes of a batch's result region.
 uint64_t out_region(int op, uint64_t seq_bytes, uint64_t records) {
+    op = base_op(op);
     return op == kOpInsert ? 0 : align_up(op == kOpQueryCounts ? records * 16 : seq_bytes, kAlign);
 }
+// Packed words holding symbols [lo, hi).
+uint64_t dense_words(uint64_t lo, uint64_t hi) { return hi > lo ? (hi + 31) / 32 - lo / 32 : 0; }
 
 // FIFO ring allocator: regions are released in allocation order.  The
 // live regions occupy [tail, head) when head > tail and wrap around the end
@@ -134,6 +145,7 @@ struct SrvBatch {
     std::vector<uint64_t> req_off;  // each request's first byte in the batch
     std::vector<uint64_t> req_rec;  // each request's first record in the batch
     uint64_t seq_bytes = 0, n_ranges = 0;
+    uint64_t packed_bytes = 0;  // dense batches: staged packed words
     uint64_t dev_off = 0, dev_bytes = 0, pin_off = 0, pin_bytes = 0;
     bool complete = false;
     int status = SBF_OK;
@@ -146,6 +158,42 @@ struct FixEntry {
     uint64_t dst, n;
     int64_t delta;
 };
+
+// Dense batches: request e's symbols [sym0, sym0 + n_sym) of the packed
+// words starting at word src_word are written as bytes at dst.  The batch's
+// work is cut into segments of kUnpackSeg symbols; entry e's segments are
+// the global segments [seg0, seg0 + ceil(n_sym / kUnpackSeg)).
+constexpr uint64_t kUnpackSeg = 8192;
+struct UnpackEntry {
+    uint64_t src_word, sym0, n_sym, dst, seg0;
+};
+
+// A-C-T-G for codes 0-3 (DnaAlphabet, Alphabet.cuh:132-141).  CTAs take the
+// batch's segments grid-strided, so many small requests and a few large
+// ones spread over the grid alike.
+__global__ void unpack_dense_kernel(const uint64_t* packed, const UnpackEntry* tab,
+                                    uint32_t n_tab, uint64_t n_segs, uint8_t* seq) {
+    for (uint64_t g = blockIdx.x; g < n_segs; g += gridDim.x) {
+        // The entry holding segment g (last entry with seg0 <= g).
+        uint32_t lo = 0, hi = n_tab;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (tab[mid].seg0 <= g)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const UnpackEntry u = tab[lo];
+        const uint64_t t0 = (g - u.seg0) * kUnpackSeg;
+        const uint64_t t1 = t0 + kUnpackSeg < u.n_sym ? t0 + kUnpackSeg : u.n_sym;
+        for (uint64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+            const uint64_t sym = u.sym0 + t;
+            const uint32_t code =
+                static_cast<uint32_t>(packed[u.src_word + sym / 32] >> (2 * (sym % 32))) & 3u;
+            seq[u.dst + t] = static_cast<uint8_t>(0x47544341u >> (8 * code));
+        }
+    }
+}
 
 __global__ void rebase_ranges_kernel(DevRange* rng, const FixEntry* tab, uint32_t n_tab) {
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -203,7 +251,7 @@ void Server::complete(SrvBatch* b, int status) {
         r->status = status;
         r->done = true;
         latencies.push_back(t - r->t_arrival);
-        (r->op != kOpInsert ? q_windows : i_windows) += r->windows;
+        (base_op(r->op) != kOpInsert ? q_windows : i_windows) += r->windows;
         ++n_reqs;
         if (t_first == 0 || r->t_arrival < t_first) t_first = r->t_arrival;
         t_last = std::max(t_last, t);
@@ -269,7 +317,8 @@ void Server::run() {
         // The longest same-operation run of queued requests within the caps.
         auto* b = new SrvBatch();
         b->op = pending.front()->op;
-        uint64_t seq = 0, nr = 0, gather = 0;
+        const bool dense = is_dense(b->op);
+        uint64_t seq = 0, nr = 0, gather = 0, packed = 0;
         size_t take = 0;
         for (SrvRequest* r : pending) {
             if (r->op != b->op) break;
@@ -280,16 +329,21 @@ void Server::run() {
                 break;
             seq += span;
             nr += r->n;
-            if (!(r->pinned && span >= kDirectBytes)) gather += span;
+            // Bytes staged for the request: its span, or its packed words.
+            const uint64_t staged = dense ? dense_words(r->lo, r->hi) * 8 : span;
+            packed += dense ? staged : 0;
+            if (!(r->pinned && staged >= kDirectBytes)) gather += staged;
             ++take;
         }
         const uint64_t n_tiles = seq / kTileKmers + 2;
+        const uint64_t unpack_tab = dense ? align_up(take * sizeof(UnpackEntry), kAlign) : 0;
         const uint64_t dev_bytes = align_up(seq, kAlign) + out_region(b->op, seq, nr) +
                                    align_up(nr * sizeof(DevRange), kAlign) +
                                    align_up(n_tiles * 4, kAlign) +
-                                   align_up(take * sizeof(FixEntry), kAlign);
-        const uint64_t pin_bytes = align_up(nr * sizeof(DevRange), kAlign) +
                                    align_up(take * sizeof(FixEntry), kAlign) +
+                                   (dense ? align_up(packed, kAlign) : 0) + unpack_tab;
+        const uint64_t pin_bytes = align_up(nr * sizeof(DevRange), kAlign) +
+                                   align_up(take * sizeof(FixEntry), kAlign) + unpack_tab +
                                    align_up(gather, kAlign);
         // Admission: wait for ring space (completions free it).
         for (;;) {
@@ -327,6 +381,7 @@ void Server::run() {
         b->pin_bytes = pin_bytes;
         b->seq_bytes = seq;
         b->n_ranges = nr;
+        b->packed_bytes = packed;
         for (size_t i = 0; i < take; ++i) {
             b->reqs.push_back(pending.front());
             pending.pop_front();
@@ -366,9 +421,9 @@ void Server::run() {
 }
 
 int Server::launch(SrvBatch* b) {
-    const bool query = b->op != kOpInsert;
-    const bool bits = b->op == kOpQueryBits;
-    const bool tally = b->op == kOpQueryCounts;
+    const bool query = base_op(b->op) != kOpInsert;
+    const bool bits = base_op(b->op) == kOpQueryBits;
+    const bool tally = base_op(b->op) == kOpQueryCounts;
     uint8_t* dbase = d_ring + b->dev_off;
     uint8_t* d_seq = dbase;
     uint8_t* d_out = query ? dbase + align_up(b->seq_bytes, kAlign) : nullptr;
@@ -378,19 +433,28 @@ int Server::launch(SrvBatch* b) {
                                                align_up(b->n_ranges * sizeof(DevRange), kAlign));
     auto* d_fix = reinterpret_cast<FixEntry*>(
         reinterpret_cast<uint8_t*>(d_tile) + align_up((b->seq_bytes / kTileKmers + 2) * 4, kAlign));
+    const bool dense = is_dense(b->op);
+    const uint64_t unpack_tab = dense ? align_up(b->reqs.size() * sizeof(UnpackEntry), kAlign) : 0;
+    uint8_t* d_packed =
+        reinterpret_cast<uint8_t*>(d_fix) + align_up(b->reqs.size() * sizeof(FixEntry), kAlign);
+    auto* d_unpack =
+        reinterpret_cast<UnpackEntry*>(d_packed + (dense ? align_up(b->packed_bytes, kAlign) : 0));
     auto* h_rng = reinterpret_cast<DevRange*>(h_ring + b->pin_off);
     auto* h_fix = reinterpret_cast<FixEntry*>(h_ring + b->pin_off +
                                               align_up(b->n_ranges * sizeof(DevRange), kAlign));
-    uint8_t* h_gather = reinterpret_cast<uint8_t*>(h_fix) +
-                        align_up(b->reqs.size() * sizeof(FixEntry), kAlign);
-    uint64_t o = 0, k = 0, g = 0;
-    uint32_t n_fix = 0;
-    // Consecutive gathered requests are one copy.
+    auto* h_unpack = reinterpret_cast<UnpackEntry*>(
+        reinterpret_cast<uint8_t*>(h_fix) + align_up(b->reqs.size() * sizeof(FixEntry), kAlign));
+    uint8_t* h_gather = reinterpret_cast<uint8_t*>(h_unpack) + unpack_tab;
+    uint64_t o = 0, k = 0, g = 0, pw = 0, n_segs = 0;
+    uint32_t n_fix = 0, n_unpack = 0;
+    // Consecutive gathered requests are one copy (into the sequence region,
+    // or into the packed-word region for dense batches).
+    uint8_t* run_base = dense ? d_packed : d_seq;
     uint64_t run_dev = 0, run_pin = 0, run_bytes = 0;
     auto flush_run = [&]() -> cudaError_t {
         cudaError_t e = cudaSuccess;
         if (run_bytes)
-            e = cudaMemcpyAsync(d_seq + run_dev, h_gather + run_pin, run_bytes,
+            e = cudaMemcpyAsync(run_base + run_dev, h_gather + run_pin, run_bytes,
                                 cudaMemcpyHostToDevice, up);
         run_bytes = 0;
         return e;
@@ -411,7 +475,30 @@ int Server::launch(SrvBatch* b) {
                 FixEntry{k, r->n, static_cast<int64_t>(o) - static_cast<int64_t>(r->lo)};
             k += r->n;
         }
-        if (r->pinned && padded >= kDirectBytes) {
+        if (dense) {
+            // Packed words of symbols [lo, hi), unpacked to d_seq + o.
+            const uint64_t nw = dense_words(r->lo, r->hi);
+            const uint8_t* src = r->base + (r->lo / 32) * 8;
+            if (nw) {
+                h_unpack[n_unpack++] = UnpackEntry{pw, r->lo % 32, span, o, n_segs};
+                n_segs += (span + kUnpackSeg - 1) / kUnpackSeg;
+                if (r->pinned && nw * 8 >= kDirectBytes) {
+                    e = flush_run();
+                    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(batch)");
+                    e = cudaMemcpyAsync(d_packed + pw * 8, src, nw * 8, cudaMemcpyHostToDevice, up);
+                    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(request)");
+                } else {
+                    std::memcpy(h_gather + g, src, nw * 8);
+                    if (run_bytes == 0) {
+                        run_dev = pw * 8;
+                        run_pin = g;
+                    }
+                    run_bytes = (g + nw * 8) - run_pin;
+                    g += nw * 8;
+                }
+                pw += nw;
+            }
+        } else if (r->pinned && padded >= kDirectBytes) {
             e = flush_run();
             if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(batch)");
             e = cudaMemcpyAsync(d_seq + o, r->base + r->lo, span, cudaMemcpyHostToDevice, up);
@@ -435,11 +522,24 @@ int Server::launch(SrvBatch* b) {
         e = cudaMemcpyAsync(d_fix, h_fix, n_fix * sizeof(FixEntry), cudaMemcpyHostToDevice, up);
         if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(rebase table)");
     }
+    if (n_unpack) {
+        e = cudaMemcpyAsync(d_unpack, h_unpack, n_unpack * sizeof(UnpackEntry),
+                            cudaMemcpyHostToDevice, up);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(unpack table)");
+    }
     if ((e = cudaEventRecord(b->ev_up, up)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
     if ((e = cudaStreamWaitEvent(comp, b->ev_up, 0)) != cudaSuccess)
         return cuda_fail(e, "cudaStreamWaitEvent");
-    // The rebase runs on the compute stream: the upload stream carries only
-    // copies, so it never waits for SMs held by the previous batch's kernel.
+    // The unpack and the rebase run on the compute stream: the upload stream
+    // carries only copies, so it never waits for SMs held by the previous
+    // batch's kernel.
+    if (n_unpack) {
+        const unsigned blocks =
+            static_cast<unsigned>(std::min<uint64_t>(n_segs, static_cast<uint64_t>(f->sms) * 8));
+        unpack_dense_kernel<<<blocks, 256, 0, comp>>>(reinterpret_cast<const uint64_t*>(d_packed),
+                                                      d_unpack, n_unpack, n_segs, d_seq);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "unpack_dense_kernel");
+    }
     if (n_fix) {
         const unsigned blocks = std::min<unsigned>((n_fix * 32 + 255) / 256, 1024);
         rebase_ranges_kernel<<<blocks, 256, 0, comp>>>(d_rng, d_fix, n_fix);
@@ -568,10 +668,12 @@ extern "C" int sbf_server_submit(sbf_server_t* h, int op, const char* base,
                                  uint64_t out_len, double arrival, uint64_t* ticket) {
     if (!h || !ticket) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     Server& s = h->s;
-    if (op != kOpInsert && op != kOpQuery && op != kOpQueryBits && op != kOpQueryCounts)
+    if ((op & ~(kOpDense | 0xF)) != 0 || base_op(op) > kOpQueryCounts)
         return set_error(SBF_ERR_INVALID_ARGUMENT,
                          "op must be 0 (insert), 1 (query), 2 (query, bit-packed) or 3 (query, "
-                         "per-record counts)");
+                         "per-record counts), optionally with 0x10 (dense-packed input)");
+    if (is_dense(op) && s.f->alphabet != SBF_ALPHABET_DNA)
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "dense-packed requests need the DNA alphabet");
     if (n && (!ranges || !base)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     auto r = std::make_unique<SrvRequest>();
     r->op = op;
@@ -589,7 +691,8 @@ extern "C" int sbf_server_submit(sbf_server_t* h, int op, const char* base,
     }
     const uint64_t span = r->hi - r->lo;
     r->windows = span >= s.f->k ? span - s.f->k + 1 : 0;
-    const bool has_result = op == kOpQueryCounts ? n > 0 : (op != kOpInsert && r->windows > 0);
+    const bool has_result =
+        base_op(op) == kOpQueryCounts ? n > 0 : (base_op(op) != kOpInsert && r->windows > 0);
     if (has_result && (!out || out_len < result_bytes(op, r->windows, n)))
         return set_error(SBF_ERR_INVALID_ARGUMENT, "query output span is too small");
     if (align_up(span, pad_of(op)) > s.cfg.max_batch_bytes || n * sizeof(DevRange) > s.cfg.max_batch_bytes)
@@ -598,7 +701,7 @@ extern "C" int sbf_server_submit(sbf_server_t* h, int op, const char* base,
                          static_cast<unsigned long long>(span),
                          static_cast<unsigned long long>(s.cfg.max_batch_bytes));
     r->out = out;
-    r->pinned = span && is_pinned(base + r->lo);
+    r->pinned = span && is_pinned(base + (is_dense(op) ? (r->lo / 32) * 8 : r->lo));
     r->t_arrival = arrival > 0 ? arrival : now_s();
     std::lock_guard<std::mutex> lk(s.mu);
     if (s.fatal != SBF_OK)

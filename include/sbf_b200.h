@@ -458,7 +458,9 @@ double sbf_server_now(void);
  * results (out[] as 32-bit words, bit i % 32 of word i / 32 for window i;
  * out_len >= 4 * ceil((span - k + 1) / 32)), 3 = query returning only
  * per-record counts (out[] as 2n uint64: record r's valid windows at 2r,
- * positive windows at 2r + 1; out_len >= 16 n).  Records are (offset, bytes)
+ * positive windows at 2r + 1; out_len >= 16 n).  op | 0x10: `base` holds
+ * 2-bit dense-packed DNA words (sbf_pack_dense_host layout) and the ranges
+ * count symbols; the words are unpacked on the GPU.  Records are (offset, bytes)
  * ranges into `base`, ordered and non-overlapping; the request's span is
  * [ranges[0].offset, end of ranges[n-1]).  A query writes one byte per
  * window of the span to out[0 .. span - k] (out_len >= span - k + 1): the

@@ -285,3 +285,53 @@ def test_count_requests_match_bytes(sbf, cuda, cfg):
     srv.close()
     assert n_counts > 20
     np.testing.assert_array_equal(f.words_host(), want_words)
+
+
+def _dense_equivalent(base):
+    """The bytes a 2-bit dense round trip gives: invalid bases (N) pack as
+    code 3 and come back as G (dense_packed.hpp:36-50)."""
+    s = base.copy()
+    s[~_VALID[s]] = ord("G")
+    return s
+
+
+def _pack_bits(hits):
+    b = np.packbits(hits.astype(np.uint8), bitorder="little")
+    n_words = max((hits.size + 31) // 32, 1)
+    b = np.concatenate([b, np.zeros(n_words * 4 - b.size, np.uint8)])
+    return b.view(np.uint32)[:(hits.size + 31) // 32]
+
+
+@pytest.mark.parametrize("cfg", [dict(), dict(use_graph=1, max_inflight=2),
+                                 dict(max_batch_bytes=1 << 18, max_inflight=4)],
+                         ids=["default", "graph", "small-batches"])
+def test_dense_requests_match_serial(sbf, cuda, cfg):
+    """Requests with 2-bit dense-packed bodies (op | 0x10), mixed with byte
+    requests of every op, equal serial execution of the same bases."""
+    rng = np.random.default_rng(43)
+    genome = random_dna(rng, 300_000)
+    reqs = [(op, _dense_equivalent(base), ranges)
+            for op, base, ranges in _make_requests(rng, genome, 160)]
+    bits = 1 << 22
+    want, want_words = _serial(sbf, genome, reqs, bits)
+    f = sbf.Filter(bits, **K31)
+    f.insert_sequence(genome)
+    srv = sbf.Server(f, staging_bytes=1 << 28, pinned_bytes=1 << 26, **cfg)
+    ops, tickets = [], []
+    for i, (op, base, ranges) in enumerate(reqs):
+        q = op if op == 0 else (1, 2, 3)[i % 3]
+        dense = i % 2 == 0
+        body = sbf.pack_dense_sequence(base) if dense else base
+        ops.append(q)
+        tickets.append(srv.submit(q | (sbf.Server.DENSE if dense else 0), body, ranges))
+    for i, (q, t, w, (_, base, ranges)) in enumerate(zip(ops, tickets, want, reqs)):
+        info, res = srv.wait(t, timeout=60.0)
+        assert info["status"] == 0
+        if q == 1:
+            np.testing.assert_array_equal(res, w, err_msg=f"request {i}")
+        elif q == 2:
+            np.testing.assert_array_equal(res, _pack_bits(w), err_msg=f"request {i}")
+        elif q == 3:
+            np.testing.assert_array_equal(res, _record_counts(base, ranges, w))
+    srv.close()
+    np.testing.assert_array_equal(f.words_host(), want_words)
