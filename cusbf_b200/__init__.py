@@ -206,6 +206,7 @@ _sig("sbf_filter_destroy", None, _vp)
 _sig("sbf_filter_clear", C.c_int, _vp, _vp)
 _sig("sbf_filter_bits", _u64, _vp)
 _sig("sbf_filter_num_shards", _u64, _vp)
+_sig("sbf_filter_kernel_path", C.c_int, _vp)
 _sig("sbf_filter_words", C.c_int, _vp, C.POINTER(_vp), C.POINTER(_u64))
 _sig("sbf_filter_load_factor", C.c_int, _vp, _vp, C.POINTER(C.c_double))
 _sig("sbf_filter_kmer_count", _u64, _vp, _u64)
@@ -421,6 +422,14 @@ class Filter:
 
     def num_shards(self) -> int:
         return _lib.sbf_filter_num_shards(self._h)
+
+    KERNELS_COMPILED, KERNELS_RUNTIME_COMPILED, KERNELS_GENERIC = 0, 1, 2
+
+    def kernel_path(self) -> int:
+        """0: tile kernels compiled into the library; 1: the same kernels
+        compiled at run time for this configuration; 2: the
+        runtime-parameterised kernels.  Results are identical."""
+        return _lib.sbf_filter_kernel_path(self._h)
 
     def clear(self, stream=None) -> None:
         _check(_lib.sbf_filter_clear(self._h, _stream(stream)))

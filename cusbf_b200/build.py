@@ -37,18 +37,39 @@ def _stale(target: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+# The tile kernel source, embedded for run-time compilation (sbf_jit.cpp).
+JIT_SOURCES = [("kJitInternal", "sbf_internal.h"), ("kJitDevice", "sbf_device.cuh"),
+               ("kJitTile", "sbf_tile.cuh")]
+
+
+def write_jit_sources(objdir: str) -> None:
+    out = []
+    for var, name in JIT_SOURCES:
+        text = open(os.path.join(CSRC, name)).read()
+        if ")SBFJIT\"" in text:
+            raise RuntimeError(f"{name} contains the raw-string delimiter")
+        out.append(f'static const char {var}[] = R"SBFJIT({text})SBFJIT";\n')
+    path = os.path.join(objdir, "sbf_jit_sources.inc")
+    data = "".join(out)
+    if not os.path.exists(path) or open(path).read() != data:
+        with open(path, "w") as fh:
+            fh.write(data)
+
+
 def build(verbose: bool = False, force: bool = False) -> str:
     srcs = sources()
     if not force and not _stale(LIB, srcs + headers() + [__file__]):
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
+    write_jit_sources(objdir)
     objs = []
     procs = []
     for src in srcs:
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         objs.append(obj)
-        cmd = [NVCC, *ARCH_FLAGS, *COMMON, "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
+        cmd = [NVCC, *ARCH_FLAGS, *COMMON, "-I", os.path.join(ROOT, "include"), "-I", objdir,
+               "-c", src, "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), file=sys.stderr)
@@ -63,7 +84,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     if failed:
         raise RuntimeError(f"nvcc failed for {failed}")
     tmp = LIB + ".tmp"
-    link = [NVCC, *ARCH_FLAGS, "-shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs, "-lz"]
+    link = [NVCC, *ARCH_FLAGS, "-shared", "-Xcompiler", "-fPIC", "-o", tmp, *objs, "-lz", "-ldl"]
     subprocess.run(link, check=True)
     os.replace(tmp, LIB)
     return LIB

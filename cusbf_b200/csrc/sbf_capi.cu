@@ -175,14 +175,13 @@ int sbf_filter::launch(bool query, bool dense, const void* input, uint64_t input
     p.err = d_err;
     p.gen = gen;
     const int which = (query ? 1 : 0) + (dense ? 2 : 0);
-    void (*fn)(TileParams) = which == 0   ? ks->insert_bytes
-                             : which == 1 ? ks->query_bytes
-                             : which == 2 ? ks->insert_dense
-                                          : ks->query_dense;
+    const void* fn = which == 0   ? ks->insert_bytes
+                     : which == 1 ? ks->query_bytes
+                     : which == 2 ? ks->insert_dense
+                                  : ks->query_dense;
     const uint64_t resident = static_cast<uint64_t>(sms) * static_cast<uint64_t>(occupancy[which]);
     const uint64_t grid = std::min<uint64_t>(p.n_tiles, std::max<uint64_t>(resident, 1));
-    fn<<<static_cast<unsigned>(grid), kThreads, ks->smem(query), st>>>(p);
-    SBF_CUDA(cudaGetLastError());
+    SBF_CUDA(launch_set_kernel(ks, fn, static_cast<unsigned>(grid), query, p, st));
     ++launches;
     return SBF_OK;
 }
@@ -347,13 +346,14 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
         return set_error(SBF_ERR_INVALID_ARGUMENT,
                          "hash count %u must be 4, 8, 12 or 16 (a multiple of the 4 shard words)",
                          hashes);
-    // Specialised tile kernels for the compiled DNA configurations; the
-    // runtime-parameterised kernels for everything else.
+    // Specialised tile kernels for the compiled DNA configurations, the same
+    // kernels compiled at run time for other DNA configurations (below, once
+    // the device is known), and the runtime-parameterised kernels for the
+    // other alphabets or when run-time compilation is not possible.
     const KernelSet* ks = alphabet == SBF_ALPHABET_DNA
                               ? find_kernels(static_cast<int>(k), static_cast<int>(s),
                                              static_cast<int>(m), static_cast<int>(hashes))
                               : nullptr;
-    if (!ks) ks = generic_kernels();
     uint64_t blocks = requested_bits / 256 + (requested_bits % 256 != 0);
     if (blocks < 1) blocks = 1;
     uint64_t shards = 1;
@@ -375,9 +375,17 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
         if (e != cudaSuccess) { rc = cuda_fail(e, "cudaGetDevice"); break; }
         e = cudaDeviceGetAttribute(&f->sms, cudaDevAttrMultiProcessorCount, f->device);
         if (e != cudaSuccess) { rc = cuda_fail(e, "cudaDeviceGetAttribute"); break; }
-        void (*fns[6])(TileParams) = {ks->insert_bytes, ks->query_bytes, ks->insert_dense,
-                                      ks->query_dense, ks->insert_ragged, ks->query_ragged};
-        for (int i = 0; i < 6 && rc == SBF_OK; ++i) {
+        if (!ks && alphabet == SBF_ALPHABET_DNA)
+            ks = jit_kernels(static_cast<int>(k), static_cast<int>(s), static_cast<int>(m),
+                             static_cast<int>(hashes), f->device);
+        if (!ks) ks = generic_kernels();
+        f->ks = ks;
+        const void* fns[6] = {ks->insert_bytes, ks->query_bytes, ks->insert_dense,
+                              ks->query_dense, ks->insert_ragged, ks->query_ragged};
+        // Run-time compiled kernels have their attributes set when loaded and
+        // run two CTAs per SM, as their shared memory allows.
+        for (int i = 0; i < 6 && ks->jit; ++i) f->occupancy[i] = 2;
+        for (int i = 0; i < 6 && rc == SBF_OK && !ks->jit; ++i) {
             // Query kernels: shard slots; insert kernels: flush staging ring.
             const int dyn = ks->smem((i & 1) != 0);
             if (dyn) {
@@ -463,6 +471,11 @@ extern "C" int sbf_filter_clear(sbf_filter_t* f, sbf_stream_t stream) {
 
 extern "C" uint64_t sbf_filter_bits(const sbf_filter_t* f) { return f ? f->filter_bits : 0; }
 extern "C" uint64_t sbf_filter_num_shards(const sbf_filter_t* f) { return f ? f->num_shards : 0; }
+
+extern "C" int sbf_filter_kernel_path(const sbf_filter_t* f) {
+    if (!f || !f->ks) return -1;
+    return f->ks->jit ? 1 : f->ks == generic_kernels() ? 2 : 0;
+}
 
 extern "C" int sbf_filter_words(const sbf_filter_t* f, uint64_t** d_words, uint64_t* n_words) {
     if (!f || !d_words || !n_words) return set_error(SBF_ERR_INVALID_ARGUMENT, "null argument");

@@ -15,7 +15,9 @@
 // therefore reproduces the per-window values bit for bit.
 #pragma once
 
+#ifndef __CUDACC_RTC__
 #include <cstdint>
+#endif
 
 namespace sbf {
 
@@ -103,6 +105,9 @@ __device__ __forceinline__ uint32_t dense16_to_code(uint32_t v) {
 __device__ __forceinline__ uint64_t mmer_hash(uint32_t mmer) {
     return static_cast<uint64_t>(mmer) * kMinimizerMul;
 }
+
+// m-mers longer than 16 bases.
+__device__ __forceinline__ uint64_t mmer_hash(uint64_t mmer) { return mmer * kMinimizerMul; }
 
 __device__ __forceinline__ uint64_t smer_hash(uint64_t smer) {
     uint64_t h = smer * kSmerMul;

@@ -233,14 +233,19 @@ __global__ void __launch_bounds__(kThreads) generic_kernel(TileParams p) {
     }
 }
 
+template <bool Q, bool D, bool R>
+const void* generic_ptr() {
+    return reinterpret_cast<const void*>(&generic_kernel<Q, D, R>);
+}
+
 const KernelSet kGeneric = {
     0, 0, 0, 0,
-    generic_kernel<false, false, false>,
-    generic_kernel<true, false, false>,
-    generic_kernel<false, true, false>,
-    generic_kernel<true, true, false>,
-    generic_kernel<false, false, true>,
-    generic_kernel<true, false, true>,
+    generic_ptr<false, false, false>(),
+    generic_ptr<true, false, false>(),
+    generic_ptr<false, true, false>(),
+    generic_ptr<true, true, false>(),
+    generic_ptr<false, false, true>(),
+    generic_ptr<true, false, true>(),
     0,
     0,
 };

@@ -1,9 +1,11 @@
 // sbf_internal.h -- types shared by the kernels and the C-ABI layer.
 #pragma once
 
+#ifndef __CUDACC_RTC__
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#endif
 
 namespace sbf {
 
@@ -74,18 +76,22 @@ enum : int {
 
 // Function table for one compiled configuration <K,S,M,H> (k = s = m = h = 0
 // for the generic table, whose kernels read TileParams::gen).
+#ifndef __CUDACC_RTC__
+// Kernels are launched with cudaLaunchKernel(fn, ...): a compiled kernel's
+// host stub, or a cudaKernel_t of a kernel compiled at run time (jit).
 struct KernelSet {
     int k, s, m, h;
-    void (*insert_bytes)(TileParams);
-    void (*query_bytes)(TileParams);
-    void (*insert_dense)(TileParams);
-    void (*query_dense)(TileParams);
-    void (*insert_ragged)(TileParams);
-    void (*query_ragged)(TileParams);
+    const void* insert_bytes;
+    const void* query_bytes;
+    const void* insert_dense;
+    const void* query_dense;
+    const void* insert_ragged;
+    const void* query_ragged;
     // Dynamic shared memory of the insert and query kernels: the tile
     // kernels' flush ring and shard slots; none for the generic kernels.
     int smem_insert = kInsertSlotBytes;
     int smem_query = kQuerySlotBytes;
+    bool jit = false;  // loaded from a run-time compiled library
     int smem(bool query) const { return query ? smem_query : smem_insert; }
 };
 
@@ -104,5 +110,12 @@ cudaError_t launch_tile_records(const DevRange* ranges, uint64_t n_ranges, int64
                                 uint64_t n_tiles, uint32_t* tile_rec, cudaStream_t stream);
 cudaError_t launch_popcount(const uint64_t* words, uint64_t n_words, unsigned long long* out,
                             cudaStream_t stream);
+// Tile kernels compiled at run time for a DNA configuration that is not
+// compiled into the library (sbf_jit.cpp); nullptr when that is not possible.
+const KernelSet* jit_kernels(int k, int s, int m, int h, int device);
+// Launches one of a KernelSet's kernels.
+cudaError_t launch_set_kernel(const KernelSet* ks, const void* fn, unsigned grid, bool query,
+                              const TileParams& p, cudaStream_t stream);
+#endif
 
 }  // namespace sbf

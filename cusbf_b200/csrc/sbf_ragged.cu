@@ -211,9 +211,8 @@ int ragged_launch(sbf_filter* f, bool query, const TileParams& p, uint32_t ctas,
     SBF_CUDA(launch_tile_records(p.ranges, p.n_ranges, p.sym_base, p.n_tiles,
                                  const_cast<uint32_t*>(p.tile_rec), st));
     SBF_CUDA(cudaMemsetAsync(p.queue, 0, sizeof(unsigned int), st));
-    void (*fn)(TileParams) = query ? f->ks->query_ragged : f->ks->insert_ragged;
-    fn<<<ragged_grid(f, query, p.n_tiles, ctas), kThreads, f->ks->smem(query), st>>>(p);
-    SBF_CUDA(cudaGetLastError());
+    const void* fn = query ? f->ks->query_ragged : f->ks->insert_ragged;
+    SBF_CUDA(launch_set_kernel(f->ks, fn, ragged_grid(f, query, p.n_tiles, ctas), query, p, st));
     f->launches += 2;
     return SBF_OK;
 }
@@ -223,6 +222,9 @@ int ragged_launch(sbf_filter* f, bool query, const TileParams& p, uint32_t ctas,
 int ragged_graph_launch(sbf_filter* f, RaggedGraph& g, bool query, const TileParams& p,
                         uint32_t ctas, cudaStream_t st) {
     if (p.n_tiles == 0) return SBF_OK;
+    // Graph kernel nodes take compiled kernels; run-time compiled ones are
+    // launched on the stream.
+    if (f->ks->jit) return ragged_launch(f, query, p, ctas, st);
     const DevRange* a_rng = p.ranges;
     uint64_t a_n = p.n_ranges;
     int64_t a_base = p.sym_base;
@@ -237,7 +239,7 @@ int ragged_graph_launch(sbf_filter* f, RaggedGraph& g, bool query, const TilePar
     rk.blockDim = dim3(256);
     rk.kernelParams = rec_args;
     cudaKernelNodeParams tk{};
-    tk.func = reinterpret_cast<void*>(query ? f->ks->query_ragged : f->ks->insert_ragged);
+    tk.func = const_cast<void*>(query ? f->ks->query_ragged : f->ks->insert_ragged);
     tk.gridDim = dim3(ragged_grid(f, query, p.n_tiles, ctas));
     tk.blockDim = dim3(kThreads);
     tk.sharedMemBytes = f->ks->smem(query);

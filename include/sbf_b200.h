@@ -157,6 +157,13 @@ int sbf_filter_clear(sbf_filter_t* filter, sbf_stream_t stream);
 uint64_t sbf_filter_bits(const sbf_filter_t* filter);
 /* Number of 256-bit shards (filter.cuh:831-833). */
 uint64_t sbf_filter_num_shards(const sbf_filter_t* filter);
+/* Which kernels a filter runs (no reference counterpart; the reference
+ * compiles every Config into the caller): 0 = tile kernels compiled into the
+ * library, 1 = the same tile kernels compiled at run time for this
+ * configuration (NVRTC, cached under $SBF_JIT_CACHE, off with SBF_JIT=0),
+ * 2 = runtime-parameterised kernels (other alphabets, or when run-time
+ * compilation is off or fails).  All three give identical results. */
+int sbf_filter_kernel_path(const sbf_filter_t* filter);
 /* Device pointer to the shard words: num_shards * 4 little-endian uint64
  * words, shard i at words [4i, 4i+4) (filter.cuh:137-142, filter_ref). */
 int sbf_filter_words(const sbf_filter_t* filter, uint64_t** d_words, uint64_t* n_words);

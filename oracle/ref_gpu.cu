@@ -18,6 +18,9 @@ using C5 = cusbf::Config<5, 4, 3, 4>;
 using C31H8 = cusbf::Config<31, 28, 16, 8>;
 using C31H16 = cusbf::Config<31, 28, 16, 16>;
 using C21 = cusbf::Config<21, 19, 11, 4>;
+using C31M21 = cusbf::Config<31, 28, 21, 4>;                       // 7
+using C25 = cusbf::Config<25, 22, 13, 4>;                          // 8
+using CP12 = cusbf::Config<12, 10, 6, 4, 256, cusbf::ProteinAlphabet>;  // 9
 
 struct Handle {
     int cfg;
@@ -47,8 +50,13 @@ SBF_REF_SHARDS(Shards5, C5)
 SBF_REF_SHARDS(Shards31H8, C31H8)
 SBF_REF_SHARDS(Shards31H16, C31H16)
 SBF_REF_SHARDS(Shards21, C21)
+SBF_REF_SHARDS(Shards31M21, C31M21)
+SBF_REF_SHARDS(Shards25, C25)
+SBF_REF_SHARDS(ShardsP12, CP12)
 
-// Configuration ids as in oracle/oracle.py REF_CONFIGS (DNA alphabet only).
+// Configuration ids: 0-6 as in oracle/oracle.py REF_CONFIGS; 7-9 extra
+// configurations (a long minimizer, one with no specialised engine kernel,
+// and a protein alphabet).
 template <typename Fn>
 int with(Handle* h, Fn&& fn) {
     if (!h) return -1;
@@ -58,6 +66,9 @@ int with(Handle* h, Fn&& fn) {
         case 4: return fn(*static_cast<cusbf::filter<C31H8>*>(h->f));
         case 5: return fn(*static_cast<cusbf::filter<C31H16>*>(h->f));
         case 6: return fn(*static_cast<cusbf::filter<C21>*>(h->f));
+        case 7: return fn(*static_cast<cusbf::filter<C31M21>*>(h->f));
+        case 8: return fn(*static_cast<cusbf::filter<C25>*>(h->f));
+        case 9: return fn(*static_cast<cusbf::filter<CP12>*>(h->f));
         default: return -1;
     }
 }
@@ -73,6 +84,9 @@ void* sbf_refgpu_create(int cfg, uint64_t bits) {
             case 4: return new Handle{4, new cusbf::filter<C31H8>(bits)};
             case 5: return new Handle{5, new cusbf::filter<C31H16>(bits)};
             case 6: return new Handle{6, new cusbf::filter<C21>(bits)};
+            case 7: return new Handle{7, new cusbf::filter<C31M21>(bits)};
+            case 8: return new Handle{8, new cusbf::filter<C25>(bits)};
+            case 9: return new Handle{9, new cusbf::filter<CP12>(bits)};
             default: break;
         }
     } catch (...) {

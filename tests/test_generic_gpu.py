@@ -12,6 +12,13 @@ from conftest import random_dna
 
 pytestmark = pytest.mark.gpu
 
+
+@pytest.fixture(autouse=True)
+def _generic_kernels(monkeypatch):
+    """DNA configurations would otherwise run tile kernels compiled at run
+    time (tests/test_jit_gpu.py); here they exercise the generic kernels."""
+    monkeypatch.setenv("SBF_JIT", "0")
+
 DNA, TRIPLET, PROTEIN = 0, 1, 2
 AMINO = b"ACDEFGHIKLMNPQRSTVWYacdefghiklmnpqrstvwyBXZ"
 

@@ -137,6 +137,8 @@ def test_repeats_long_runs(sbf, cuda, oracle_mod):
     dict(k=31, s=30, m=16, hashes=4), dict(k=31, s=31, m=16, hashes=4),
     dict(k=31, s=28, m=16, hashes=8), dict(k=31, s=28, m=16, hashes=16),
     dict(k=21, s=19, m=11, hashes=4), dict(k=5, s=4, m=3, hashes=4), dict(k=3, s=2, m=2, hashes=4),
+    dict(k=31, s=28, m=21, hashes=4), dict(k=31, s=30, m=21, hashes=4),
+    dict(k=31, s=31, m=21, hashes=4),
 ])
 def test_other_configs(sbf, cuda, oracle_mod, cfg):
     rng = np.random.default_rng(cfg["k"] * 100 + cfg["hashes"] + cfg["s"])

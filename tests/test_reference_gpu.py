@@ -99,11 +99,21 @@ def test_large_single_launch(sbf, cuda, refgpu):
 @pytest.mark.parametrize("cfg_id,cfg", [(4, dict(k=31, s=28, m=16, hashes=8)),
                                         (5, dict(k=31, s=28, m=16, hashes=16)),
                                         (6, dict(k=21, s=19, m=11, hashes=4)),
-                                        (1, dict(k=5, s=4, m=3, hashes=4))])
+                                        (1, dict(k=5, s=4, m=3, hashes=4)),
+                                        (7, dict(k=31, s=28, m=21, hashes=4)),
+                                        (8, dict(k=25, s=22, m=13, hashes=4)),
+                                        (9, dict(k=12, s=10, m=6, hashes=4, alphabet=2))])
 def test_other_configs(sbf, cuda, refgpu, cfg_id, cfg):
+    """Specialised (4, 5, 6, 1, 7) and generic (8, and the protein alphabet 9)
+    engine kernels against the reference GPU path for that configuration."""
     torch = cuda
     rng = np.random.default_rng(cfg_id)
-    ins = random_dna(rng, 3_000_000, b"ACGTACGTACGTACGTACGTN")
-    qry = np.concatenate([ins[:1_000_000], random_dna(rng, 1_000_000)])
+    if cfg.get("alphabet") == 2:
+        a = np.frombuffer(b"ACDEFGHIKLMNPQRSTVWYacdefghiklmnpqrstvwy*X-", np.uint8)
+        ins = a[rng.integers(0, a.size, 3_000_000)]
+        qry = np.concatenate([ins[:1_000_000], a[rng.integers(0, a.size, 1_000_000)]])
+    else:
+        ins = random_dna(rng, 3_000_000, b"ACGTACGTACGTACGTACGTN")
+        qry = np.concatenate([ins[:1_000_000], random_dna(rng, 1_000_000)])
     _compare(sbf, torch, refgpu, cfg_id, cfg, 1 << 24, torch.from_numpy(ins).cuda(),
              torch.from_numpy(qry).cuda())
