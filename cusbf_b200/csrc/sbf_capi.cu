@@ -346,10 +346,11 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
         return set_error(SBF_ERR_INVALID_ARGUMENT,
                          "hash count %u must be 4, 8, 12 or 16 (a multiple of the 4 shard words)",
                          hashes);
-    // Specialised tile kernels for the compiled DNA configurations, the same
-    // kernels compiled at run time for other DNA configurations (below, once
-    // the device is known), and the runtime-parameterised kernels for the
-    // other alphabets or when run-time compilation is not possible.
+    // Specialised tile kernels for the compiled DNA configurations; for any
+    // other configuration, kernels compiled at run time (below, once the
+    // device is known: the tile kernels for DNA, the generic kernels with
+    // constant parameters for the other alphabets), or the
+    // runtime-parameterised kernels when run-time compilation is not possible.
     const KernelSet* ks = alphabet == SBF_ALPHABET_DNA
                               ? find_kernels(static_cast<int>(k), static_cast<int>(s),
                                              static_cast<int>(m), static_cast<int>(hashes))
@@ -375,16 +376,17 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
         if (e != cudaSuccess) { rc = cuda_fail(e, "cudaGetDevice"); break; }
         e = cudaDeviceGetAttribute(&f->sms, cudaDevAttrMultiProcessorCount, f->device);
         if (e != cudaSuccess) { rc = cuda_fail(e, "cudaDeviceGetAttribute"); break; }
-        if (!ks && alphabet == SBF_ALPHABET_DNA)
+        if (!ks)
             ks = jit_kernels(static_cast<int>(k), static_cast<int>(s), static_cast<int>(m),
-                             static_cast<int>(hashes), f->device);
+                             static_cast<int>(hashes), alphabet, f->device);
         if (!ks) ks = generic_kernels();
         f->ks = ks;
         const void* fns[6] = {ks->insert_bytes, ks->query_bytes, ks->insert_dense,
                               ks->query_dense, ks->insert_ragged, ks->query_ragged};
-        // Run-time compiled kernels have their attributes set when loaded and
-        // run two CTAs per SM, as their shared memory allows.
-        for (int i = 0; i < 6 && ks->jit; ++i) f->occupancy[i] = 2;
+        // Run-time compiled kernels have their attributes set when loaded;
+        // their occupancy is the set's (two CTAs per SM for the tile
+        // kernels, as their shared memory allows).
+        for (int i = 0; i < 6 && ks->jit; ++i) f->occupancy[i] = ks->jit_occupancy;
         for (int i = 0; i < 6 && rc == SBF_OK && !ks->jit; ++i) {
             // Query kernels: shard slots; insert kernels: flush staging ring.
             const int dyn = ks->smem((i & 1) != 0);

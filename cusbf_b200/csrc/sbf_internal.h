@@ -91,7 +91,8 @@ struct KernelSet {
     // kernels' flush ring and shard slots; none for the generic kernels.
     int smem_insert = kInsertSlotBytes;
     int smem_query = kQuerySlotBytes;
-    bool jit = false;  // loaded from a run-time compiled library
+    bool jit = false;    // loaded from a run-time compiled library
+    int jit_occupancy = 2;  // resident CTAs per SM assumed for run-time compiled sets
     int smem(bool query) const { return query ? smem_query : smem_insert; }
 };
 
@@ -110,9 +111,11 @@ cudaError_t launch_tile_records(const DevRange* ranges, uint64_t n_ranges, int64
                                 uint64_t n_tiles, uint32_t* tile_rec, cudaStream_t stream);
 cudaError_t launch_popcount(const uint64_t* words, uint64_t n_words, unsigned long long* out,
                             cudaStream_t stream);
-// Tile kernels compiled at run time for a DNA configuration that is not
-// compiled into the library (sbf_jit.cpp); nullptr when that is not possible.
-const KernelSet* jit_kernels(int k, int s, int m, int h, int device);
+// Kernels compiled at run time for a configuration that is not compiled into
+// the library (sbf_jit.cpp): the tile kernels for DNA, the generic kernels
+// with the configuration as constants for the other alphabets; nullptr when
+// that is not possible.
+const KernelSet* jit_kernels(int k, int s, int m, int h, int alphabet, int device);
 // Launches one of a KernelSet's kernels.
 cudaError_t launch_set_kernel(const KernelSet* ks, const void* fn, unsigned grid, bool query,
                               const TileParams& p, cudaStream_t stream);

@@ -1,5 +1,5 @@
-// sbf_jit.cpp -- tile kernels for DNA configurations that are not compiled
-// into the library.  The reference is header-only, so every Config<K,S,M,H>
+// sbf_jit.cpp -- kernels for configurations that are not compiled into the
+// library.  The reference is header-only, so every Config<K,S,M,H>
 // a caller names gets kernels specialised at compile time.  A prebuilt
 // library can only hold a few, so for any other configuration the same tile
 // kernel source (sbf_tile.cuh and its two headers, embedded in the library
@@ -10,8 +10,10 @@
 // Compilation takes about ten seconds, so the cubin is cached on disk under
 // $SBF_JIT_CACHE (default ~/.cache/sbf_b200), keyed by the configuration, the
 // device architecture, the NVRTC version and a hash of the embedded source.
-// SBF_JIT=0 turns this off; then, and on any failure, the filter runs the
-// runtime-parameterised kernels (sbf_generic.cu), which give the same
+// The protein and DNA-triplet alphabets get the generic kernels
+// (sbf_generic.cuh) compiled the same way with the configuration as template
+// constants.  SBF_JIT=0 turns this off; then, and on any failure, the filter
+// runs the runtime-parameterised generic kernels, which give the same
 // results more slowly.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
@@ -37,12 +39,13 @@
 #include "../../include/sbf_b200.h"
 #include "sbf_host.h"
 #include "sbf_internal.h"
-#include "sbf_jit_sources.inc"  // kJitInternal, kJitDevice, kJitTile (generated)
+#include "sbf_jit_sources.inc"  // kJitInternal, kJitDevice, kJitTile, kJitGeneric (generated)
 
 namespace sbf {
 namespace {
 
-// Fixed-width integer types for NVRTC, which has no <cstdint>.
+// Fixed-width integer types for NVRTC, which has no <cstdint>, then the
+// kernel header.
 const char kPrelude[] =
     "typedef unsigned char uint8_t;\n"
     "typedef unsigned short uint16_t;\n"
@@ -51,8 +54,7 @@ const char kPrelude[] =
     "typedef signed char int8_t;\n"
     "typedef short int16_t;\n"
     "typedef int int32_t;\n"
-    "typedef long long int64_t;\n"
-    "#include \"sbf_tile.cuh\"\n";
+    "typedef long long int64_t;\n";
 
 // NVRTC is opened by path ($SBF_NVRTC_PATH, else the CUDA toolkit this
 // library was built with) into its own namespace: a process may already hold
@@ -137,25 +139,40 @@ struct Compiled {
     std::vector<char> cubin;
 };
 
-std::string name_expr(int k, int s, int m, int h, int v) {
-    char buf[160];
-    std::snprintf(buf, sizeof buf, "&sbf::tile_kernel<sbf::Cfg<%d, %d, %d, %d>, %s, %s, %s>", k, s,
-                  m, h, kVariants[v][0] ? "true" : "false", kVariants[v][1] ? "true" : "false",
-                  kVariants[v][2] ? "true" : "false");
+// One configuration to compile: DNA gets the tile kernels, other alphabets
+// the generic kernels with the configuration as template constants.
+struct JitConfig {
+    int k, s, m, h, alphabet;
+    uint32_t bits, width;
+    bool tile() const { return alphabet == SBF_ALPHABET_DNA; }
+};
+
+std::string name_expr(const JitConfig& c, int v) {
+    char cfg[96], buf[192];
+    if (c.tile())
+        std::snprintf(cfg, sizeof cfg, "sbf::tile_kernel<sbf::Cfg<%d, %d, %d, %d>", c.k, c.s, c.m,
+                      c.h);
+    else
+        std::snprintf(cfg, sizeof cfg, "sbf::generic_kernel<sbf::FixedGen<%d, %d, %d, %d, %u, %u, %d>",
+                      c.k, c.s, c.m, c.h, c.bits, c.width, c.alphabet);
+    std::snprintf(buf, sizeof buf, "&%s, %s, %s, %s>", cfg, kVariants[v][0] ? "true" : "false",
+                  kVariants[v][1] ? "true" : "false", kVariants[v][2] ? "true" : "false");
     return buf;
 }
 
-bool compile(int k, int s, int m, int h, const std::string& arch, Compiled* out) {
+bool compile(const JitConfig& c, const std::string& arch, Compiled* out) {
     const Nvrtc& nv = nvrtc();
     if (!nv.ok) return false;
-    const char* headers[] = {kJitInternal, kJitDevice, kJitTile};
-    const char* names[] = {"sbf_internal.h", "sbf_device.cuh", "sbf_tile.cuh"};
+    const char* headers[] = {kJitInternal, kJitDevice, kJitTile, kJitGeneric};
+    const char* names[] = {"sbf_internal.h", "sbf_device.cuh", "sbf_tile.cuh", "sbf_generic.cuh"};
+    const std::string src = std::string(kPrelude) +
+                            (c.tile() ? "#include \"sbf_tile.cuh\"\n" : "#include \"sbf_generic.cuh\"\n");
     nvrtcProgram prog;
-    if (nv.create(&prog, kPrelude, "sbf_jit.cu", 3, headers, names) != NVRTC_SUCCESS)
+    if (nv.create(&prog, src.c_str(), "sbf_jit.cu", 4, headers, names) != NVRTC_SUCCESS)
         return false;
     std::vector<std::string> exprs;
     for (int v = 0; v < 6; ++v) {
-        exprs.push_back(name_expr(k, s, m, h, v));
+        exprs.push_back(name_expr(c, v));
         nv.add_name(prog, exprs.back().c_str());
     }
     const std::string arch_opt = "-arch=" + arch;
@@ -226,13 +243,15 @@ struct JitEntry {
 };
 
 std::mutex g_mu;
-std::map<std::tuple<int, int, int, int>, std::unique_ptr<JitEntry>> g_sets;
-std::set<std::tuple<int, int, int, int>> g_failed;
+std::map<std::tuple<int, int, int, int, int>, std::unique_ptr<JitEntry>> g_sets;
+std::set<std::tuple<int, int, int, int, int>> g_failed;
 
 }  // namespace
 
-const KernelSet* jit_kernels(int k, int s, int m, int h, int device) {
+const KernelSet* jit_kernels(int k, int s, int m, int h, int alphabet, int device) {
     if (!jit_enabled()) return nullptr;
+    JitConfig jc{k, s, m, h, alphabet, 0, 0};
+    if (!alphabet_geometry(alphabet, &jc.bits, &jc.width)) return nullptr;
     int major = 0, minor = 0;
     if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess ||
         cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device) != cudaSuccess) {
@@ -240,7 +259,7 @@ const KernelSet* jit_kernels(int k, int s, int m, int h, int device) {
         return nullptr;
     }
     if (major != 10 || minor != 0) return nullptr;  // the library targets sm_100a
-    const auto key = std::make_tuple(k, s, m, h);
+    const auto key = std::make_tuple(k, s, m, h, alphabet);
     std::lock_guard<std::mutex> lk(g_mu);
     if (g_failed.count(key)) return nullptr;
     auto it = g_sets.find(key);
@@ -249,20 +268,21 @@ const KernelSet* jit_kernels(int k, int s, int m, int h, int device) {
         int nv_major = 0, nv_minor = 0;
         if (nvrtc().ok) nvrtc().version(&nv_major, &nv_minor);
         uint64_t hash = 0xcbf29ce484222325ULL;
-        for (const char* src : {kJitInternal, kJitDevice, kJitTile, kPrelude})
+        for (const char* src : {kJitInternal, kJitDevice, kJitTile, kJitGeneric, kPrelude})
             hash = fnv1a(hash, src, std::strlen(src));
-        const int meta[] = {k, s, m, h, nv_major, nv_minor};
+        const int meta[] = {k, s, m, h, alphabet, nv_major, nv_minor};
         hash = fnv1a(hash, meta, sizeof meta);
         hash = fnv1a(hash, arch.data(), arch.size());
         char file[128];
-        std::snprintf(file, sizeof file, "tile_k%d_s%d_m%d_h%d_%016llx.bin", k, s, m, h,
+        std::snprintf(file, sizeof file, "%s_k%d_s%d_m%d_h%d_a%d_%016llx.bin",
+                      jc.tile() ? "tile" : "generic", k, s, m, h, alphabet,
                       static_cast<unsigned long long>(hash));
         const std::string dir = cache_dir();
         const std::string path = dir + "/" + file;
         Compiled c;
         if (!read_cache(path, &c)) {
             c = Compiled{};
-            if (!compile(k, s, m, h, arch, &c)) {
+            if (!compile(jc, arch, &c)) {
                 g_failed.insert(key);
                 return nullptr;
             }
@@ -288,6 +308,12 @@ const KernelSet* jit_kernels(int k, int s, int m, int h, int device) {
         }
         e->ks = KernelSet{k, s, m, h, fns[0], fns[1], fns[2], fns[3], fns[4], fns[5]};
         e->ks.jit = true;
+        if (!jc.tile()) {
+            // The generic kernels use no dynamic shared memory and few
+            // registers.
+            e->ks.smem_insert = e->ks.smem_query = 0;
+            e->ks.jit_occupancy = 4;
+        }
         it = g_sets.emplace(key, std::move(e)).first;
     }
     JitEntry& e = *it->second;
@@ -296,6 +322,7 @@ const KernelSet* jit_kernels(int k, int s, int m, int h, int device) {
                               e.ks.query_dense,  e.ks.insert_ragged, e.ks.query_ragged};
         for (int v = 0; v < 6; ++v) {
             const int dyn = e.ks.smem(kVariants[v][0]);
+            if (dyn == 0) continue;
             if (cudaKernelSetAttributeForDevice(
                     reinterpret_cast<cudaKernel_t>(const_cast<void*>(fns[v])),
                     cudaFuncAttributeMaxDynamicSharedMemorySize, dyn, device) != cudaSuccess) {

@@ -145,3 +145,43 @@ print(f.kernel_path())
                        timeout=300)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip().splitlines()[-1] == "1", r.stdout + r.stderr
+
+
+ALPHA_CONFIGS = [dict(k=12, s=10, m=6, hashes=4, alphabet=2), dict(k=5, s=4, m=3, hashes=8, alphabet=2),
+                 dict(k=10, s=8, m=5, hashes=16, alphabet=1), dict(k=3, s=2, m=2, hashes=4, alphabet=1)]
+
+
+@pytest.mark.parametrize("cfg", ALPHA_CONFIGS, ids=["prot12", "prot5h8", "trip10h16", "trip3"])
+def test_runtime_compiled_alphabets_match_oracle(sbf, cuda, oracle_mod, jit_cache, cfg):
+    """Protein and DNA-triplet configurations run the generic kernels compiled
+    with the configuration as constants."""
+    rng = np.random.default_rng(cfg["k"] * 3 + cfg["alphabet"])
+    if cfg["alphabet"] == 2:
+        a = np.frombuffer(b"ACDEFGHIKLMNPQRSTVWYacdefghiklmnpqrstvwy*X-", np.uint8)
+        ins = a[rng.integers(0, a.size, 150_000)]
+        qry = np.concatenate([ins[:40_000], a[rng.integers(0, a.size, 40_000)]])
+        width = 1
+    else:
+        ins = random_dna(rng, 150_001, b"ACGTACGTACGTacgtN")
+        qry = np.concatenate([ins[:60_000], random_dna(rng, 60_000)])
+        width = 3
+    bits = 1 << 17
+    o = oracle_mod.Oracle(**cfg)
+    w = o.new_words(bits)
+    o.insert(w, ins)
+    want = o.contains(w, qry)
+    f = sbf.Filter(bits, **cfg)
+    assert f.kernel_path() == sbf.Filter.KERNELS_RUNTIME_COMPILED
+    f.insert_sequence(ins)
+    np.testing.assert_array_equal(f.words_host(), w)
+    np.testing.assert_array_equal(f.contains_sequence(qry), want)
+    packed = sbf.pack_dense_sequence(qry, alphabet=cfg["alphabet"])
+    n_sym = qry.size // width
+    np.testing.assert_array_equal(f.contains_dense_packed(packed, n_sym),
+                                  o.contains_dense(w, packed, n_sym))
+    # record batches (symbol-aligned ranges) with per-record counts
+    ranges = [(i * 30 * width, 25 * width) for i in range(qry.size // (30 * width))]
+    recs = []
+    f.query_record_batch(qry, ranges, consume=recs.append)
+    for (off, n), r in zip(ranges, recs):
+        np.testing.assert_array_equal(r["hits"], o.contains(w, qry[off:off + n]))
