@@ -39,7 +39,8 @@ def _stale(target: str, deps: list[str]) -> bool:
 
 # The tile kernel source, embedded for run-time compilation (sbf_jit.cpp).
 JIT_SOURCES = [("kJitInternal", "sbf_internal.h"), ("kJitDevice", "sbf_device.cuh"),
-               ("kJitTile", "sbf_tile.cuh"), ("kJitGeneric", "sbf_generic.cuh")]
+               ("kJitFlush", "sbf_flush.cuh"), ("kJitTile", "sbf_tile.cuh"),
+               ("kJitGeneric", "sbf_generic.cuh")]
 
 
 def write_jit_sources(objdir: str) -> None:

@@ -386,7 +386,11 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
         // Run-time compiled kernels have their attributes set when loaded;
         // their occupancy is the set's (two CTAs per SM for the tile
         // kernels, as their shared memory allows).
-        for (int i = 0; i < 6 && ks->jit; ++i) f->occupancy[i] = ks->jit_occupancy;
+        for (int i = 0; i < 6 && ks->jit; ++i) {
+            const int dyn = ks->smem((i & 1) != 0);
+            f->occupancy[i] = dyn ? std::min(ks->jit_occupancy, (227 << 10) / dyn)
+                                  : ks->jit_occupancy;
+        }
         for (int i = 0; i < 6 && rc == SBF_OK && !ks->jit; ++i) {
             // Query kernels: shard slots; insert kernels: flush staging ring.
             const int dyn = ks->smem((i & 1) != 0);

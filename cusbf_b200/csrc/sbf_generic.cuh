@@ -25,6 +25,7 @@
 #pragma once
 
 #include "sbf_device.cuh"
+#include "sbf_flush.cuh"
 #include "sbf_internal.h"
 
 namespace sbf {
@@ -105,11 +106,16 @@ __device__ __forceinline__ uint32_t eval_kmer(const GenericCfg& c, uint32_t shar
 // The configuration comes from the launch (RuntimeGen, one build for every
 // configuration) or from template constants (FixedGen, compiled at run time
 // for one configuration so loops unroll and shifts are constants).
+// FixedGen inserts flush each run with one 32-byte bulk OR-reduction from
+// the flush ring in the launch's dynamic shared memory; RuntimeGen launches
+// have none and use four 8-byte atomics.
 struct RuntimeGen {
+    static constexpr bool kBulkFlush = false;
     __device__ __forceinline__ static GenericCfg get(const TileParams& p) { return p.gen; }
 };
 template <int K, int S, int M, int H, int Bits, int Width, int Alphabet>
 struct FixedGen {
+    static constexpr bool kBulkFlush = true;
     __device__ __forceinline__ static GenericCfg get(const TileParams&) {
         return GenericCfg{K, S, M, H, Bits, Width, Alphabet};
     }
@@ -118,6 +124,9 @@ struct FixedGen {
 template <class G, bool kQuery, bool kDense, bool kRagged>
 __global__ void __launch_bounds__(kThreads) generic_kernel(TileParams p) {
     const GenericCfg c = G::get(p);
+    extern __shared__ __align__(16) uint64_t flush_slots[];
+    FlushRing ring{flush_slots + 4 * threadIdx.x, 0u};
+    (void)ring;
     const uint64_t n = p.n_kmers;
     const uint64_t n_strips = (n + kStrip - 1) / kStrip;
     const uint64_t km_mask = low_mask(c.k * c.bits);
@@ -166,12 +175,16 @@ __global__ void __launch_bounds__(kThreads) generic_kernel(TileParams p) {
             }
             rv = rp = 0;
         };
-        auto flush_run = [&]() {
+        auto flush_run_now = [&]() {
             if (!kQuery && in_run) {
-                uint64_t* dst = p.words + static_cast<uint64_t>(run_shard) * 4;
+                if constexpr (G::kBulkFlush) {
+                    flush_run(p.words, run_shard, acc, ring);
+                } else {
+                    uint64_t* dst = p.words + static_cast<uint64_t>(run_shard) * 4;
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    if (acc[i]) atomicOr(reinterpret_cast<unsigned long long*>(dst + i), acc[i]);
+                    for (int i = 0; i < 4; ++i)
+                        if (acc[i]) atomicOr(reinterpret_cast<unsigned long long*>(dst + i), acc[i]);
+                }
             }
         };
         for (uint64_t w = w0; w < w_end; ++w) {
@@ -202,7 +215,7 @@ __global__ void __launch_bounds__(kThreads) generic_kernel(TileParams p) {
                           ((words[2] & m[2]) == m[2]) && ((words[3] & m[3]) == m[3]);
                 } else {
                     if (!in_run || shard != run_shard) {
-                        flush_run();
+                        flush_run_now();
                         run_shard = shard;
                         in_run = true;
                         acc[0] = acc[1] = acc[2] = acc[3] = 0;
@@ -228,12 +241,13 @@ __global__ void __launch_bounds__(kThreads) generic_kernel(TileParams p) {
                 hits |= static_cast<uint32_t>(hit) << (w - w0);
             }
         }
-        flush_run();
+        flush_run_now();
         if constexpr (kRagged) flush_record();
         if constexpr (kQuery) {
             if (p.out_bits) p.out_bits[w0 / kStrip] = hits;
         }
     }
+    if constexpr (!kQuery && G::kBulkFlush) flush_ring_drain();
     if constexpr (kRagged) {
         if (p.counts) {
 #pragma unroll

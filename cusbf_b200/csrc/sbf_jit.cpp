@@ -39,7 +39,7 @@
 #include "../../include/sbf_b200.h"
 #include "sbf_host.h"
 #include "sbf_internal.h"
-#include "sbf_jit_sources.inc"  // kJitInternal, kJitDevice, kJitTile, kJitGeneric (generated)
+#include "sbf_jit_sources.inc"  // kJit* kernel sources (generated)
 
 namespace sbf {
 namespace {
@@ -163,12 +163,13 @@ std::string name_expr(const JitConfig& c, int v) {
 bool compile(const JitConfig& c, const std::string& arch, Compiled* out) {
     const Nvrtc& nv = nvrtc();
     if (!nv.ok) return false;
-    const char* headers[] = {kJitInternal, kJitDevice, kJitTile, kJitGeneric};
-    const char* names[] = {"sbf_internal.h", "sbf_device.cuh", "sbf_tile.cuh", "sbf_generic.cuh"};
+    const char* headers[] = {kJitInternal, kJitDevice, kJitFlush, kJitTile, kJitGeneric};
+    const char* names[] = {"sbf_internal.h", "sbf_device.cuh", "sbf_flush.cuh", "sbf_tile.cuh",
+                           "sbf_generic.cuh"};
     const std::string src = std::string(kPrelude) +
                             (c.tile() ? "#include \"sbf_tile.cuh\"\n" : "#include \"sbf_generic.cuh\"\n");
     nvrtcProgram prog;
-    if (nv.create(&prog, src.c_str(), "sbf_jit.cu", 4, headers, names) != NVRTC_SUCCESS)
+    if (nv.create(&prog, src.c_str(), "sbf_jit.cu", 5, headers, names) != NVRTC_SUCCESS)
         return false;
     std::vector<std::string> exprs;
     for (int v = 0; v < 6; ++v) {
@@ -268,7 +269,7 @@ const KernelSet* jit_kernels(int k, int s, int m, int h, int alphabet, int devic
         int nv_major = 0, nv_minor = 0;
         if (nvrtc().ok) nvrtc().version(&nv_major, &nv_minor);
         uint64_t hash = 0xcbf29ce484222325ULL;
-        for (const char* src : {kJitInternal, kJitDevice, kJitTile, kJitGeneric, kPrelude})
+        for (const char* src : {kJitInternal, kJitDevice, kJitFlush, kJitTile, kJitGeneric, kPrelude})
             hash = fnv1a(hash, src, std::strlen(src));
         const int meta[] = {k, s, m, h, alphabet, nv_major, nv_minor};
         hash = fnv1a(hash, meta, sizeof meta);
@@ -309,9 +310,9 @@ const KernelSet* jit_kernels(int k, int s, int m, int h, int alphabet, int devic
         e->ks = KernelSet{k, s, m, h, fns[0], fns[1], fns[2], fns[3], fns[4], fns[5]};
         e->ks.jit = true;
         if (!jc.tile()) {
-            // The generic kernels use no dynamic shared memory and few
-            // registers.
-            e->ks.smem_insert = e->ks.smem_query = 0;
+            // The generic kernels use few registers; inserts take the flush
+            // ring's dynamic shared memory, queries none.
+            e->ks.smem_query = 0;
             e->ks.jit_occupancy = 4;
         }
         it = g_sets.emplace(key, std::move(e)).first;

@@ -36,6 +36,7 @@
 #pragma once
 
 #include "sbf_device.cuh"
+#include "sbf_flush.cuh"
 #include "sbf_internal.h"
 
 namespace sbf {
@@ -278,39 +279,6 @@ __device__ __forceinline__ void smer_masks(const uint32_t* c, int r, uint64_t m[
     m[0] = m[1] = m[2] = m[3] = 0;
 #pragma unroll
     for (int j = 0; j < C::H; ++j) m[j & 3] |= uint64_t{1} << bit_address<C::H>(h, j);
-}
-
-// A run's four word masks are merged into its shard with one 32-byte TMA
-// bulk reduction (cp.reduce.async.bulk .or.b64) from a shared-memory staging
-// slot: one L2 sector operation instead of four 8-byte atomics.  Each thread
-// cycles through kFlushSlots slots; before reusing a slot it waits until the
-// bulk operation issued kFlushSlots flushes earlier has read it.
-struct FlushRing {
-    uint64_t* slot0;  // this thread's slot 0; slot k at slot0 + k * kThreads * 4
-    uint32_t count;
-};
-
-__device__ __forceinline__ void flush_run(uint64_t* words, uint32_t shard, const uint64_t a[4],
-                                          FlushRing& ring) {
-    static_assert(kFlushSlots == 8, "wait_group.read immediate below assumes 8 slots");
-    uint64_t* slot = ring.slot0 + (ring.count & (kFlushSlots - 1)) * (kThreads * 4);
-    asm volatile("cp.async.bulk.wait_group.read 7;" ::: "memory");
-    *reinterpret_cast<ulonglong2*>(slot) = make_ulonglong2(a[0], a[1]);
-    *reinterpret_cast<ulonglong2*>(slot + 2) = make_ulonglong2(a[2], a[3]);
-    fence_proxy_async_smem();
-    asm volatile(
-        "cp.reduce.async.bulk.global.shared::cta.bulk_group.or.b64 [%0], [%1], 32;" ::"l"(
-            words + static_cast<uint64_t>(shard) * 4),
-        "r"(smem_addr(slot))
-        : "memory");
-    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-    ++ring.count;
-}
-
-__device__ __forceinline__ void flush_ring_drain() {
-    // Every bulk reduction issued by this thread has completed (its global
-    // writes performed and its shared-memory slot read).
-    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
 // Insert: the mask of window j is T_j = OR of the one-hot masks of its F
