@@ -404,7 +404,7 @@ def run_ragged(args, world: int, rank: int, local_rank: int) -> None:
         pf.close()
 
     # End to end through the host API: pinned inputs and outputs.
-    e2e = e2e_tuned = rb = None
+    e2e = e2e_tuned = e2e_bits = rb = None
     if not args.no_e2e:
         h_genome = torch.from_numpy(genome).pin_memory().numpy()
         h_reads_t = torch.empty(d_reads.numel(), dtype=torch.uint8).pin_memory()
@@ -448,6 +448,24 @@ def run_ragged(args, world: int, rank: int, local_rank: int) -> None:
             w2 = time.perf_counter()
             res.append(((w1 - w0) * 1e3, (w2 - w1) * 1e3))
         e2e_tuned = e2e_obj(res, {"insert": ti.as_dict(), "query": tq.as_dict()})
+        # The same step with bit-packed query results (an eighth of the download).
+        h_bits = torch.empty(max((n_out + 31) // 32, 1), dtype=torch.int32).pin_memory().numpy()
+        res = []
+        for _ in range(max(1, args.e2e_steps) + 1):
+            f.clear(stream)
+            torch.cuda.synchronize(dev)
+            w0 = time.perf_counter()
+            f.ragged_insert(h_genome, g_ranges, tuning=ti, stream=stream)
+            w1 = time.perf_counter()
+            _, rqb = f.ragged_query_bits(h_reads, r_ranges, out=h_bits.view(np.uint32), tuning=tq,
+                                         stream=stream)
+            w2 = time.perf_counter()
+            assert rqb.positive_kmers == q_pos
+            res.append(((w1 - w0) * 1e3, (w2 - w1) * 1e3))
+        e2e_bits = e2e_obj(res[1:], {"insert": ti.as_dict(), "query": tq.as_dict()})
+        e2e_bits["d2h_bytes_per_step"] = int(4 * ((n_out + 31) // 32))
+        e2e_bits["api"] = ("sbf_ragged_insert + sbf_ragged_query_bits (host buffers, pinned; "
+                           "one result bit per window)")
         # The reference's single-launch record batch (host normalisation with
         # separators, one plain launch), insert and aggregate query.
         if not args.no_baselines:
@@ -506,6 +524,7 @@ def run_ragged(args, world: int, rank: int, local_rank: int) -> None:
         "record_batch_e2e": rb,
         "e2e": e2e,
         "e2e_tuned": e2e_tuned,
+        "e2e_bits": e2e_bits,
         "gpu_launches": 4 * args.steps,
         "clocks": clock_info,
     }
@@ -1148,6 +1167,7 @@ def summarize_ragged(d: dict) -> dict:
             "speedup_vs_plain_per_record": d.get("speedup_vs_plain"),
             "plain_hits_identical": pl.get("query_hits_identical_to_ragged"),
             "e2e_kmers_per_s": e2e.get("value"), "e2e_tuned_kmers_per_s": tuned.get("value"),
+            "e2e_bits_kmers_per_s": (d.get("e2e_bits") or {}).get("value"),
             "record_batch_e2e_kmers_per_s": rb.get("value")}
 
 

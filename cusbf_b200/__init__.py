@@ -251,6 +251,8 @@ _sig("sbf_ragged_insert", C.c_int, _vp, _vp, _u64, _vp, _u64, C.POINTER(RaggedTu
      C.POINTER(InsertReport))
 _sig("sbf_ragged_query", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, C.POINTER(RaggedTuning),
      _vp, C.POINTER(QueryReport))
+_sig("sbf_ragged_query_bits", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp, _u64, C.POINTER(RaggedTuning),
+     _vp, C.POINTER(QueryReport))
 _sig("sbf_ragged_autotune", C.c_int, _vp, C.c_int, _vp, _u64, _vp, _u64, _u64, _vp,
      C.POINTER(RaggedTuning))
 _sig("sbf_ragged_tuning_lookup", C.c_int, _vp, C.c_int, _u64, _u64, C.POINTER(RaggedTuning))
@@ -738,6 +740,22 @@ def _ragged_methods():
                                       _tuning(tuning), _stream(stream), C.byref(rep)))
         return rep
 
+    def ragged_query_bits(self, seq, ranges, out=None, tuning=None, stream=None):
+        """Returns (uint32 result words, QueryReport): window i -> bit i % 32
+        of word i // 32."""
+        b = _host_bytes(seq)
+        r = _ranges(ranges)
+        w = self.kmer_count(b.size)
+        nw = (w + 31) // 32
+        if out is None:
+            out = np.zeros(max(nw, 1), np.uint32)
+        o = out.numpy() if hasattr(out, "numpy") else out
+        rep = QueryReport()
+        _check(_lib.sbf_ragged_query_bits(self._h, _np_ptr(b), b.size, _np_ptr(r), r.shape[0],
+                                          _np_ptr(o), o.nbytes // 4, _tuning(tuning),
+                                          _stream(stream), C.byref(rep)))
+        return o[:nw], rep
+
     def ragged_query(self, seq, ranges, out=None, tuning=None, stream=None):
         """Returns (hits, QueryReport); `out` may be a preallocated host array
         (pinned for the fastest copies) of at least len - k + 1 bytes."""
@@ -769,7 +787,8 @@ def _ragged_methods():
         return t if st == OK else None
 
     for f in (ragged_insert_async, ragged_contains_async, ragged_contains_counts_async,
-              ragged_insert, ragged_query, ragged_autotune, ragged_tuning_lookup):
+              ragged_insert, ragged_query, ragged_query_bits, ragged_autotune,
+              ragged_tuning_lookup):
         setattr(Filter, f.__name__, f)
 
 

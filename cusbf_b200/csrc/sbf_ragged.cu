@@ -367,20 +367,28 @@ static int check_tuning(sbf_ragged_tuning& t) {
 // stages bytes [c*cw, c*cw + cw + K - 1) and the records clipped to them
 // (pieces shorter than K hold no window and are dropped: their bytes read as
 // outside every record, which invalidates exactly the windows that cross).
+// With h_bits, query results are bit-packed (window i -> bit i % 32 of word
+// i / 32) and chunks hold a multiple of 32 windows, so each chunk's result
+// words start on a word boundary.
 static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_t len,
                            const sbf_record_range* ranges, uint64_t n, sbf_ragged_tuning t,
-                           cudaStream_t st, uint8_t* h_out, unsigned long long counts[2]) {
+                           cudaStream_t st, uint8_t* h_out, unsigned long long counts[2],
+                           uint32_t* h_bits = nullptr) {
     counts[0] = counts[1] = 0;
+    const bool bits = h_bits != nullptr;
     const uint64_t K = f->k;
     const uint64_t W = f->kmers_of(len);
+    auto out_bytes = [&](uint64_t windows) { return bits ? (windows + 31) / 32 * 4 : windows; };
     if (W == 0 || n == 0) {
-        if (query && W) std::memset(h_out, 0, W);
+        if (query && W) std::memset(bits ? reinterpret_cast<uint8_t*>(h_bits) : h_out, 0,
+                                    out_bytes(W));
         return SBF_OK;
     }
     RaggedState* r = nullptr;
     SBF_TRY(ragged_state(f, &r));
     SBF_TRY(check_tuning(t));
-    const uint64_t cw = std::max<uint64_t>(t.chunk_bytes > K ? t.chunk_bytes - (K - 1) : 1, 1024);
+    uint64_t cw = std::max<uint64_t>(t.chunk_bytes > K ? t.chunk_bytes - (K - 1) : 1, 1024);
+    if (bits) cw = cw / 32 * 32;
     const uint64_t n_chunks = (W + cw - 1) / cw;
     const uint64_t max_bytes = cw + K - 1;
     const uint64_t max_pieces = max_bytes / K + 2;
@@ -395,7 +403,7 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
         SBF_TRY(grow_device(s.d_seq, s.d_seq_cap, max_bytes + 16));
         SBF_TRY(grow_device(s.d_rng, s.d_rng_cap, max_pieces * sizeof(DevRange)));
         SBF_TRY(grow_device(s.d_tile_rec, s.tile_cap, ((cw + 16) / kTileKmers + 2) * 4));
-        if (query) SBF_TRY(grow_device(s.d_out, s.out_cap, cw + 16));
+        if (query) SBF_TRY(grow_device(s.d_out, s.out_cap, out_bytes(cw) + 16));
         s.busy = false;
     }
     // The copy stream starts after work already queued on `st`.
@@ -432,14 +440,14 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
         SBF_CUDA(cudaStreamWaitEvent(st, s.ev_copied, 0));
         if (np) {
             const TileParams p = ragged_params(f, query, s.d_seq, b_hi - b_lo, s.d_rng, np,
-                                               s.d_tile_rec, s.d_out, r->d_ctl, d_counts);
+                                               s.d_tile_rec, s.d_out, r->d_ctl, d_counts, bits);
             if (t.use_graph)
                 SBF_TRY(ragged_graph_launch(f, s.graph[query ? 1 : 0], query, p, t.ctas_per_sm,
                                             st));
             else
                 SBF_TRY(ragged_launch(f, query, p, t.ctas_per_sm, st));
         } else if (query) {
-            SBF_CUDA(cudaMemsetAsync(s.d_out, 0, w_hi - w_lo, st));
+            SBF_CUDA(cudaMemsetAsync(s.d_out, 0, out_bytes(w_hi - w_lo), st));
         }
         // Downloads run on their own stream so the next chunk's kernel does
         // not queue behind this chunk's download.  The host waits for
@@ -448,7 +456,8 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
         if (query) {
             SBF_CUDA(cudaEventRecord(s.ev_kernel, st));
             SBF_CUDA(cudaStreamWaitEvent(r->d2h_stream, s.ev_kernel, 0));
-            SBF_CUDA(cudaMemcpyAsync(h_out + w_lo, s.d_out, w_hi - w_lo, cudaMemcpyDeviceToHost,
+            void* dst = bits ? static_cast<void*>(h_bits + w_lo / 32) : h_out + w_lo;
+            SBF_CUDA(cudaMemcpyAsync(dst, s.d_out, out_bytes(w_hi - w_lo), cudaMemcpyDeviceToHost,
                                      r->d2h_stream));
             SBF_CUDA(cudaEventRecord(s.ev_done, r->d2h_stream));
         } else {
@@ -595,6 +604,33 @@ extern "C" int sbf_ragged_query(const sbf_filter_t* cf, const char* h_seq, uint6
     SBF_TRY(resolve_tuning(f, true, len, n, tuning, &t));
     unsigned long long counts[2];
     SBF_TRY(ragged_pipeline(f, true, h_seq, len, ranges, n, t, S_(stream), h_out, counts));
+    if (report) {
+        report->records_queried = n;
+        report->queried_bases = 0;
+        for (uint64_t i = 0; i < n; ++i) report->queried_bases += ranges[i].sequence_bytes;
+        report->queried_kmers = counts[0];
+        report->positive_kmers = counts[1];
+    }
+    return SBF_OK;
+}
+
+extern "C" int sbf_ragged_query_bits(const sbf_filter_t* cf, const char* h_seq, uint64_t len,
+                                     const sbf_record_range* ranges, uint64_t n, uint32_t* h_bits,
+                                     uint64_t n_words, const sbf_ragged_tuning* tuning,
+                                     sbf_stream_t stream, sbf_query_report* report) {
+    auto* f = const_cast<sbf_filter*>(cf);
+    if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
+    SBF_TRY(f->require_byte_symbols("the ragged host pipeline"));
+    if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
+    SBF_TRY(validate_ranges(len, ranges, n));
+    const uint64_t W = f->kmers_of(len);
+    if (W && (!h_bits || n_words < (W + 31) / 32))
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "ragged query bit output span is too small");
+    sbf_ragged_tuning t{};
+    SBF_TRY(resolve_tuning(f, true, len, n, tuning, &t));
+    unsigned long long counts[2];
+    SBF_TRY(ragged_pipeline(f, true, h_seq, len, ranges, n, t, S_(stream), nullptr, counts,
+                            h_bits));
     if (report) {
         report->records_queried = n;
         report->queried_bases = 0;

@@ -399,6 +399,13 @@ int sbf_ragged_query(const sbf_filter_t* filter, const char* h_seq, uint64_t len
                      const sbf_record_range* ranges, uint64_t n, uint8_t* h_out,
                      uint64_t out_len, const sbf_ragged_tuning* tuning, sbf_stream_t stream,
                      sbf_query_report* report);
+/* sbf_ragged_query with bit-packed results (window i of the buffer -> bit
+ * i % 32 of h_bits[i / 32]; n_words >= ceil((len - k + 1) / 32)): an eighth
+ * of the download.  Chunks hold a multiple of 32 windows. */
+int sbf_ragged_query_bits(const sbf_filter_t* filter, const char* h_seq, uint64_t len,
+                          const sbf_record_range* ranges, uint64_t n, uint32_t* h_bits,
+                          uint64_t n_words, const sbf_ragged_tuning* tuning, sbf_stream_t stream,
+                          sbf_query_report* report);
 /* Times chunk size x stages x graph replay, then CTAs per SM for the
  * winner, on a prefix of the batch
  * (sample_bytes, 0 = 256 MiB), stores the fastest in the tuning table

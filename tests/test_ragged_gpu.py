@@ -181,3 +181,21 @@ def test_ragged_autotune_persists(sbf, cuda, oracle_mod, tmp_path, monkeypatch):
     hits, _ = f.ragged_query(seq, ranges)
     hits2, _ = f.ragged_query(seq, ranges, tuning=tq)
     np.testing.assert_array_equal(hits, hits2)
+
+
+@pytest.mark.parametrize("tuning", TUNINGS[:4], ids=["default", "4k-s1", "5000-s2-graph",
+                                                     "70k-s3-graph"])
+def test_ragged_query_bits_match_bytes(sbf, cuda, tuning):
+    """The bit-packed ragged query equals the byte query bit for bit, across
+    chunk boundaries (chunks hold a multiple of 32 windows)."""
+    rng = np.random.default_rng(77)
+    seq, ranges = _batch(rng, 400, 0, 3000)
+    f = sbf.Filter(1 << 20, **K31)
+    f.ragged_insert(seq, ranges[::3])
+    hits, rep = f.ragged_query(seq, ranges, tuning=tuning)
+    words, rep_b = f.ragged_query_bits(seq, ranges, tuning=tuning)
+    b = np.packbits(hits.astype(np.uint8), bitorder="little")
+    b = np.concatenate([b, np.zeros(words.size * 4 - b.size, np.uint8)])
+    np.testing.assert_array_equal(words, b.view(np.uint32))
+    assert rep_b.positive_kmers == rep.positive_kmers and rep_b.queried_kmers == rep.queried_kmers
+    assert rep.positive_kmers > 0
