@@ -363,10 +363,24 @@ static int check_tuning(sbf_ragged_tuning& t) {
 // Host pipeline
 // ---------------------------------------------------------------------------
 
+// Clips chunk-overlapping records to the chunk's bytes [b_lo, b_hi) and
+// rebases them to the chunk, in place.  Pieces shorter than K hold no window;
+// the windows that cross one span a record start or bytes outside every
+// record either way, so they stay invalid.
+__global__ void clip_ranges_kernel(DevRange* r, uint64_t n, uint64_t b_lo, uint64_t b_hi) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const DevRange x = r[i];
+        const uint64_t a = x.offset > b_lo ? x.offset : b_lo;
+        const uint64_t end = x.offset + x.bytes;
+        const uint64_t e = end < b_hi ? end : b_hi;
+        r[i] = DevRange{a - b_lo, e > a ? e - a : 0};
+    }
+}
+
 // Windows [0, W) of the batch are cut into chunks of `cw` windows; chunk c
-// stages bytes [c*cw, c*cw + cw + K - 1) and the records clipped to them
-// (pieces shorter than K hold no window and are dropped: their bytes read as
-// outside every record, which invalidates exactly the windows that cross).
+// stages bytes [c*cw, c*cw + cw + K - 1) and the records that overlap them,
+// copied as given (one memcpy of the slice) and clipped on the GPU.
 // With h_bits, query results are bit-packed (window i -> bit i % 32 of word
 // i / 32) and chunks hold a multiple of 32 windows, so each chunk's result
 // words start on a word boundary.
@@ -393,6 +407,7 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
     const uint64_t max_bytes = cw + K - 1;
     const uint64_t max_pieces = max_bytes / K + 2;
     const bool pinned_in = is_pinned(h_seq);
+    const bool pinned_rng = is_pinned(ranges);  // slices upload without a host copy
     unsigned long long* d_counts = ctl_counts(r);
     SBF_CUDA(cudaMemsetAsync(d_counts, 0, 2 * sizeof(unsigned long long), st));
     const uint32_t S = t.stages;
@@ -411,7 +426,8 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
     SBF_CUDA(cudaEventRecord(ev_start, st));
     SBF_CUDA(cudaStreamWaitEvent(r->copy_stream, ev_start, 0));
     SBF_CUDA(cudaStreamWaitEvent(r->d2h_stream, ev_start, 0));
-    uint64_t rec = 0;  // first record whose end exceeds the chunk's first byte
+    uint64_t rec = 0;      // first record whose end exceeds the chunk's first byte
+    uint64_t rec_end = 0;  // first record that starts at or after the chunk's end
     for (uint64_t c = 0; c < n_chunks; ++c) {
         RaggedSlot& s = r->slot[c % S];
         if (s.busy) SBF_CUDA(cudaEventSynchronize(s.ev_done));
@@ -419,12 +435,18 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
         const uint64_t w_hi = std::min<uint64_t>(W, w_lo + cw);
         const uint64_t b_lo = w_lo, b_hi = w_hi + K - 1;
         while (rec < n && ranges[rec].sequence_offset + ranges[rec].sequence_bytes <= b_lo) ++rec;
-        uint64_t np = 0;
-        for (uint64_t j = rec; j < n && ranges[j].sequence_offset < b_hi; ++j) {
-            const uint64_t a = std::max<uint64_t>(ranges[j].sequence_offset, b_lo);
-            const uint64_t e =
-                std::min<uint64_t>(ranges[j].sequence_offset + ranges[j].sequence_bytes, b_hi);
-            if (e >= a + K) s.pin_rng[np++] = DevRange{a - b_lo, e - a};
+        rec_end = std::max(rec_end, rec);
+        while (rec_end < n && ranges[rec_end].sequence_offset < b_hi) ++rec_end;
+        const uint64_t np = rec_end - rec;
+        if (np * sizeof(DevRange) > s.pin_rng_cap || np * sizeof(DevRange) > s.d_rng_cap) {
+            // Many records shorter than K in one chunk: grow with headroom.
+            SBF_TRY(grow_pinned(s.pin_rng, s.pin_rng_cap, 2 * np * sizeof(DevRange)));
+            SBF_TRY(grow_device(s.d_rng, s.d_rng_cap, 2 * np * sizeof(DevRange)));
+        }
+        const void* rng_src = ranges + rec;
+        if (np && !pinned_rng) {
+            std::memcpy(s.pin_rng, ranges + rec, np * sizeof(DevRange));
+            rng_src = s.pin_rng;
         }
         const uint8_t* src = reinterpret_cast<const uint8_t*>(h_seq) + b_lo;
         if (!pinned_in) {
@@ -434,11 +456,14 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
         SBF_CUDA(cudaMemcpyAsync(s.d_seq, src, b_hi - b_lo, cudaMemcpyHostToDevice,
                                  r->copy_stream));
         if (np)
-            SBF_CUDA(cudaMemcpyAsync(s.d_rng, s.pin_rng, np * sizeof(DevRange),
+            SBF_CUDA(cudaMemcpyAsync(s.d_rng, rng_src, np * sizeof(DevRange),
                                      cudaMemcpyHostToDevice, r->copy_stream));
         SBF_CUDA(cudaEventRecord(s.ev_copied, r->copy_stream));
         SBF_CUDA(cudaStreamWaitEvent(st, s.ev_copied, 0));
         if (np) {
+            const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((np + 255) / 256, 1024));
+            clip_ranges_kernel<<<blocks, 256, 0, st>>>(s.d_rng, np, b_lo, b_hi);
+            SBF_CUDA(cudaGetLastError());
             const TileParams p = ragged_params(f, query, s.d_seq, b_hi - b_lo, s.d_rng, np,
                                                s.d_tile_rec, s.d_out, r->d_ctl, d_counts, bits);
             if (t.use_graph)

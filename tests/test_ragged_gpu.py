@@ -199,3 +199,24 @@ def test_ragged_query_bits_match_bytes(sbf, cuda, tuning):
     np.testing.assert_array_equal(words, b.view(np.uint32))
     assert rep_b.positive_kmers == rep.positive_kmers and rep_b.queried_kmers == rep.queried_kmers
     assert rep.positive_kmers > 0
+
+
+def test_ragged_pinned_range_tables(sbf, cuda):
+    """Pinned record tables are uploaded slice by slice without a host copy;
+    results equal the pageable-table path."""
+    torch = cuda
+    rng = np.random.default_rng(81)
+    seq, ranges = _batch(rng, 600, 0, 400)
+    r = np.asarray(ranges, np.uint64)
+    pinned = torch.empty(r.shape, dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+    pinned[:] = r
+    small = dict(chunk_bytes=4096, stages=2, ctas_per_sm=0, use_graph=0)
+    a = sbf.Filter(1 << 20, **K31)
+    b = sbf.Filter(1 << 20, **K31)
+    a.ragged_insert(seq, r[::2], tuning=small)
+    b.ragged_insert(seq, np.ascontiguousarray(pinned[::2]), tuning=small)
+    np.testing.assert_array_equal(a.words_host(), b.words_host())
+    ha, ra = a.ragged_query(seq, r, tuning=small)
+    hb, rb = a.ragged_query(seq, pinned, tuning=small)
+    np.testing.assert_array_equal(ha, hb)
+    assert ra.positive_kmers == rb.positive_kmers > 0
