@@ -340,10 +340,13 @@ static void tune_store(const TuneKey& key, const sbf_ragged_tuning& t, double ms
     std::fclose(fp);
 }
 
-static sbf_ragged_tuning default_tuning() {
+// Defaults when no tuning-table entry matches: queries stage larger chunks,
+// three in flight (the shape the autotuner picks for read batches; their
+// uploads are the larger stream), inserts 64 MiB chunks, two in flight.
+static sbf_ragged_tuning default_tuning(bool query = false) {
     sbf_ragged_tuning t{};
-    t.chunk_bytes = uint64_t{64} << 20;
-    t.stages = 2;
+    t.chunk_bytes = query ? uint64_t{256} << 20 : uint64_t{64} << 20;
+    t.stages = query ? 3 : 2;
     t.ctas_per_sm = 0;
     t.use_graph = 0;
     return t;
@@ -507,7 +510,7 @@ static int resolve_tuning(const sbf_filter* f, bool query, uint64_t len, uint64_
     if (given) {
         *out = *given;
     } else if (!tune_lookup(tune_key(f, query, len, n), out)) {
-        *out = default_tuning();
+        *out = default_tuning(query);
     }
     return check_tuning(*out);
 }
@@ -670,7 +673,7 @@ extern "C" int sbf_ragged_tuning_lookup(const sbf_filter_t* f, int query, uint64
                                         uint64_t n, sbf_ragged_tuning* out) {
     if (!f || !out) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     if (tune_lookup(tune_key(f, query != 0, len, n), out)) return SBF_OK;
-    *out = default_tuning();
+    *out = default_tuning(query != 0);
     return set_error(SBF_ERR_INVALID_ARGUMENT, "no tuned entry for this shape (defaults returned)");
 }
 
@@ -686,14 +689,22 @@ extern "C" int sbf_ragged_autotune(sbf_filter_t* f, int query, const char* h_seq
     SBF_TRY(f->require_byte_symbols("the ragged host pipeline"));
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
     SBF_TRY(validate_ranges(len, ranges, n));
-    if (sample_bytes == 0) sample_bytes = uint64_t{256} << 20;
+    // Four of the largest candidate chunks, so the sample shows pipelining.
+    if (sample_bytes == 0) sample_bytes = uint64_t{1} << 30;
     const uint64_t sl = std::min<uint64_t>(len, sample_bytes);
     uint64_t sn = 0;
     while (sn < n && ranges[sn].sequence_offset < sl) ++sn;
     std::vector<sbf_record_range> sr(ranges, ranges + sn);
     if (sn && sr[sn - 1].sequence_offset + sr[sn - 1].sequence_bytes > sl)
         sr[sn - 1].sequence_bytes = sl - sr[sn - 1].sequence_offset;
-    std::vector<uint8_t> out(query ? std::max<uint64_t>(f->kmers_of(sl), 1) : 1);
+    // Pinned result buffer, as a streaming caller would use: downloads into
+    // pageable memory would slow every candidate and skew the choice.
+    PinnedBuf out;
+    struct Release {
+        PinnedBuf& b;
+        ~Release() { b.release(); }
+    } release_out{out};
+    SBF_TRY(out.ensure(query ? std::max<uint64_t>(f->kmers_of(sl), 1) : 1));
     const uint64_t chunks[] = {uint64_t{16} << 20, uint64_t{64} << 20, uint64_t{256} << 20};
     const uint32_t stage_opts[] = {2, 3};
     const uint32_t graph_opts[] = {0, 1};
@@ -705,7 +716,7 @@ extern "C" int sbf_ragged_autotune(sbf_filter_t* f, int query, const char* h_seq
         for (int rep = 0; rep < 2; ++rep) {  // the first run warms buffers and graphs
             const auto t0 = std::chrono::steady_clock::now();
             SBF_TRY(ragged_pipeline(f, query != 0, h_seq, sl, sr.data(), sn, t, S_(stream),
-                                    out.data(), counts));
+                                    static_cast<uint8_t*>(out.p), counts));
             const auto t1 = std::chrono::steady_clock::now();
             ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
         }

@@ -357,8 +357,9 @@ int sbf_record_batch_counts_noalloc(const sbf_filter_t* filter, const char* d_se
 
 /* Host pipeline knobs; zero fields take defaults. */
 typedef struct {
-    uint64_t chunk_bytes; /* bytes staged per chunk (default 64 MiB, min 4096) */
-    uint32_t stages;      /* chunks in flight, 1..4 (default 2) */
+    uint64_t chunk_bytes; /* bytes staged per chunk (default 64 MiB insert, 256 MiB
+                             query; min 4096) */
+    uint32_t stages;      /* chunks in flight, 1..4 (default 2 insert, 3 query) */
     uint32_t ctas_per_sm; /* resident CTAs per SM, 0 = occupancy limit */
     uint32_t use_graph;   /* replay each chunk's device work as a CUDA graph */
 } sbf_ragged_tuning;
@@ -408,7 +409,7 @@ int sbf_ragged_query_bits(const sbf_filter_t* filter, const char* h_seq, uint64_
                           sbf_query_report* report);
 /* Times chunk size x stages x graph replay, then CTAs per SM for the
  * winner, on a prefix of the batch
- * (sample_bytes, 0 = 256 MiB), stores the fastest in the tuning table
+ * (sample_bytes, 0 = 1 GiB), stores the fastest in the tuning table
  * (SBF_TUNE_TABLE, default $HOME/.cache/cusbf_b200/ragged_tuning.tsv) under
  * the batch's shape (operation, configuration, log2 bytes, log2 mean record
  * bytes) and returns it.  An insert tune inserts the prefix. */
