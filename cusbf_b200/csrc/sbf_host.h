@@ -116,6 +116,12 @@ struct sbf_filter {
 namespace sbf {
 void ragged_release(sbf_filter* f);
 void fastq_device_release(sbf_filter* f);
+// Checks that records are ordered, non-overlapping and inside [0, len)
+// (normalized_record_batch.hpp:123-147); large batches are checked on several
+// host threads.  `total_bytes`, when given, receives the sum of the record
+// lengths.
+int validate_ranges(uint64_t len, const sbf_record_range* r, uint64_t n,
+                    uint64_t* total_bytes = nullptr);
 // Host record batches without the symbol-alignment check of the public entry
 // points (FASTX chunks hold records of any length; normalisation pads each
 // to a symbol boundary).

@@ -22,7 +22,6 @@
 
 namespace sbf {
 
-int validate_ranges(uint64_t len, const sbf_record_range* r, uint64_t n);
 
 namespace {
 

@@ -49,7 +49,6 @@ static_assert(sizeof(DevRange) == sizeof(sbf_record_range), "record layout");
 
 namespace sbf {
 
-int validate_ranges(uint64_t len, const sbf_record_range* r, uint64_t n);
 const void* tile_records_kernel_ptr();
 
 constexpr int kMaxStages = 4;
@@ -437,9 +436,21 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
         const uint64_t w_lo = c * cw;
         const uint64_t w_hi = std::min<uint64_t>(W, w_lo + cw);
         const uint64_t b_lo = w_lo, b_hi = w_hi + K - 1;
-        while (rec < n && ranges[rec].sequence_offset + ranges[rec].sequence_bytes <= b_lo) ++rec;
-        rec_end = std::max(rec_end, rec);
-        while (rec_end < n && ranges[rec_end].sequence_offset < b_hi) ++rec_end;
+        // Validated records are ordered and non-overlapping, so both their
+        // starts and their ends are non-decreasing: binary searches find the
+        // chunk's records without touching the ones in between.
+        rec = static_cast<uint64_t>(
+            std::partition_point(ranges + rec, ranges + n,
+                                 [b_lo](const sbf_record_range& x) {
+                                     return x.sequence_offset + x.sequence_bytes <= b_lo;
+                                 }) -
+            ranges);
+        rec_end = static_cast<uint64_t>(
+            std::partition_point(ranges + std::max(rec_end, rec), ranges + n,
+                                 [b_hi](const sbf_record_range& x) {
+                                     return x.sequence_offset < b_hi;
+                                 }) -
+            ranges);
         const uint64_t np = rec_end - rec;
         if (np * sizeof(DevRange) > s.pin_rng_cap || np * sizeof(DevRange) > s.d_rng_cap) {
             // Many records shorter than K in one chunk: grow with headroom.
@@ -602,15 +613,15 @@ extern "C" int sbf_ragged_insert(sbf_filter_t* f, const char* h_seq, uint64_t le
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
     SBF_TRY(f->require_byte_symbols("the ragged host pipeline"));
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
-    SBF_TRY(validate_ranges(len, ranges, n));
+    uint64_t bases = 0;
+    SBF_TRY(validate_ranges(len, ranges, n, &bases));
     sbf_ragged_tuning t{};
     SBF_TRY(resolve_tuning(f, false, len, n, tuning, &t));
     unsigned long long counts[2];
     SBF_TRY(ragged_pipeline(f, false, h_seq, len, ranges, n, t, S_(stream), nullptr, counts));
     if (report) {
         report->records_indexed = n;
-        report->indexed_bases = 0;
-        for (uint64_t i = 0; i < n; ++i) report->indexed_bases += ranges[i].sequence_bytes;
+        report->indexed_bases = bases;
         report->inserted_kmers = counts[0];
     }
     return SBF_OK;
@@ -624,7 +635,8 @@ extern "C" int sbf_ragged_query(const sbf_filter_t* cf, const char* h_seq, uint6
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
     SBF_TRY(f->require_byte_symbols("the ragged host pipeline"));
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
-    SBF_TRY(validate_ranges(len, ranges, n));
+    uint64_t bases = 0;
+    SBF_TRY(validate_ranges(len, ranges, n, &bases));
     const uint64_t W = f->kmers_of(len);
     if (W && (!h_out || out_len < W))
         return set_error(SBF_ERR_INVALID_ARGUMENT, "ragged query output span is too small");
@@ -634,8 +646,7 @@ extern "C" int sbf_ragged_query(const sbf_filter_t* cf, const char* h_seq, uint6
     SBF_TRY(ragged_pipeline(f, true, h_seq, len, ranges, n, t, S_(stream), h_out, counts));
     if (report) {
         report->records_queried = n;
-        report->queried_bases = 0;
-        for (uint64_t i = 0; i < n; ++i) report->queried_bases += ranges[i].sequence_bytes;
+        report->queried_bases = bases;
         report->queried_kmers = counts[0];
         report->positive_kmers = counts[1];
     }
@@ -650,7 +661,8 @@ extern "C" int sbf_ragged_query_bits(const sbf_filter_t* cf, const char* h_seq, 
     if (!f) return set_error(SBF_ERR_INVALID_ARGUMENT, "filter is null");
     SBF_TRY(f->require_byte_symbols("the ragged host pipeline"));
     if (n && (!ranges || !h_seq)) return set_error(SBF_ERR_INVALID_ARGUMENT, "null pointer");
-    SBF_TRY(validate_ranges(len, ranges, n));
+    uint64_t bases = 0;
+    SBF_TRY(validate_ranges(len, ranges, n, &bases));
     const uint64_t W = f->kmers_of(len);
     if (W && (!h_bits || n_words < (W + 31) / 32))
         return set_error(SBF_ERR_INVALID_ARGUMENT, "ragged query bit output span is too small");
@@ -661,8 +673,7 @@ extern "C" int sbf_ragged_query_bits(const sbf_filter_t* cf, const char* h_seq, 
                             h_bits));
     if (report) {
         report->records_queried = n;
-        report->queried_bases = 0;
-        for (uint64_t i = 0; i < n; ++i) report->queried_bases += ranges[i].sequence_bytes;
+        report->queried_bases = bases;
         report->queried_kmers = counts[0];
         report->positive_kmers = counts[1];
     }

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "../../include/sbf_b200.h"
@@ -49,16 +50,59 @@ bool symbol_valid(int alphabet, const char* p) {
 // Host layout
 // ---------------------------------------------------------------------------
 
-int validate_ranges(uint64_t len, const sbf_record_range* r, uint64_t n) {
-    uint64_t next = 0;
-    for (uint64_t i = 0; i < n; ++i) {
-        if (r[i].sequence_offset < next)
+// Checks records [lo, hi), the first against the end of record lo - 1.
+// Returns 0, 1 (out of order or overlapping) or 2 (outside the sequence) for
+// the first bad record, and the segment's byte total.
+static int check_range_segment(uint64_t len, const sbf_record_range* r, uint64_t lo, uint64_t hi,
+                               uint64_t* total) {
+    uint64_t next = lo ? r[lo - 1].sequence_offset + r[lo - 1].sequence_bytes : 0;
+    uint64_t sum = 0;
+    for (uint64_t i = lo; i < hi; ++i) {
+        if (r[i].sequence_offset < next) return 1;
+        if (r[i].sequence_offset > len || r[i].sequence_bytes > len - r[i].sequence_offset)
+            return 2;
+        next = r[i].sequence_offset + r[i].sequence_bytes;
+        sum += r[i].sequence_bytes;
+    }
+    *total = sum;
+    return 0;
+}
+
+int validate_ranges(uint64_t len, const sbf_record_range* r, uint64_t n, uint64_t* total_bytes) {
+    // One pass at about 1.5 ns per record: batches of tens of millions of
+    // short reads are split over host threads so the check does not hold up
+    // the uploads that follow it.
+    constexpr uint64_t kPerThread = uint64_t{1} << 21;
+    const uint64_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint64_t parts = std::max<uint64_t>(
+        1, std::min<uint64_t>({(n + kPerThread - 1) / kPerThread, hw, 16}));
+    std::vector<int> status(parts, 0);
+    std::vector<uint64_t> sums(parts, 0);
+    auto seg = [&](uint64_t p) {
+        status[p] = check_range_segment(len, r, n * p / parts, n * (p + 1) / parts, &sums[p]);
+    };
+    if (parts == 1) {
+        seg(0);
+    } else {
+        std::vector<std::thread> pool;
+        pool.reserve(parts - 1);
+        for (uint64_t p = 1; p < parts; ++p) pool.emplace_back(seg, p);
+        seg(0);
+        for (auto& t : pool) t.join();
+    }
+    // The first bad record decides the message, as a serial scan would.
+    for (uint64_t p = 0; p < parts; ++p) {
+        if (status[p] == 1)
             return set_error(SBF_ERR_INVALID_ARGUMENT,
                              "record batch ranges must be ordered and non-overlapping");
-        if (r[i].sequence_offset > len || r[i].sequence_bytes > len - r[i].sequence_offset)
+        if (status[p] == 2)
             return set_error(SBF_ERR_INVALID_ARGUMENT,
                              "record batch range exceeds the source sequence");
-        next = r[i].sequence_offset + r[i].sequence_bytes;
+    }
+    if (total_bytes) {
+        uint64_t t = 0;
+        for (uint64_t s : sums) t += s;
+        *total_bytes = t;
     }
     return SBF_OK;
 }

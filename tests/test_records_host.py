@@ -52,6 +52,32 @@ def test_normalize_rejects_overlap(sbf):
         sbf.validate_record_batch(8, [(0, 4), (4, 5)])
 
 
+def test_validate_large_batch_reports_first_bad_record(sbf):
+    # Batches of millions of records are checked in segments on several host
+    # threads; the result and message must be those of a serial scan.
+    n, size = 6_000_000, 10
+    r = np.empty((n, 2), np.uint64)
+    r[:, 0] = np.arange(n, dtype=np.uint64) * size
+    r[:, 1] = size
+    total = n * size
+    sbf.validate_record_batch(total, r)
+    # Overlap across a segment boundary (segments start at multiples of n/3).
+    bad = r.copy()
+    bad[1_999_999, 1] = size + 1
+    with pytest.raises(sbf.SbfError, match="ordered and non-overlapping"):
+        sbf.validate_record_batch(total, bad)
+    # Two faults: the earlier one (out of bounds) decides the message.
+    bad = r.copy()
+    bad[4_000_000, 1] = total
+    bad[5_500_000, 0] -= 1
+    with pytest.raises(sbf.SbfError, match="exceeds the source sequence"):
+        sbf.validate_record_batch(total, bad)
+    bad = r.copy()
+    bad[5_999_999, 0] -= 1
+    with pytest.raises(sbf.SbfError, match="ordered and non-overlapping"):
+        sbf.validate_record_batch(total, bad)
+
+
 def _py_normalize(seq, ranges, k):
     out, recs = bytearray(), []
     for i, (o, n) in enumerate(ranges):
