@@ -426,10 +426,13 @@ def run_ragged(args, world: int, rank: int, local_rank: int) -> None:
         def e2e_obj(res, tuning):
             ims = float(np.median([r[0] for r in res]))
             qms = float(np.median([r[1] for r in res]))
+            expand = sbf.host_expand_threads()
             return {"value": world * kmers_step / ((ims + qms) / 1e3), "unit": "k-mers/s",
                     "h2d_bytes_per_step": int(genome.size + h_reads.size + 32 * (
                         g_ranges.shape[0] + r_ranges.shape[0])),
-                    "d2h_bytes_per_step": int(n_out), "ms_per_step": ims + qms,
+                    "d2h_bytes_per_step": int(4 * ((n_out + 31) // 32) if expand else n_out),
+                    "host_result_bytes": int(n_out), "host_expand_threads": expand,
+                    "ms_per_step": ims + qms,
                     "insert_ms": ims, "query_ms": qms, "tuning": tuning,
                     "api": "sbf_ragged_insert + sbf_ragged_query (host buffers, pinned)"}
 
@@ -464,6 +467,8 @@ def run_ragged(args, world: int, rank: int, local_rank: int) -> None:
             res.append(((w1 - w0) * 1e3, (w2 - w1) * 1e3))
         e2e_bits = e2e_obj(res[1:], {"insert": ti.as_dict(), "query": tq.as_dict()})
         e2e_bits["d2h_bytes_per_step"] = int(4 * ((n_out + 31) // 32))
+        e2e_bits["host_result_bytes"] = e2e_bits["d2h_bytes_per_step"]
+        e2e_bits.pop("host_expand_threads", None)
         e2e_bits["api"] = ("sbf_ragged_insert + sbf_ragged_query_bits (host buffers, pinned; "
                            "one result bit per window)")
         # The reference's single-launch record batch (host normalisation with
@@ -955,11 +960,16 @@ def main() -> None:
         e_ms, e_wall = max_over_ranks([e_ms, e_wall], dist, dev)
         assert int(h_out[:n_q_windows].sum(dtype=torch.int64)) == positives, \
             "host-API query disagrees with the device-resident query"
+        expand = sbf.host_expand_threads()
         e2e = {"value": world * kmers_step / (max(e_ms, e_wall) / 1e3), "unit": "k-mers/s",
                "h2d_bytes_per_step": int(joined.size + qnp.size),
-               "d2h_bytes_per_step": int(n_q_windows), "ms_per_step": max(e_ms, e_wall),
-               "steps": len(res),
-               "api": "sbf_insert_sequence + sbf_contains_sequence (host buffers, pinned)"}
+               "d2h_bytes_per_step": int(4 * ((n_q_windows + 31) // 32) if expand
+                                         else n_q_windows),
+               "host_result_bytes": int(n_q_windows), "host_expand_threads": expand,
+               "ms_per_step": max(e_ms, e_wall), "steps": len(res),
+               "api": "sbf_insert_sequence + sbf_contains_sequence (host buffers, pinned; one "
+                      "result byte per window in host memory, downloaded as bits and expanded "
+                      "by host threads when host_expand_threads > 0)"}
         # The same step with bit-packed results (one bit per window).
         n_words = (n_q_windows + 31) // 32
         h_bits = torch.empty(max(n_words, 1), dtype=torch.int32).pin_memory()

@@ -266,6 +266,8 @@ _sig("sbf_server_drain", C.c_int, _vp)
 _sig("sbf_server_get_stats", C.c_int, _vp, C.c_int, C.POINTER(ServerStats))
 _sig("sbf_contains_sequence_bits_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp)
 _sig("sbf_contains_sequence_bits", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp)
+_sig("sbf_expand_result_bits", C.c_int, _vp, _u64, _vp, _u32)
+_sig("sbf_host_expand_threads", C.c_int)
 _sig("sbf_filter_save", C.c_int, _vp, C.c_char_p, _vp)
 _sig("sbf_filter_file_info", C.c_int, C.c_char_p, C.POINTER(_u32), C.POINTER(_u32),
      C.POINTER(_u32), C.POINTER(_u32), C.POINTER(_u64))
@@ -944,6 +946,25 @@ _fastx_methods()
 
 
 _SYMBOL_WIDTH = {ALPHABET_DNA: 1, ALPHABET_PROTEIN: 1, ALPHABET_DNA_TRIPLET: 3}
+
+
+def host_expand_threads() -> int:
+    """Host threads that host-output queries expand bit-packed results with
+    (0: they download one byte per window; SBF_HOST_EXPAND[_THREADS])."""
+    return _lib.sbf_host_expand_threads()
+
+
+def expand_result_bits(bits, n_windows: int, out=None, threads: int = 0) -> np.ndarray:
+    """Bit-packed results (window i -> bit i % 32 of word i // 32) to one
+    byte per window, on host threads (sbf_expand_result_bits)."""
+    b = np.ascontiguousarray(np.asarray(bits).view(np.uint32).reshape(-1))
+    if b.size * 32 < n_windows:
+        raise ValueError("bit words hold fewer than n_windows results")
+    o = np.empty(max(n_windows, 1), np.uint8) if out is None else out
+    if o.size < n_windows:
+        raise ValueError("output holds fewer than n_windows bytes")
+    _check(_lib.sbf_expand_result_bits(_np_ptr(b), n_windows, _np_ptr(o), threads))
+    return o[:n_windows]
 
 
 def pack_dense_sequence(seq, alphabet: int = ALPHABET_DNA) -> np.ndarray:

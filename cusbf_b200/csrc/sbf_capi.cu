@@ -16,8 +16,9 @@
 #include <string>
 
 #include "../../include/sbf_b200.h"
-#include "sbf_internal.h"
+#include "sbf_expand.h"
 #include "sbf_host.h"
+#include "sbf_internal.h"
 
 using namespace sbf;
 
@@ -198,6 +199,13 @@ int sbf_filter::check_device_error(cudaStream_t st) const {
     return SBF_OK;
 }
 
+ExpandPool* sbf::host_expand_pool(sbf_filter* f) {
+    if (f->expand_threads < 0) f->expand_threads = host_expand_threads();
+    if (f->expand_threads == 0) return nullptr;
+    if (!f->expand) f->expand = new ExpandPool(f->expand_threads);
+    return f->expand;
+}
+
 // Host bytes -> device in chunks of whole windows with a (k-1)-symbol overlap,
 // kPipeSlots chunks in flight: uploads on copy_stream, kernels on `st`,
 // downloads on d2h_stream, so the three overlap across chunks.  `out_host`/`out_dev` receive query bytes.
@@ -209,6 +217,11 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
     // c * chunk_kmers / 32.
     const bool bits = bits_host != nullptr;
     if (n_kmers == 0) return SBF_OK;
+    // Byte results for a host buffer come down one bit per window and are
+    // expanded by host threads while later chunks upload (kbits: the kernel
+    // writes bit-packed results).
+    ExpandPool* pool = query && out_host != nullptr && !bits ? host_expand_pool(this) : nullptr;
+    const bool kbits = bits || pool != nullptr;
     // Symbols <-> bytes: byte input has one byte per symbol; dense input has
     // 32 symbols per 8-byte word, so chunks are cut at word boundaries.
     const uint64_t chunk_target = host_chunk_bytes();
@@ -217,12 +230,12 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
     if (dense) {
         // About chunk_target packed bytes, a whole number of words (and of
         // 32-window result words in bit-packed mode).
-        const uint64_t unit = bits ? per_word * 32 : per_word;
+        const uint64_t unit = kbits ? per_word * 32 : per_word;
         const uint64_t syms = chunk_target / 8 * per_word;
         chunk_kmers = std::max<uint64_t>(syms / unit * unit, unit);
     } else {
         const uint64_t t = chunk_target / width;
-        chunk_kmers = bits ? std::max<uint64_t>(t / 32 * 32, 1024) : t;
+        chunk_kmers = kbits ? std::max<uint64_t>(t / 32 * 32, 1024) : t;
     }
     const uint64_t n_chunks = (n_kmers + chunk_kmers - 1) / chunk_kmers;
     auto chunk_span = [&](uint64_t c, uint64_t& first_byte, uint64_t& bytes, uint64_t& kmers,
@@ -244,10 +257,22 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
         dense ? dense_words(chunk_kmers + k - 1) * 8 + 8 : (chunk_kmers + k) * width;
     const bool in_pinned = is_pinned(h_in);
     if (bits) out_host = reinterpret_cast<uint8_t*>(bits_host);
-    // Output bytes of a chunk of `kmers` windows, and the chunk's output offset.
-    auto out_size = [&](uint64_t kmers) { return bits ? (kmers + 31) / 32 * 4 : kmers; };
+    // Downloaded bytes of a chunk of `kmers` windows, and the chunk's offset
+    // in the host output.
+    auto out_size = [&](uint64_t kmers) { return kbits ? (kmers + 31) / 32 * 4 : kmers; };
     auto out_offset = [&](uint64_t c) { return bits ? c * chunk_kmers / 8 : c * chunk_kmers; };
-    const bool out_pinned = out_host != nullptr && is_pinned(out_host);
+    // Expanded results always pass through the pinned staging.
+    const bool out_pinned = out_host != nullptr && pool == nullptr && is_pinned(out_host);
+    // Moves a downloaded chunk from the pinned staging to the host output.
+    auto drain = [&](uint64_t c, int slot) {
+        uint64_t pf, pb, pk, po;
+        chunk_span(c, pf, pb, pk, po);
+        if (pool)
+            pool->run(static_cast<const uint32_t*>(stage_out.pin[slot]), out_host + out_offset(c),
+                      pk);
+        else
+            std::memcpy(out_host + out_offset(c), stage_out.pin[slot], out_size(pk));
+    };
     SBF_TRY(stage_in.ensure_device(max_in));
     if (!in_pinned) SBF_TRY(stage_in.ensure_pinned(max_in));
     if (query && out_dev == nullptr) SBF_TRY(stage_out.ensure_device(out_size(chunk_kmers)));
@@ -267,12 +292,8 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
         // The slot's previous kernel and download must be finished before
         // its buffers are reused.
         SBF_CUDA(cudaEventSynchronize(ev_done[slot]));
-        if (query && out_host != nullptr && !out_pinned && c >= kPipeSlots) {
-            // Drain the host output of the chunk that used this slot before.
-            uint64_t pf, pb, pk, po;
-            chunk_span(c - kPipeSlots, pf, pb, pk, po);
-            std::memcpy(out_host + out_offset(c - kPipeSlots), stage_out.pin[slot], out_size(pk));
-        }
+        if (query && out_host != nullptr && !out_pinned && c >= kPipeSlots)
+            drain(c - kPipeSlots, slot);  // the chunk that used this slot before
         const char* src = static_cast<const char*>(h_in) + first_byte;
         if (!in_pinned) {
             std::memcpy(stage_in.pin[slot], src, bytes);
@@ -287,8 +308,8 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
             dout = out_dev ? out_dev + c * chunk_kmers
                            : static_cast<uint8_t*>(stage_out.dev[slot]);
         }
-        SBF_TRY(launch(query, dense, stage_in.dev[slot], bytes, kmers, bits ? nullptr : dout, st,
-                       bits ? reinterpret_cast<uint32_t*>(dout) : nullptr));
+        SBF_TRY(launch(query, dense, stage_in.dev[slot], bytes, kmers, kbits ? nullptr : dout, st,
+                       kbits ? reinterpret_cast<uint32_t*>(dout) : nullptr));
         SBF_CUDA(cudaEventRecord(ev_kernel[slot], st));
         if (query && out_host != nullptr) {
             void* hdst = out_pinned ? static_cast<void*>(out_host + out_offset(c))
@@ -304,15 +325,16 @@ int sbf_filter::host_pipeline(bool query, bool dense, const void* h_in, uint64_t
     // `st` completes after every kernel and download of this call.
     SBF_CUDA(cudaEventRecord(ev_kernel[0], d2h_stream));
     SBF_CUDA(cudaStreamWaitEvent(st, ev_kernel[0], 0));
-    SBF_CUDA(cudaStreamSynchronize(st));
     if (query && out_host != nullptr && !out_pinned) {
+        // The last chunks, each as soon as its download is done.
         const uint64_t first = n_chunks > kPipeSlots ? n_chunks - kPipeSlots : 0;
         for (uint64_t c = first; c < n_chunks; ++c) {
-            uint64_t pf, pb, pk, po;
-            chunk_span(c, pf, pb, pk, po);
-            std::memcpy(out_host + out_offset(c), stage_out.pin[c % kPipeSlots], out_size(pk));
+            const int slot = static_cast<int>(c % kPipeSlots);
+            SBF_CUDA(cudaEventSynchronize(ev_done[slot]));
+            drain(c, slot);
         }
     }
+    SBF_CUDA(cudaStreamSynchronize(st));
     return check_device_error(st);
 }
 
@@ -456,6 +478,7 @@ extern "C" void sbf_filter_destroy(sbf_filter_t* f) {
     f->rb_meta.release();
     f->rb_hits.release();
     f->rb_stats.release();
+    delete f->expand;
     if (f->d_words) cudaFree(f->d_words);
     if (f->d_err) cudaFree(f->d_err);
     for (int i = 0; i < kPipeSlots; ++i) {

@@ -53,6 +53,7 @@ struct DevBuf {
 
 struct RaggedState;
 struct FastqDevice;
+class ExpandPool;
 
 }  // namespace sbf
 
@@ -89,6 +90,12 @@ struct sbf_filter {
     // Record-batch staging (sbf_records.cu).
     sbf::DevBuf rb_dense, rb_norm, rb_meta, rb_hits, rb_stats;
 
+    // Host threads that expand bit-packed query results into host bytes
+    // (sbf_expand.cpp), created on first use; expand_threads < 0 until the
+    // first host-output query decides (0 = download bytes).
+    sbf::ExpandPool* expand = nullptr;
+    int expand_threads = -1;
+
     uint64_t kmers_of(uint64_t symbols) const;
     // Windows of a byte sequence (symbols = bytes / width).
     uint64_t kmers_of_bytes(uint64_t bytes) const { return kmers_of(bytes / width); }
@@ -116,6 +123,9 @@ struct sbf_filter {
 namespace sbf {
 void ragged_release(sbf_filter* f);
 void fastq_device_release(sbf_filter* f);
+// The filter's pool for expanding bit-packed results into host bytes, or
+// nullptr when host-output queries download bytes (sbf_expand.cpp).
+ExpandPool* host_expand_pool(sbf_filter* f);
 // Checks that records are ordered, non-overlapping and inside [0, len)
 // (normalized_record_batch.hpp:123-147); large batches are checked on several
 // host threads.  `total_bytes`, when given, receives the sum of the record

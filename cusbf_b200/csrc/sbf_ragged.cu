@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "../../include/sbf_b200.h"
+#include "sbf_expand.h"
 #include "sbf_host.h"
 #include "sbf_internal.h"
 #include "sbf_ragged.h"
@@ -67,6 +68,12 @@ struct RaggedSlot {
     size_t tile_cap = 0;
     uint8_t* d_out = nullptr;
     size_t out_cap = 0;
+    // Bit-packed results of a byte-output query, expanded on the host once
+    // downloaded: windows [pend_lo, pend_lo + pend_n) of the batch.
+    uint32_t* pin_out = nullptr;
+    size_t pin_out_cap = 0;
+    uint64_t pend_lo = 0, pend_n = 0;
+    bool pend = false;
     cudaEvent_t ev_copied = nullptr, ev_kernel = nullptr, ev_done = nullptr;
     bool busy = false;
     RaggedGraph graph[2];  // per operation (insert, query)
@@ -116,6 +123,7 @@ static int grow_pinned(T*& p, size_t& cap, size_t bytes) {
 static void release_slot(RaggedSlot& s) {
     if (s.pin_seq) cudaFreeHost(s.pin_seq);
     if (s.pin_rng) cudaFreeHost(s.pin_rng);
+    if (s.pin_out) cudaFreeHost(s.pin_out);
     if (s.d_seq) cudaFree(s.d_seq);
     if (s.d_rng) cudaFree(s.d_rng);
     if (s.d_tile_rec) cudaFree(s.d_tile_rec);
@@ -394,17 +402,21 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
     const bool bits = h_bits != nullptr;
     const uint64_t K = f->k;
     const uint64_t W = f->kmers_of(len);
-    auto out_bytes = [&](uint64_t windows) { return bits ? (windows + 31) / 32 * 4 : windows; };
     if (W == 0 || n == 0) {
         if (query && W) std::memset(bits ? reinterpret_cast<uint8_t*>(h_bits) : h_out, 0,
-                                    out_bytes(W));
+                                    bits ? (W + 31) / 32 * 4 : W);
         return SBF_OK;
     }
+    // Byte results come down one bit per window and are expanded by host
+    // threads (kbits: the kernel writes bit-packed results).
+    ExpandPool* pool = query && !bits ? host_expand_pool(f) : nullptr;
+    const bool kbits = bits || pool != nullptr;
+    auto out_bytes = [&](uint64_t windows) { return kbits ? (windows + 31) / 32 * 4 : windows; };
     RaggedState* r = nullptr;
     SBF_TRY(ragged_state(f, &r));
     SBF_TRY(check_tuning(t));
     uint64_t cw = std::max<uint64_t>(t.chunk_bytes > K ? t.chunk_bytes - (K - 1) : 1, 1024);
-    if (bits) cw = cw / 32 * 32;
+    if (kbits) cw = std::max<uint64_t>(cw / 32 * 32, 1024);
     const uint64_t n_chunks = (W + cw - 1) / cw;
     const uint64_t max_bytes = cw + K - 1;
     const uint64_t max_pieces = max_bytes / K + 2;
@@ -421,7 +433,9 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
         SBF_TRY(grow_device(s.d_rng, s.d_rng_cap, max_pieces * sizeof(DevRange)));
         SBF_TRY(grow_device(s.d_tile_rec, s.tile_cap, ((cw + 16) / kTileKmers + 2) * 4));
         if (query) SBF_TRY(grow_device(s.d_out, s.out_cap, out_bytes(cw) + 16));
+        if (pool) SBF_TRY(grow_pinned(s.pin_out, s.pin_out_cap, out_bytes(cw) + 16));
         s.busy = false;
+        s.pend = false;
     }
     // The copy stream starts after work already queued on `st`.
     cudaEvent_t ev_start = r->slot[0].ev_done;
@@ -433,6 +447,10 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
     for (uint64_t c = 0; c < n_chunks; ++c) {
         RaggedSlot& s = r->slot[c % S];
         if (s.busy) SBF_CUDA(cudaEventSynchronize(s.ev_done));
+        if (s.pend) {
+            pool->run(s.pin_out, h_out + s.pend_lo, s.pend_n);
+            s.pend = false;
+        }
         const uint64_t w_lo = c * cw;
         const uint64_t w_hi = std::min<uint64_t>(W, w_lo + cw);
         const uint64_t b_lo = w_lo, b_hi = w_hi + K - 1;
@@ -479,7 +497,7 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
             clip_ranges_kernel<<<blocks, 256, 0, st>>>(s.d_rng, np, b_lo, b_hi);
             SBF_CUDA(cudaGetLastError());
             const TileParams p = ragged_params(f, query, s.d_seq, b_hi - b_lo, s.d_rng, np,
-                                               s.d_tile_rec, s.d_out, r->d_ctl, d_counts, bits);
+                                               s.d_tile_rec, s.d_out, r->d_ctl, d_counts, kbits);
             if (t.use_graph)
                 SBF_TRY(ragged_graph_launch(f, s.graph[query ? 1 : 0], query, p, t.ctas_per_sm,
                                             st));
@@ -495,14 +513,32 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
         if (query) {
             SBF_CUDA(cudaEventRecord(s.ev_kernel, st));
             SBF_CUDA(cudaStreamWaitEvent(r->d2h_stream, s.ev_kernel, 0));
-            void* dst = bits ? static_cast<void*>(h_bits + w_lo / 32) : h_out + w_lo;
+            void* dst = bits   ? static_cast<void*>(h_bits + w_lo / 32)
+                        : pool ? static_cast<void*>(s.pin_out)
+                               : static_cast<void*>(h_out + w_lo);
             SBF_CUDA(cudaMemcpyAsync(dst, s.d_out, out_bytes(w_hi - w_lo), cudaMemcpyDeviceToHost,
                                      r->d2h_stream));
+            if (pool) {
+                s.pend = true;
+                s.pend_lo = w_lo;
+                s.pend_n = w_hi - w_lo;
+            }
             SBF_CUDA(cudaEventRecord(s.ev_done, r->d2h_stream));
         } else {
             SBF_CUDA(cudaEventRecord(s.ev_done, st));
         }
         s.busy = true;
+    }
+    if (pool) {
+        // The last chunks, each as soon as its download is done.
+        const uint64_t first = n_chunks > S ? n_chunks - S : 0;
+        for (uint64_t c = first; c < n_chunks; ++c) {
+            RaggedSlot& s = r->slot[c % S];
+            if (!s.pend) continue;
+            SBF_CUDA(cudaEventSynchronize(s.ev_done));
+            pool->run(s.pin_out, h_out + s.pend_lo, s.pend_n);
+            s.pend = false;
+        }
     }
     SBF_CUDA(cudaEventRecord(r->slot[0].ev_kernel, r->d2h_stream));
     SBF_CUDA(cudaStreamWaitEvent(st, r->slot[0].ev_kernel, 0));

@@ -182,6 +182,18 @@ int sbf_contains_sequence_bits_async(const sbf_filter_t* filter, const char* d_s
 /* Host input and host bit output through the pinned chunk pipeline. */
 int sbf_contains_sequence_bits(const sbf_filter_t* filter, const char* h_seq, uint64_t bytes,
                                uint32_t* h_bits, uint64_t n_words, sbf_stream_t stream);
+/* Host only, no GPU work: expands bit-packed results into one byte per
+ * window (out[i] = bit i % 32 of bits[i / 32], 0 or 1) on up to `threads`
+ * host threads (0 = half the hardware threads, at most 4).  The host-output
+ * queries (sbf_contains_sequence, sbf_ragged_query, ...) download bits and
+ * expand them this way on hosts with at least 8 hardware threads, with 4
+ * threads (SBF_HOST_EXPAND_THREADS overrides); SBF_HOST_EXPAND=0 makes them
+ * download bytes instead, =1 always expand. */
+int sbf_expand_result_bits(const uint32_t* bits, uint64_t n_windows, uint8_t* out,
+                           uint32_t threads);
+/* Host threads that host-output queries of filters created from now on will
+ * expand bit-packed results with (0: they download one byte per window). */
+int sbf_host_expand_threads(void);
 
 /* ---- persistence (no reference counterpart) ------------------------------
  * A saved filter is a 40-byte header (magic "SBFB200", version, k, s, m,
