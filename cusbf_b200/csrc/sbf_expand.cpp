@@ -83,6 +83,32 @@ bool have_avx2() {
     return yes;
 }
 
+void blocks_any(const uint32_t* bits, uint64_t j0, uint8_t* out, uint64_t b0, uint64_t b1) {
+    if (have_avx2())
+        blocks_avx2(bits, j0, out, b0, b1);
+    else
+        blocks_scalar(bits, j0, out, b0, b1);
+}
+
+// Head bytes up to the first 32-byte boundary of `out`, whole 32-window
+// blocks after it, and the tail; returns the head length and block count.
+void split(const uint8_t* out, uint64_t n, uint64_t* head, uint64_t* blocks) {
+    *head = std::min<uint64_t>(n, (32 - (reinterpret_cast<uintptr_t>(out) & 31u)) & 31u);
+    *blocks = (n - *head) / 32;
+}
+
+void edges(const uint32_t* bits, uint8_t* out, uint64_t n, uint64_t head, uint64_t blocks) {
+    for (uint64_t i = 0; i < head; ++i) out[i] = bit_at(bits, i);
+    for (uint64_t i = head + 32 * blocks; i < n; ++i) out[i] = bit_at(bits, i);
+}
+
+void expand_serial(const ExpandItem& it) {
+    uint64_t head, blocks;
+    split(it.out, it.n, &head, &blocks);
+    edges(it.bits, it.out, it.n, head, blocks);
+    if (blocks) blocks_any(it.bits, head, it.out + head, 0, blocks);
+}
+
 }  // namespace
 
 ExpandPool::ExpandPool(int threads) : threads_(std::max(threads, 1)) {
@@ -99,13 +125,26 @@ ExpandPool::~ExpandPool() {
 }
 
 void ExpandPool::part(int t, int parts) {
+    if (job_.items) {
+        for (size_t i = static_cast<size_t>(t); i < job_.n_items; i += static_cast<size_t>(parts))
+            expand_serial(job_.items[i]);
+        return;
+    }
     const uint64_t lo = job_.blocks * static_cast<uint64_t>(t) / parts;
     const uint64_t hi = job_.blocks * static_cast<uint64_t>(t + 1) / parts;
-    if (lo == hi) return;
-    if (have_avx2())
-        blocks_avx2(job_.bits, job_.j0, job_.body, lo, hi);
-    else
-        blocks_scalar(job_.bits, job_.j0, job_.body, lo, hi);
+    if (lo < hi) blocks_any(job_.bits, job_.j0, job_.body, lo, hi);
+}
+
+void ExpandPool::dispatch() {
+    {
+        std::lock_guard<std::mutex> g(m_);
+        pending_ = threads_ - 1;
+        ++gen_;
+    }
+    cv_.notify_all();
+    part(0, threads_);
+    std::unique_lock<std::mutex> l(m_);
+    done_cv_.wait(l, [&] { return pending_ == 0; });
 }
 
 void ExpandPool::worker(int t) {
@@ -127,30 +166,35 @@ void ExpandPool::worker(int t) {
 
 void ExpandPool::run(const uint32_t* bits, uint8_t* out, uint64_t n) {
     if (n == 0) return;
-    // Head bytes up to the first 32-byte boundary of `out`, then whole
-    // 32-window blocks, then the tail.
-    const uint64_t head = std::min<uint64_t>(
-        n, (32 - (reinterpret_cast<uintptr_t>(out) & 31u)) & 31u);
-    for (uint64_t i = 0; i < head; ++i) out[i] = bit_at(bits, i);
-    const uint64_t blocks = (n - head) / 32;
-    const uint64_t tail0 = head + 32 * blocks;
-    for (uint64_t i = tail0; i < n; ++i) out[i] = bit_at(bits, i);
+    uint64_t head, blocks;
+    split(out, n, &head, &blocks);
+    edges(bits, out, n, head, blocks);
     if (blocks == 0) return;
-    job_ = Job{bits, head, out + head, blocks};
+    job_ = Job{bits, head, out + head, blocks, nullptr, 0};
     // Small jobs are not worth waking the pool.
     if (threads_ == 1 || blocks < 4096) {
         part(0, 1);
         return;
     }
-    {
-        std::lock_guard<std::mutex> g(m_);
-        pending_ = threads_ - 1;
-        ++gen_;
+    dispatch();
+}
+
+void ExpandPool::run_items(const ExpandItem* items, size_t n_items) {
+    if (n_items == 0) return;
+    if (n_items == 1) {
+        run(items[0].bits, items[0].out, items[0].n);
+        return;
     }
-    cv_.notify_all();
-    part(0, threads_);
-    std::unique_lock<std::mutex> l(m_);
-    done_cv_.wait(l, [&] { return pending_ == 0; });
+    uint64_t total = 0;
+    for (size_t i = 0; i < n_items; ++i) total += items[i].n;
+    job_ = Job{};
+    job_.items = items;
+    job_.n_items = n_items;
+    if (threads_ == 1 || total < 32 * 4096) {
+        part(0, 1);
+        return;
+    }
+    dispatch();
 }
 
 int host_expand_threads() {

@@ -12,6 +12,13 @@ namespace sbf {
 // A fixed pool of host threads (the caller counts as one) that writes
 // out[i] = bit i % 32 of bits[i / 32] for i < n; it reads only the words
 // that hold those bits.
+// One expansion: out[i] = bit i of `bits` for i < n.
+struct ExpandItem {
+    const uint32_t* bits;
+    uint8_t* out;
+    uint64_t n;
+};
+
 class ExpandPool {
 public:
     explicit ExpandPool(int threads);
@@ -19,6 +26,8 @@ public:
     ExpandPool(const ExpandPool&) = delete;
     ExpandPool& operator=(const ExpandPool&) = delete;
     void run(const uint32_t* bits, uint8_t* out, uint64_t n);  // returns when done
+    // Many expansions (one per served request), each on one thread.
+    void run_items(const ExpandItem* items, size_t n_items);
 
 private:
     struct Job {
@@ -26,7 +35,10 @@ private:
         uint64_t j0 = 0;          // window of the first block
         uint8_t* body = nullptr;  // 32-byte aligned
         uint64_t blocks = 0;
+        const ExpandItem* items = nullptr;  // run_items: the list, else null
+        size_t n_items = 0;
     };
+    void dispatch();  // runs job_ on every thread, returns when all are done
     void worker(int t);
     void part(int t, int parts);
 

@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "../../include/sbf_b200.h"
+#include "sbf_expand.h"
 #include "sbf_host.h"
 #include "sbf_internal.h"
 #include "sbf_ragged.h"
@@ -67,7 +68,6 @@ constexpr int kOpInsert = 0, kOpQuery = 1, kOpQueryBits = 2, kOpQueryCounts = 3;
 constexpr int kOpDense = 0x10;
 int base_op(int op) { return op & 0xF; }
 bool is_dense(int op) { return (op & kOpDense) != 0; }
-uint64_t pad_of(int op) { return base_op(op) == kOpQueryBits ? 32 : 16; }
 uint64_t result_bytes(int op, uint64_t windows, uint64_t records) {
     op = base_op(op);
     return op == kOpQueryBits     ? (windows + 31) / 32 * 4
@@ -147,6 +147,9 @@ struct SrvBatch {
     uint64_t seq_bytes = 0, n_ranges = 0;
     uint64_t packed_bytes = 0;  // dense batches: staged packed words
     uint64_t dev_off = 0, dev_bytes = 0, pin_off = 0, pin_bytes = 0;
+    // Byte-result queries expanded on the host: the downloaded bits, the
+    // last res_bytes of the batch's pinned region.
+    uint64_t res_bytes = 0;
     bool complete = false;
     int status = SBF_OK;
     cudaEvent_t ev_up = nullptr, ev_comp = nullptr, ev_done = nullptr;
@@ -210,6 +213,17 @@ __global__ void rebase_ranges_kernel(DevRange* rng, const FixEntry* tab, uint32_
 struct Server {
     sbf_filter* f = nullptr;
     sbf_server_config cfg{};
+    // Byte-result queries (op 1) download one bit per window and the
+    // completion thread expands them into the requests' buffers with this
+    // pool (null: bytes are downloaded).
+    std::unique_ptr<ExpandPool> pool;
+    bool expands(int op) const { return pool != nullptr && base_op(op) == kOpQuery; }
+    // Requests start on 32-byte boundaries of the batch where results are
+    // bit-packed (so each request's bits start on a word), else 16.
+    uint64_t pad(int op) const { return base_op(op) == kOpQueryBits || expands(op) ? 32 : 16; }
+    uint8_t* pinned_results(const SrvBatch* b) const {
+        return h_ring + b->pin_off + b->pin_bytes - b->res_bytes;
+    }
     cudaStream_t up = nullptr, comp = nullptr, down = nullptr;
     uint8_t* d_ring = nullptr;
     uint8_t* h_ring = nullptr;
@@ -294,6 +308,18 @@ void Server::finish() {
                 fatal = b->status;
                 fatal_msg = sbf_last_error_message();
             }
+        } else if (b->status == SBF_OK && expands(b->op)) {
+            // Downloaded bits -> each request's result bytes.
+            std::vector<ExpandItem> items;
+            items.reserve(b->reqs.size());
+            for (size_t i = 0; i < b->reqs.size(); ++i) {
+                SrvRequest* r = b->reqs[i];
+                if (r->windows)
+                    items.push_back(ExpandItem{
+                        reinterpret_cast<const uint32_t*>(pinned_results(b) + b->req_off[i] / 8),
+                        static_cast<uint8_t*>(r->out), r->windows});
+            }
+            pool->run_items(items.data(), items.size());
         }
         complete(b, b->status);
         lk.lock();
@@ -323,7 +349,7 @@ void Server::run() {
         for (SrvRequest* r : pending) {
             if (r->op != b->op) break;
             if (cfg.max_batch_requests && take >= cfg.max_batch_requests) break;
-            const uint64_t span = align_up(r->hi - r->lo, pad_of(r->op));
+            const uint64_t span = align_up(r->hi - r->lo, pad(r->op));
             if (take > 0 && (seq + span > cfg.max_batch_bytes ||
                              (nr + r->n) * sizeof(DevRange) > cfg.max_batch_bytes))
                 break;
@@ -342,9 +368,10 @@ void Server::run() {
                                    align_up(n_tiles * 4, kAlign) +
                                    align_up(take * sizeof(FixEntry), kAlign) +
                                    (dense ? align_up(packed, kAlign) : 0) + unpack_tab;
+        const uint64_t res_bytes = expands(b->op) ? align_up(seq / 8 + 64, kAlign) : 0;
         const uint64_t pin_bytes = align_up(nr * sizeof(DevRange), kAlign) +
                                    align_up(take * sizeof(FixEntry), kAlign) + unpack_tab +
-                                   align_up(gather, kAlign);
+                                   align_up(gather, kAlign) + res_bytes;
         // Admission: wait for ring space (completions free it).
         for (;;) {
             uint64_t doff = 0, poff = 0;
@@ -379,6 +406,7 @@ void Server::run() {
         }
         b->dev_bytes = dev_bytes;
         b->pin_bytes = pin_bytes;
+        b->res_bytes = res_bytes;
         b->seq_bytes = seq;
         b->n_ranges = nr;
         b->packed_bytes = packed;
@@ -422,7 +450,8 @@ void Server::run() {
 
 int Server::launch(SrvBatch* b) {
     const bool query = base_op(b->op) != kOpInsert;
-    const bool bits = base_op(b->op) == kOpQueryBits;
+    const bool expand = expands(b->op);
+    const bool bits = base_op(b->op) == kOpQueryBits || expand;
     const bool tally = base_op(b->op) == kOpQueryCounts;
     uint8_t* dbase = d_ring + b->dev_off;
     uint8_t* d_seq = dbase;
@@ -465,7 +494,7 @@ int Server::launch(SrvBatch* b) {
     for (size_t i = 0; i < b->reqs.size(); ++i) {
         SrvRequest* r = b->reqs[i];
         const uint64_t span = r->hi - r->lo;
-        const uint64_t padded = align_up(span, pad_of(r->op));
+        const uint64_t padded = align_up(span, pad(r->op));
         b->req_off[i] = o;
         b->req_rec[i] = k;
         if (r->n) {
@@ -578,8 +607,11 @@ int Server::launch(SrvBatch* b) {
         SrvRequest* r = b->reqs[i];
         if (tally ? r->n == 0 : r->windows == 0) continue;
         const uint64_t src = tally ? b->req_rec[i] * 16 : bits ? b->req_off[i] / 8 : b->req_off[i];
-        if ((e = cudaMemcpyAsync(r->out, d_out + src, result_bytes(b->op, r->windows, r->n),
-                                 cudaMemcpyDeviceToHost, down)) != cudaSuccess)
+        void* dst = expand ? static_cast<void*>(pinned_results(b) + src) : r->out;
+        const uint64_t bytes = expand ? (r->windows + 31) / 32 * 4
+                                      : result_bytes(b->op, r->windows, r->n);
+        if ((e = cudaMemcpyAsync(dst, d_out + src, bytes, cudaMemcpyDeviceToHost, down)) !=
+            cudaSuccess)
             return cuda_fail(e, "cudaMemcpyAsync(hits)");
     }
     if ((e = cudaEventRecord(b->ev_done, down)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
@@ -657,6 +689,7 @@ extern "C" int sbf_server_create(sbf_filter_t* f, const sbf_server_config* confi
         sbf_server_destroy(h);
         return rc;
     }
+    if (const int t = host_expand_threads(); t > 0) s.pool = std::make_unique<ExpandPool>(t);
     s.worker = std::thread([&s] { s.run(); });
     s.completer = std::thread([&s] { s.finish(); });
     *out = h;
@@ -695,7 +728,7 @@ extern "C" int sbf_server_submit(sbf_server_t* h, int op, const char* base,
         base_op(op) == kOpQueryCounts ? n > 0 : (base_op(op) != kOpInsert && r->windows > 0);
     if (has_result && (!out || out_len < result_bytes(op, r->windows, n)))
         return set_error(SBF_ERR_INVALID_ARGUMENT, "query output span is too small");
-    if (align_up(span, pad_of(op)) > s.cfg.max_batch_bytes || n * sizeof(DevRange) > s.cfg.max_batch_bytes)
+    if (align_up(span, s.pad(op)) > s.cfg.max_batch_bytes || n * sizeof(DevRange) > s.cfg.max_batch_bytes)
         return set_error(SBF_ERR_INVALID_ARGUMENT,
                          "request of %llu bytes exceeds the server's batch cap of %llu bytes",
                          static_cast<unsigned long long>(span),

@@ -101,12 +101,17 @@ def _served(sbf, genome, reqs, bits, **cfg):
 @pytest.mark.parametrize("cfg", [dict(), dict(use_graph=1, max_inflight=2),
                                  dict(max_batch_bytes=1 << 18, max_inflight=4)],
                          ids=["default", "graph", "small-batches"])
-def test_served_equals_serial(sbf, cuda, cfg):
+@pytest.mark.parametrize("expand", ["0", "1"], ids=["byte-download", "host-expand"])
+def test_served_equals_serial(sbf, cuda, monkeypatch, cfg, expand):
+    """Byte results (op 1) either come down as bytes or as bits that the
+    completion thread expands; both equal the serial byte-download path."""
     rng = np.random.default_rng(17)
     genome = random_dna(rng, 400_000)
     reqs = _make_requests(rng, genome, 250)
     bits = 1 << 22
+    monkeypatch.setenv("SBF_HOST_EXPAND", "0")
     want, want_words = _serial(sbf, genome, reqs, bits)
+    monkeypatch.setenv("SBF_HOST_EXPAND", expand)
     got, words, stats = _served(sbf, genome, reqs, bits, **cfg)
     np.testing.assert_array_equal(words, want_words)
     for i, (w, g) in enumerate(zip(want, got)):
