@@ -202,7 +202,15 @@ int sbf_filter::check_device_error(cudaStream_t st) const {
 ExpandPool* sbf::host_expand_pool(sbf_filter* f) {
     if (f->expand_threads < 0) f->expand_threads = host_expand_threads();
     if (f->expand_threads == 0) return nullptr;
-    if (!f->expand) f->expand = new ExpandPool(f->expand_threads);
+    if (!f->expand) {
+        try {
+            f->expand = new ExpandPool(f->expand_threads);
+        } catch (...) {
+            // No host threads to be had: download bytes from now on.
+            f->expand_threads = 0;
+            return nullptr;
+        }
+    }
     return f->expand;
 }
 

@@ -112,7 +112,18 @@ void expand_serial(const ExpandItem& it) {
 }  // namespace
 
 ExpandPool::ExpandPool(int threads) : threads_(std::max(threads, 1)) {
-    for (int t = 1; t < threads_; ++t) workers_.emplace_back([this, t] { worker(t); });
+    try {
+        for (int t = 1; t < threads_; ++t) workers_.emplace_back([this, t] { worker(t); });
+    } catch (...) {
+        // Stop the workers that did start, then report the failure.
+        {
+            std::lock_guard<std::mutex> g(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& w : workers_) w.join();
+        throw;
+    }
 }
 
 ExpandPool::~ExpandPool() {
@@ -226,8 +237,12 @@ extern "C" int sbf_expand_result_bits(const uint32_t* bits, uint64_t n_windows, 
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     const int t = threads ? static_cast<int>(std::min(threads, 64u))
                           : static_cast<int>(std::min(4u, std::max(1u, hw / 2)));
-    sbf::ExpandPool pool(t);
-    pool.run(bits, out, n_windows);
+    try {
+        sbf::ExpandPool pool(t);
+        pool.run(bits, out, n_windows);
+    } catch (...) {
+        return sbf::set_error(SBF_ERR_RESOURCE, "cannot start host expansion threads");
+    }
     return SBF_OK;
 }
 

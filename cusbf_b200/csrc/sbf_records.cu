@@ -86,7 +86,13 @@ int validate_ranges(uint64_t len, const sbf_record_range* r, uint64_t n, uint64_
     } else {
         std::vector<std::thread> pool;
         pool.reserve(parts - 1);
-        for (uint64_t p = 1; p < parts; ++p) pool.emplace_back(seg, p);
+        uint64_t started = 1;
+        try {
+            for (; started < parts; ++started) pool.emplace_back(seg, started);
+        } catch (...) {
+            // Fewer host threads than asked for: check the rest here.
+        }
+        for (uint64_t p = started; p < parts; ++p) seg(p);
         seg(0);
         for (auto& t : pool) t.join();
     }

@@ -689,9 +689,21 @@ extern "C" int sbf_server_create(sbf_filter_t* f, const sbf_server_config* confi
         sbf_server_destroy(h);
         return rc;
     }
-    if (const int t = host_expand_threads(); t > 0) s.pool = std::make_unique<ExpandPool>(t);
-    s.worker = std::thread([&s] { s.run(); });
-    s.completer = std::thread([&s] { s.finish(); });
+    if (const int t = host_expand_threads(); t > 0) {
+        try {
+            s.pool = std::make_unique<ExpandPool>(t);
+        } catch (...) {
+            s.pool.reset();  // no host threads to be had: download bytes
+        }
+    }
+    try {
+        s.worker = std::thread([&s] { s.run(); });
+        s.completer = std::thread([&s] { s.finish(); });
+    } catch (...) {
+        // Nothing is queued yet, so destroy only joins what did start.
+        sbf_server_destroy(h);
+        return set_error(SBF_ERR_RESOURCE, "cannot start the server threads");
+    }
     *out = h;
     return SBF_OK;
 }
