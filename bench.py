@@ -751,6 +751,7 @@ def run_served(args, world: int, rank: int, local_rank: int) -> None:
                                f"{rate:.0f} req/s, filter of the 100 Mbp genome resident",
                    "query_results": {1: "one byte per window", 2: "bit-packed (op 2)",
                                      3: "per-read (valid, positive) counts (op 3)"}[op_q],
+                   "host_expand_threads": (sbf.host_expand_threads() if op_q == 1 else 0),
                    "request_bodies": ("2-bit dense-packed words (op | 0x10; N packs as G)"
                                       if dense_flag else "ASCII bytes"),
                    "k": K, "s": S, "m": M, "hashes": H, "filter_bits": bits,
