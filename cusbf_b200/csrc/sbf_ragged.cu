@@ -359,11 +359,12 @@ static sbf_ragged_tuning default_tuning(bool query = false) {
     return t;
 }
 
-static int check_tuning(sbf_ragged_tuning& t) {
-    if (t.chunk_bytes == 0) t.chunk_bytes = default_tuning().chunk_bytes;
+// Zero fields take the operation's defaults.
+static int check_tuning(sbf_ragged_tuning& t, bool query) {
+    if (t.chunk_bytes == 0) t.chunk_bytes = default_tuning(query).chunk_bytes;
     if (t.chunk_bytes < 4096)
         return set_error(SBF_ERR_INVALID_ARGUMENT, "ragged chunk_bytes must be at least 4096");
-    if (t.stages == 0) t.stages = 2;
+    if (t.stages == 0) t.stages = default_tuning(query).stages;
     if (t.stages < 1 || t.stages > kMaxStages)
         return set_error(SBF_ERR_INVALID_ARGUMENT, "ragged stages must be 1..%d", kMaxStages);
     return SBF_OK;
@@ -414,7 +415,7 @@ static int ragged_pipeline(sbf_filter* f, bool query, const char* h_seq, uint64_
     auto out_bytes = [&](uint64_t windows) { return kbits ? (windows + 31) / 32 * 4 : windows; };
     RaggedState* r = nullptr;
     SBF_TRY(ragged_state(f, &r));
-    SBF_TRY(check_tuning(t));
+    SBF_TRY(check_tuning(t, query));
     uint64_t cw = std::max<uint64_t>(t.chunk_bytes > K ? t.chunk_bytes - (K - 1) : 1, 1024);
     if (kbits) cw = std::max<uint64_t>(cw / 32 * 32, 1024);
     const uint64_t n_chunks = (W + cw - 1) / cw;
@@ -559,7 +560,7 @@ static int resolve_tuning(const sbf_filter* f, bool query, uint64_t len, uint64_
     } else if (!tune_lookup(tune_key(f, query, len, n), out)) {
         *out = default_tuning(query);
     }
-    return check_tuning(*out);
+    return check_tuning(*out, query);
 }
 
 }  // namespace sbf
