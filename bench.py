@@ -64,17 +64,21 @@ def workload_spec(name: str, scale: float) -> dict:
                     rec_lo=int(13e6 * scale), rec_hi=int(21e6 * scale), gc=0.36,
                     features=dict(tandem_frac=0.03, n_run_frac=0.001),
                     bits_per_kmer=21.4, n_reads=int(20e6 * scale), read_len=150,
-                    positive_frac=0.5, sub_rate=0.01)
+                    positive_frac=0.5, sub_rate=0.01,
+                    l2="filter 256 MiB (about 2x L2); query input 3 GB, larger than L2 "
+                       "(no flush)")
     if name == "c1":
         return dict(name="plain-small", genome_bp=int(2e6 * scale), n_records=1,
                     rec_lo=int(2e6 * scale), rec_hi=int(2e6 * scale), gc=0.5, features={},
                     bits_per_kmer=85.7, n_reads=0, read_len=150, positive_frac=0.5,
-                    sub_rate=0.0, fresh_query_bp=int(2e6 * scale))
+                    sub_rate=0.0, fresh_query_bp=int(2e6 * scale),
+                    l2="L2-resident by design: 32 MiB filter and 2-4 MB inputs stay in L2 "
+                       "between steps (no flush); judged against L2 bandwidth")
     raise SystemExit(f"unknown config {name}")
 
 
 def build_host_genome(spec: dict, seed: int):
-    from cusbf_b200.synthetic import (genome_records, join_records, record_lengths,
+    from workloads.synthetic import (genome_records, join_records, record_lengths,
                                       uniform_dna)
 
     if spec["n_records"] == 1 and not spec["features"]:
@@ -129,6 +133,38 @@ def random_sector_rate(words_tensor, torch, n_reads: int = 1 << 26, reps: int = 
         best = ms if best is None else min(best, ms)
         del out
     return n_reads / (best / 1e3)
+
+
+def l2_copy_bandwidth(torch, dev, nbytes: int = 24 << 20, reps: int = 200) -> float:
+    """Bytes/s (read + write) of a device copy whose source and destination
+    (2 x 24 MiB) stay in L2: `reps` copies replayed as one CUDA graph, best
+    of 5 replays, CUDA events.  The denominator for L2-resident filters."""
+    a = torch.ones(nbytes, dtype=torch.uint8, device=dev)
+    b = torch.empty_like(a)
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        for _ in range(3):
+            b.copy_(a)
+    torch.cuda.current_stream(dev).wait_stream(side)
+    torch.cuda.synchronize(dev)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        for _ in range(reps):
+            b.copy_(a)
+    g.replay()
+    torch.cuda.synchronize(dev)
+    best = None
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.replay()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del g
+    return 2 * nbytes * reps / (best / 1e3)
 
 
 def valid_windows(seq: np.ndarray) -> int:
@@ -211,9 +247,73 @@ class ClockSampler:
 # Reference arm: the reference's arithmetic on the host cores
 # ---------------------------------------------------------------------------
 
-def cpu_reference_run(joined: np.ndarray, reads_joined: np.ndarray | None, n_shards: int,
-                      steps: int, warmup: int, sample_bp: int, sample_reads_bytes: int,
-                      threads: int) -> dict:
+CPU_SAMPLE_BP = 32_000_000
+CPU_SAMPLE_READS = 80_000
+CPU_BASELINE_STEPS = 20
+
+
+def cpu_sample(spec: dict, joined: np.ndarray, seed: int) -> tuple[np.ndarray, np.ndarray]:
+    """The bounded sample of a plain workload that both CPU legs time (the
+    main arm's cpu_baseline and --impl reference): the first CPU_SAMPLE_BP
+    bytes of the joined genome, and CPU_SAMPLE_READS reads of the workload's
+    length drawn from that prefix (same positive share and substitution
+    rate), joined with separators.  Without reads (the small plain workload)
+    the query is the workload's own: genome + separator + fresh sequence."""
+    from workloads.synthetic import SEPARATOR, reads_host, uniform_dna
+
+    ins = joined[:min(joined.size, CPU_SAMPLE_BP)]
+    if spec["n_reads"] > 0:
+        rl = spec["read_len"]
+        rd = reads_host([ins], CPU_SAMPLE_READS, rl, seed=seed + 7, sub_rate=spec["sub_rate"],
+                        positive_frac=spec["positive_frac"])
+        q = np.full((CPU_SAMPLE_READS, rl + 1), SEPARATOR, dtype=np.uint8)
+        q[:, :-1] = rd
+        return ins, q.reshape(-1)[:-1]
+    fresh = uniform_dna(spec["fresh_query_bp"], seed=1337, gc=spec["gc"])
+    return ins, np.concatenate([joined, np.frombuffer(b"N", np.uint8), fresh])
+
+
+def query_counts(spec: dict, joined: np.ndarray) -> tuple[int, int]:
+    """(valid k-mers, windows) of the workload's query input, computed on the
+    host: reads of one length joined by one separator, or (small plain
+    workload) genome + separator + fresh sequence."""
+    if spec["n_reads"] > 0:
+        rl = spec["read_len"]
+        n_bytes = spec["n_reads"] * (rl + 1) - 1
+        return spec["n_reads"] * max(0, rl - K + 1), max(0, n_bytes - K + 1)
+    from workloads.synthetic import uniform_dna
+
+    fresh = uniform_dna(spec["fresh_query_bp"], seed=1337, gc=spec["gc"])
+    q = np.concatenate([joined, np.frombuffer(b"N", np.uint8), fresh])
+    return valid_windows(q), max(0, q.size - K + 1)
+
+
+def plain_config(spec: dict, world: int, filter_bits: int, n_ins_valid: int, n_q_valid: int,
+                 n_q_windows: int) -> dict:
+    """The `config` object of a plain workload's JSON line (both arms)."""
+    if spec["n_reads"] > 0:
+        query = f"{spec['n_reads']:,} x {spec['read_len']} bp reads queried"
+    else:
+        query = (f"the same {spec['genome_bp'] / 1e6:.3g} Mbp + a fresh "
+                 f"{spec['fresh_query_bp'] / 1e6:.3g} Mbp queried")
+    return {
+        "workload": f"{spec['name']}: {spec['genome_bp'] / 1e9:.3g} Gbp in "
+                    f"{spec['n_records']} records inserted, {query}",
+        "k": K, "s": S, "m": M, "hashes": H, "filter_bits": int(filter_bits),
+        "bits_per_kmer_requested": spec["bits_per_kmer"],
+        "insert_kmers": int(n_ins_valid), "query_kmers": int(n_q_valid),
+        "query_windows": int(n_q_windows), "parallelism": f"replicas x{world} (weak)",
+        "l2": spec.get("l2", "inputs larger than L2 (no flush needed)"),
+        "step": "clear (untimed memset inside the step) + insert launch + query launch",
+    }
+
+
+def cpu_reference_run(ins: np.ndarray, qry: np.ndarray, n_shards: int, steps: int,
+                      warmup: int, threads: int) -> dict:
+    """Times the reference's own arithmetic (oracle/_ref, else the C port)
+    inserting `ins` into an empty filter of `n_shards` shards and querying
+    `qry` against it, `steps` times after `warmup`, on `threads` host
+    threads."""
     from oracle import oracle as o
 
     if o.RefCpu.available():
@@ -224,8 +324,6 @@ def cpu_reference_run(joined: np.ndarray, reads_joined: np.ndarray | None, n_sha
     else:
         impl, kind = o.Oracle(K, S, M, H, threads=threads), "port"
         desc = "oracle/sbf_oracle.c: C restatement of the reference semantics, pthreads"
-    ins = joined[:sample_bp]
-    qry = reads_joined[:sample_reads_bytes] if reads_joined is not None else joined[:sample_bp]
     n_ins = valid_windows(ins)
     n_q = valid_windows(qry)
     words = np.zeros(n_shards * 4, dtype=np.uint64)
@@ -244,7 +342,7 @@ def cpu_reference_run(joined: np.ndarray, reads_joined: np.ndarray | None, n_sha
                        f"{qry.size / 1e6:.1f} MB of joined reads queried "
                        f"({n_ins + n_q:,} valid k-mers) per step, filter {n_shards * 32 >> 20} MiB; "
                        + desc,
-                ms_per_step=per * 1e3, kmers_per_step=n_ins + n_q)
+                ms_per_step=per * 1e3, kmers_per_step=n_ins + n_q, steps=len(times))
 
 
 def host_cores() -> int:
@@ -281,7 +379,7 @@ def run_ragged(args, world: int, rank: int, local_rank: int) -> None:
     / contains_sequence_async per record, the reference's only per-record
     form) on a sample, and end to end with the reference's single-launch
     record batch (host normalisation + one launch)."""
-    from cusbf_b200.synthetic import lognormal_lengths, ragged_reads_device, uniform_dna
+    from workloads.synthetic import lognormal_lengths, ragged_reads_device, uniform_dna
 
     spec = ragged_spec(args.scale)
     seed = args.seed + 1000 * rank
@@ -580,7 +678,7 @@ def run_served(args, world: int, rank: int, local_rank: int) -> None:
     import torch
 
     import cusbf_b200 as sbf
-    from cusbf_b200.synthetic import reads_device, uniform_dna
+    from workloads.synthetic import reads_device, uniform_dna
 
     scale = args.scale
     spec = workload_spec("c2", 1.0)
@@ -864,7 +962,7 @@ def main() -> None:
     n_shards = f.num_shards()
 
     d_genome = torch.from_numpy(joined).to(dev)
-    from cusbf_b200.synthetic import SEPARATOR, reads_device, uniform_dna
+    from workloads.synthetic import SEPARATOR, reads_device, uniform_dna
 
     if spec["n_reads"] > 0:
         reads = reads_device(d_genome, spec["n_reads"], spec["read_len"],
@@ -926,7 +1024,9 @@ def main() -> None:
     ms_per_step = total_ms / args.steps
     value = whole_job_rate(world, kmers_step, ms_per_step)
 
-    # Parity spot check of this run against the oracle on a slice.
+    # Positive windows of the device-resident query: the end-to-end forms
+    # below must return the same count (bit-exact parity with the reference
+    # at this size is a GPU test, not part of the timed arm).
     positives = int(d_out.sum(dtype=torch.int64).item())
 
     # End-to-end through the host API with pinned buffers.
@@ -1091,35 +1191,44 @@ def main() -> None:
                 "insert": {"achieved": round(i_achieved, 1), "frac": round(i_achieved / peak, 4),
                            "algorithmic_bytes": int(i_bytes), "traffic": i_traffic,
                            "model": f"L + 64R (R/N={r_per_i:.4f} counted on a 6 Mbp sample)"}}
+    roofline_other = None
+    if args.config != "c3" or args.scale != 1.0:
+        # The committed DRAM bytes per window come from the 3.1 Gbp capture.
+        roofline["traffic"] = None
+        roofline["insert"]["traffic"] = None
+    if args.config in ("c1", "c2"):
+        # L2-resident (c1) or L2-straddling (c2) filters: the same algorithmic
+        # bytes against the L2 copy bandwidth measured live.
+        l2_peak = l2_copy_bandwidth(torch, dev) / 1e9
+        l2_roof = dict(roofline, bound="l2", peak=round(l2_peak, 1),
+                       frac=round(q_achieved / l2_peak, 4),
+                       peak_source="measured live: L2-resident device copy (2 x 24 MiB, 200 "
+                                   "copies in one CUDA graph, read + write bytes)",
+                       insert=dict(roofline["insert"], frac=round(i_achieved / l2_peak, 4)))
+        if args.config == "c1":
+            roofline, roofline_other = l2_roof, ("roofline_hbm", roofline)
+        else:
+            roofline_other = ("roofline_l2", l2_roof)
 
     cpu = None
     if not args.no_cpu_baseline:
-        cpu = cpu_reference_run(joined, q_sample, n_shards, steps=2, warmup=1,
-                                sample_bp=min(joined.size, 8_000_000),
-                                sample_reads_bytes=min(q_sample.size, 3_000_000),
+        c_ins, c_qry = cpu_sample(spec, joined, args.seed)
+        cpu = cpu_reference_run(c_ins, c_qry, n_shards, steps=CPU_BASELINE_STEPS, warmup=1,
                                 threads=host_cores())
-        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample", "steps")}
 
     line = {
         "metric": METRIC, "value": value, "unit": "k-mers/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded stand-in with the configuration's shapes; no public genome)",
-        "config": {
-            "workload": f"{spec['name']}: {spec['genome_bp'] / 1e9:.3g} Gbp in "
-                        f"{spec['n_records']} records inserted, {spec['n_reads']:,} x "
-                        f"{spec['read_len']} bp reads queried",
-            "k": K, "s": S, "m": M, "hashes": H, "filter_bits": f.filter_bits(),
-            "bits_per_kmer_requested": spec["bits_per_kmer"],
-            "insert_kmers": n_ins_valid, "query_kmers": n_q_valid,
-            "query_windows": n_q_windows, "parallelism": f"replicas x{world} (weak)",
-            "l2": "inputs larger than L2 (no flush needed)",
-            "step": "clear (untimed memset inside the step) + insert launch + query launch",
-        },
+        "config": plain_config(spec, world, f.filter_bits(), n_ins_valid, n_q_valid,
+                               n_q_windows),
         "insert": {"ms": ins_ms, "kmers_per_s": n_ins_valid / (ins_ms / 1e3)},
         "query": {"ms": q_ms, "kmers_per_s": n_q_valid / (q_ms / 1e3),
                   "positives": positives},
         "roofline": roofline,
+        **(dict([roofline_other]) if roofline_other else {}),
         "sector_roofline": sector,
         "cpu_baseline": cpu,
         "e2e": e2e,
@@ -1147,6 +1256,13 @@ def main() -> None:
         line["served_dense_bits"] = run_form(["--config", "c5", "--duration", "2.0",
                                               "--server-dense", "--server-bits", "--no-serial"],
                                              summarize_served)
+        line["c1"] = run_form(["--config", "c1", "--steps", "20", "--warmup", "5"],
+                              summarize_plain)
+        line["c2"] = run_form(["--config", "c2", "--steps", "10", "--warmup", "3"],
+                              summarize_plain)
+        # Last, so that it stays in the tail of the line: the headline figures
+        # of every configuration in a few hundred bytes.
+        line["summary"] = compact_summary(line)
     print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -1185,6 +1301,58 @@ def summarize_ragged(d: dict) -> dict:
             "record_batch_e2e_kmers_per_s": rb.get("value")}
 
 
+def summarize_plain(d: dict) -> dict:
+    """Summary of a plain-configuration line (c1, c2) for the default run."""
+    out = {"metric": d["metric"], "workload": d["config"]["workload"],
+           "filter_bits": d["config"]["filter_bits"], "l2": d["config"]["l2"],
+           "kmers_per_s": d["value"], "insert_kmers_per_s": d["insert"]["kmers_per_s"],
+           "query_kmers_per_s": d["query"]["kmers_per_s"], "ms_per_step": d["ms_per_step"],
+           "steps": d["steps"], "warmup": d["warmup"],
+           "e2e_kmers_per_s": (d.get("e2e") or {}).get("value"),
+           "cpu_baseline": d.get("cpu_baseline")}
+    for key in ("roofline", "roofline_l2", "roofline_hbm"):
+        r = d.get(key)
+        if r:
+            out[key] = {"bound": r["bound"], "achieved": r["achieved"], "peak": r["peak"],
+                        "unit": r["unit"], "frac": r["frac"], "insert_frac": r["insert"]["frac"],
+                        "peak_source": r["peak_source"]}
+    return out
+
+
+def compact_summary(line: dict) -> dict:
+    """Headline numbers of the default run, G k-mers/s unless named."""
+    def g(x):
+        return None if x is None else round(x / 1e9, 2)
+
+    out = {"c3": {"gkmers": g(line["value"]), "ins": g(line["insert"]["kmers_per_s"]),
+                  "qry": g(line["query"]["kmers_per_s"]), "e2e": g((line.get("e2e") or {}).get("value")),
+                  "frac_hbm": line["roofline"]["frac"],
+                  "sector_frac_q": line["sector_roofline"]["query_frac"]}}
+    for c in ("c1", "c2"):
+        d = line.get(c) or {}
+        if "kmers_per_s" in d:
+            out[c] = {"gkmers": g(d["kmers_per_s"]), "ins": g(d["insert_kmers_per_s"]),
+                      "qry": g(d["query_kmers_per_s"]), "e2e": g(d.get("e2e_kmers_per_s")),
+                      "frac": (d.get("roofline") or {}).get("frac"),
+                      "bound": (d.get("roofline") or {}).get("bound")}
+            if "roofline_l2" in d:
+                out[c]["frac_l2"] = d["roofline_l2"]["frac"]
+    rb = line.get("ragged_batch") or {}
+    if "kmers_per_s" in rb:
+        out["c4"] = {"gkmers": g(rb["kmers_per_s"]), "e2e": g(rb.get("e2e_kmers_per_s")),
+                     "e2e_tuned": g(rb.get("e2e_tuned_kmers_per_s")),
+                     "plain_per_record": g(rb.get("plain_per_record_kmers_per_s")),
+                     "speedup_vs_plain": rb.get("speedup_vs_plain_per_record"),
+                     "identical": rb.get("plain_hits_identical")}
+    for key in ("served", "served_bits", "served_counts", "served_dense_bits"):
+        sv = line.get(key) or {}
+        if "latency_ms" in sv:
+            lat = sv["latency_ms"]
+            out[key] = {"req_s": round(sv["requests_per_s"]), "p50_ms": round(lat["p50"], 2),
+                        "p99_ms": round(lat["p99"], 2), "p999_ms": round(lat["p999"], 2)}
+    return out
+
+
 def summarize_served(d: dict) -> dict:
     sv, one, pl = d["served"], d.get("one_request_per_launch") or {}, d["plain_per_record"]
     return {"metric": d["metric"], "workload": d["config"]["workload"],
@@ -1201,32 +1369,17 @@ def summarize_served(d: dict) -> dict:
 
 def run_reference_arm(args, spec, world) -> None:
     """The reference's own CPU implementation of the path (rank 0 only), on
-    a bounded sample: the start of the workload's first genome record and
-    20,000 reads sampled from it, with the full workload's filter size."""
-    from cusbf_b200.synthetic import (SEPARATOR, genome_record, reads_host, record_lengths,
-                                      uniform_dna)
+    the bounded sample that the main arm's cpu_baseline also times
+    (cpu_sample), with the full workload's filter size and the main arm's
+    `config`.  Nothing here loads the engine's library."""
     from oracle.oracle import num_shards
 
-    if spec["n_records"] == 1 and not spec["features"]:
-        joined = uniform_dna(spec["genome_bp"], seed=args.seed, gc=spec["gc"])
-    else:
-        lens = record_lengths(spec["genome_bp"], spec["n_records"], spec["rec_lo"],
-                              spec["rec_hi"], seed=args.seed)
-        joined = genome_record(0, min(lens[0], 8_000_000), args.seed, gc=spec["gc"],
-                               **spec["features"])
-    n_valid_full = spec["genome_bp"] - spec["n_records"] * (K - 1)
-    shards = num_shards(int(round(spec["bits_per_kmer"] * n_valid_full)))
-    reads_joined = None
-    if spec["n_reads"] > 0:
-        n = min(spec["n_reads"], 20_000)
-        rd = reads_host([joined], n, spec["read_len"], seed=args.seed + 7,
-                        sub_rate=spec["sub_rate"], positive_frac=spec["positive_frac"])
-        q = np.full((n, spec["read_len"] + 1), SEPARATOR, dtype=np.uint8)
-        q[:, :-1] = rd
-        reads_joined = q.reshape(-1)[:-1]
-    res = cpu_reference_run(joined, reads_joined, shards, steps=args.steps,
-                            warmup=args.warmup, sample_bp=min(joined.size, 4_000_000),
-                            sample_reads_bytes=reads_joined.size if reads_joined is not None else 0,
+    joined, _, n_ins_valid = build_host_genome(spec, seed=args.seed)
+    requested = int(round(spec["bits_per_kmer"] * n_ins_valid))
+    shards = num_shards(requested)
+    n_q_valid, n_q_windows = query_counts(spec, joined)
+    c_ins, c_qry = cpu_sample(spec, joined, args.seed)
+    res = cpu_reference_run(c_ins, c_qry, shards, steps=args.steps, warmup=args.warmup,
                             threads=host_cores())
     line = {
         "metric": METRIC, "value": res["value"], "unit": "k-mers/s", "impl": "reference",
@@ -1234,19 +1387,18 @@ def run_reference_arm(args, spec, world) -> None:
         "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded stand-in with the configuration's shapes; no public genome)",
-        "config": {"workload": f"{spec['name']}: bounded sample per step (see cpu_baseline)",
-                   "k": K, "s": S, "m": M, "hashes": H, "filter_shards": shards},
+        "config": plain_config(spec, world, shards * 256, n_ins_valid, n_q_valid, n_q_windows),
         "cpu_baseline": {"value": res["value"], "unit": "k-mers/s", "cores": res["cores"],
                          "kind": res["kind"], "sample": res["sample"]},
         "e2e": {"value": res["value"], "unit": "k-mers/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     if not args.no_reference_gpu:
-        line["reference_gpu"] = reference_gpu_run(args, spec)
+        line["reference_gpu"] = reference_gpu_run(args, spec, joined, n_ins_valid)
     print(json.dumps(line), flush=True)
 
 
-def reference_gpu_run(args, spec) -> dict:
+def reference_gpu_run(args, spec, joined: np.ndarray, n_ins_valid: int) -> dict:
     """The unmodified reference cuSBF GPU path (oracle/_ref, compiled from the
     reference headers) on this workload at full size, device-resident inputs,
     timed like the main arm: insert_sequence_async over the genome joined with
@@ -1257,9 +1409,8 @@ def reference_gpu_run(args, spec) -> dict:
         return {"unavailable": "oracle/_ref/libsbf_refgpu.so was not built"}
     import torch
 
-    from cusbf_b200.synthetic import SEPARATOR, reads_device, uniform_dna
+    from workloads.synthetic import SEPARATOR, reads_device, uniform_dna
 
-    joined, _, n_ins_valid = build_host_genome(spec, seed=args.seed)
     dev = torch.device("cuda", 0)
     d_genome = torch.from_numpy(joined).to(dev)
     if spec["n_reads"] > 0:

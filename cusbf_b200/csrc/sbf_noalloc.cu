@@ -2,11 +2,14 @@
 // allocation: sbf_record_batch_counts_noalloc.
 //
 // For callers that may not allocate device memory at call time: a serving
-// loop or a capture-replay caller whose memory is fixed up front, or an
-// allocator hook that must not re-enter the CUDA allocator.  The other record
-// batch entry points keep grow-only device buffers inside the filter and may
-// cudaMalloc when a batch is larger than any before it; this one uses only a
-// fixed 8 MiB scratch area compiled into the library.
+// loop whose device memory is reserved once at start-up and must not grow
+// while requests are in flight, or an allocator hook that must not re-enter
+// the CUDA allocator it is part of.  The other record batch entry points keep
+// grow-only device buffers inside the filter and may cudaMalloc when a batch
+// is larger than any before it; this one uses only a fixed 8 MiB scratch area
+// compiled into the library.  It is synchronous: it copies the caller's host
+// range table in and the counts out, and returns once its stream has reached
+// the end of the call.
 //
 // The counts are those of the reference's valid_record_kmer_count
 // (include/cusbf/normalized_record_batch.hpp:88-110) and
@@ -105,7 +108,10 @@ int scratch_for(int device, void** out) {
             return cuda_fail(e, "cudaSetDevice");
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_count_scratch);
-        if (current != device) cudaSetDevice(current);
+        if (current != device) {
+            const cudaError_t r = cudaSetDevice(current);
+            if (r != cudaSuccess) return cuda_fail(r, "cudaSetDevice (restoring the caller's device)");
+        }
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_count_scratch)");
         g_scratch_ptr[device] = p;
     }
@@ -142,14 +148,23 @@ extern "C" int sbf_record_batch_counts_noalloc(const sbf_filter_t* f, const char
     const uint64_t windows = f->kmers_of(len);
     if (d_hits && hits_len < windows)
         return set_error(SBF_ERR_INVALID_ARGUMENT, "hit span is shorter than the batch's windows");
+    // The scratch address and the launch below belong to the filter's device,
+    // so that device must be the caller's current one.
+    int current = -1;
+    cudaError_t e = cudaGetDevice(&current);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (current != f->device)
+        return set_error(SBF_ERR_INVALID_ARGUMENT,
+                         "sbf_record_batch_counts_noalloc: the current device (%d) is not the "
+                         "filter's device (%d)",
+                         current, f->device);
     void* scratch = nullptr;
     if ((s = scratch_for(f->device, &scratch)) != SBF_OK) return s;
     auto* d_ranges = static_cast<sbf_record_range*>(scratch);
     auto* d_valid = reinterpret_cast<unsigned long long*>(d_ranges + n);
     auto* d_pos = d_valid + n;
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    cudaError_t e =
-        cudaMemcpyAsync(d_ranges, ranges, n * sizeof(sbf_record_range), cudaMemcpyHostToDevice, st);
+    e = cudaMemcpyAsync(d_ranges, ranges, n * sizeof(sbf_record_range), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync(ranges)");
     const uint64_t warps = n < static_cast<uint64_t>(f->sms) * 64 ? n : static_cast<uint64_t>(f->sms) * 64;
     record_counts_kernel<<<static_cast<unsigned>((warps * 32 + 255) / 256), 256, 0, st>>>(

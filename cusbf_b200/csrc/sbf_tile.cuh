@@ -766,11 +766,17 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
         const uint32_t parity = (it >> 1) & 1u;
         const bool ok = mbar_wait_bounded(&bars[b], parity);
         if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicExch(p.err, kDevErrStageTimeout);
-            // Give the other buffer's copy (if any) a bounded chance to land
-            // before the CTA's shared memory is released.
-            if (tiles[(it + 1) % 3] < p.n_tiles)
-                (void)mbar_wait_bounded(&bars[b ^ 1], ((it + 1) >> 1) & 1u);
+            // Both staging buffers may still have a bulk copy in flight:
+            // this tile's (whose wait ran out) and the next tile's.  Give
+            // each one more bounded wait before the CTA's shared memory is
+            // released, so no copy lands in memory a later CTA owns.
+            if (tid == 0) {
+                atomicExch(p.err, kDevErrStageTimeout);
+                (void)mbar_wait_bounded(&bars[b], parity);
+                if (tiles[(it + 1) % 3] < p.n_tiles)
+                    (void)mbar_wait_bounded(&bars[b ^ 1], ((it + 1) >> 1) & 1u);
+            }
+            __syncthreads();
             if constexpr (!kQuery) flush_ring_drain();
             return;
         }

@@ -334,17 +334,22 @@ int sbf_contains_record_batch_async(const sbf_filter_t* filter, const char* d_se
  * (count_positive_kmers_per_record, detail/count_positive_kmers.cuh:21-45);
  * positive_out[i] = 0 without d_hits.  Both outputs are host arrays of n.
  *
- * For callers that may not allocate device memory at call time (a serving
- * loop or a capture-replay caller whose memory is fixed up front, an
- * allocator hook that must not re-enter the CUDA allocator): the other
- * record-batch entry points may grow device buffers inside the filter, this
- * one only uses an 8 MiB scratch area compiled into the library, and calls
- * no cudaMalloc or cudaFree.  Limit: n <= 262144 records; larger batches
- * return SBF_ERR_INVALID_ARGUMENT.  The first call on a device looks the
- * scratch address up (cudaGetSymbolAddress, with that device made current),
- * so make it before any stream capture.  Calls share the scratch: calls on
- * one device must not overlap (serialise them on one stream or host thread),
- * or they race.  Returns after the stream has reached the end of the call. */
+ * For callers that may not allocate device memory at call time: a serving
+ * loop whose device memory is reserved once at start-up and must not grow
+ * while requests are in flight, or an allocator hook that must not re-enter
+ * the CUDA allocator it belongs to.  The other record-batch entry points may
+ * grow device buffers inside the filter; this one only uses an 8 MiB scratch
+ * area compiled into the library (held by every device that loads the
+ * library until the process exits), and calls no cudaMalloc or cudaFree.
+ * Limit: n <= 262144 records; larger batches return
+ * SBF_ERR_INVALID_ARGUMENT.  The filter's device must be the current device
+ * (else SBF_ERR_INVALID_ARGUMENT).  The first call on a device looks the
+ * scratch address up (cudaGetSymbolAddress), so make that first call before
+ * any stream capture.  Calls share the scratch, which keeps the last call's
+ * contents: calls on one device must not overlap on the GPU (serialise them
+ * on one stream or host thread), or they race.  The call is synchronous: it
+ * copies `ranges` from host memory, copies the counts back to the host
+ * arrays, and returns after the stream has reached the end of the call. */
 int sbf_record_batch_counts_noalloc(const sbf_filter_t* filter, const char* d_seq, uint64_t len,
                                     const sbf_record_range* ranges, uint64_t n,
                                     const uint8_t* d_hits, uint64_t hits_len,

@@ -54,7 +54,7 @@ def sha(a: np.ndarray) -> str:
 def plain_small_inputs():
     """The plain-method small workload: one 2 Mbp uniform ACGT record (seed
     42), queried with itself plus a fresh 2 Mbp record (seed 1337)."""
-    from cusbf_b200.synthetic import uniform_dna
+    from workloads.synthetic import uniform_dna
 
     ins = uniform_dna(2_000_000, seed=42)
     fresh = uniform_dna(2_000_000, seed=1337)
@@ -100,7 +100,7 @@ def main() -> None:
         "set_bits": int(np.unpackbits(w.view(np.uint8)).sum()),
     }
 
-    from cusbf_b200.synthetic import genome_records, join_records
+    from workloads.synthetic import genome_records, join_records
 
     recs = genome_records(total_bp=20_000_000, n_records=3, seed=7, gc=0.36,
                           tandem_frac=0.03, n_run_frac=0.001)

@@ -118,7 +118,7 @@ def _sha(a):
 
 def test_golden_digest_plain_small(oracle_mod):
     """The plain-method small workload (2 Mbp, 85.7 bits/k-mer) digests."""
-    from cusbf_b200.synthetic import uniform_dna
+    from workloads.synthetic import uniform_dna
 
     d = json.load(open(os.path.join(GOLDEN, "digests.json")))["plain_small"]
     ins = uniform_dna(2_000_000, seed=42)

@@ -57,7 +57,7 @@ def _compare(sbf, torch, refgpu, cfg_id, cfg, bits, d_ins, d_qry):
 def test_plain_small_workload(sbf, cuda, refgpu):
     """2 Mbp uniform record at 85.7 bits per k-mer; query it plus a fresh 2 Mbp."""
     torch = cuda
-    from cusbf_b200.synthetic import uniform_dna
+    from workloads.synthetic import uniform_dna
 
     ins = uniform_dna(2_000_000, seed=42)
     qry = np.concatenate([ins, np.frombuffer(b"N", np.uint8), uniform_dna(2_000_000, seed=1337)])
@@ -70,7 +70,7 @@ def test_genome_like_with_repeats_and_n_runs(sbf, cuda, refgpu):
     """Records with tandem repeats, interspersed repeat copies and N runs,
     joined with separators; reads with substitutions joined with separators."""
     torch = cuda
-    from cusbf_b200.synthetic import SEPARATOR, genome_records, join_records, reads_device
+    from workloads.synthetic import SEPARATOR, genome_records, join_records, reads_device
 
     recs = genome_records(24_000_000, 4, seed=5, gc=0.38, tandem_frac=0.03, n_run_frac=0.001,
                           interspersed_frac=0.3, processes=1)
