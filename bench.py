@@ -649,6 +649,100 @@ SERVED_METRIC = ("served k-mers/s and p50/p99/p999 latency, Poisson 20k req/s (l
                  "1-100k x 150 bp reads, 5% inserts of 1-10 Mbp) on the resident 100 Mbp filter")
 
 
+FASTX_METRIC = ("GB/s of FASTA insert and FASTQ query from files, parsed on the GPU, each block "
+                "replayed as one CUDA graph vs stream launches vs the host parser")
+
+
+def run_fastx_files(args) -> None:
+    """FASTA insert (100 Mbp genome, 80-column lines) and FASTQ query (4M x
+    150 bp reads, half sampled from the genome with 1% substitutions) through
+    insert_fastx_file / query_fastx_file, with the GPU parser replaying each
+    block as one CUDA graph, with stream launches, and with the host parser.
+    Reports and filter words must agree across the three."""
+    import tempfile
+
+    import torch
+
+    import cusbf_b200 as sbf
+    from workloads.synthetic import reads_device, uniform_dna
+
+    n_reads = max(int(4_000_000 * args.scale), 1000)
+    genome = uniform_dna(max(int(100_000_000 * args.scale), 10_000), seed=args.seed, gc=0.41)
+    dev = torch.device("cuda", 0)
+    d_genome = torch.from_numpy(genome).to(dev)
+    reads = reads_device(d_genome, n_reads, 150, seed=args.seed + 7, sub_rate=0.01,
+                         positive_frac=0.5, device=str(dev)).cpu().numpy()
+    del d_genome
+    rec = np.empty((n_reads, 307), np.uint8)  # "@r\n" seq "\n+\n" qual "\n"
+    rec[:, 0:3] = np.frombuffer(b"@r\n", np.uint8)
+    rec[:, 3:153] = reads
+    rec[:, 153:156] = np.frombuffer(b"\n+\n", np.uint8)
+    rec[:, 156:306] = ord("I")
+    rec[:, 306] = ord("\n")
+    width = 80
+    n_lines = -(-genome.size // width)
+    fa = np.full(n_lines * (width + 1), ord("\n"), np.uint8)
+    body = fa[:n_lines * (width + 1)].reshape(n_lines, width + 1)
+    pad = np.zeros(n_lines * width, np.uint8)
+    pad[:genome.size] = genome
+    body[:, :width] = pad.reshape(n_lines, width)
+    tail = n_lines * width - genome.size
+    fa_bytes = b">genome\n" + (fa.tobytes()[:-(tail + 1)] + b"\n" if tail else fa.tobytes())
+    results = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        fq_path, fa_path = os.path.join(tmp, "reads.fq"), os.path.join(tmp, "genome.fa")
+        rec.tofile(fq_path)
+        with open(fa_path, "wb") as fh:
+            fh.write(fa_bytes)
+        fq_bytes, fa_size = os.path.getsize(fq_path), os.path.getsize(fa_path)
+        bits = 1 << 31
+        for mode in ("graph", "stream", "host"):
+            os.environ["SBF_FASTX_PARSER"] = "host" if mode == "host" else "device"
+            os.environ["SBF_FASTX_GRAPH"] = "1" if mode == "graph" else "0"
+            f = sbf.Filter(bits, k=K, s=S, m=M, hashes=H)
+            ins_t, q_t = [], []
+            for rep_i in range(1 + max(args.steps, 1)):
+                f.clear()
+                torch.cuda.synchronize(dev)
+                t0 = time.perf_counter()
+                irep = f.insert_fastx_file(fa_path)
+                t1 = time.perf_counter()
+                qrep = f.query_fastx_file(fq_path)
+                t2 = time.perf_counter()
+                if rep_i:
+                    ins_t.append(t1 - t0)
+                    q_t.append(t2 - t1)
+            words = f.words_host()
+            f.close()
+            results[mode] = {"insert_gb_per_s": fa_size / min(ins_t) / 1e9,
+                             "query_gb_per_s": fq_bytes / min(q_t) / 1e9,
+                             "insert_kmers_per_s": irep.inserted_kmers / min(ins_t),
+                             "query_kmers_per_s": qrep.queried_kmers / min(q_t),
+                             "insert_report": irep.as_dict(), "query_report": qrep.as_dict(),
+                             "_words": words}
+        os.environ.pop("SBF_FASTX_PARSER", None)
+        os.environ.pop("SBF_FASTX_GRAPH", None)
+    same = all(results[m]["insert_report"] == results["graph"]["insert_report"] and
+               results[m]["query_report"] == results["graph"]["query_report"] and
+               np.array_equal(results[m]["_words"], results["graph"]["_words"])
+               for m in ("stream", "host"))
+    for m in results:
+        results[m].pop("_words")
+    g = results["graph"]
+    line = {"metric": FASTX_METRIC, "value": g["query_gb_per_s"], "unit": "GB/s",
+            "n_gpus": 1, "steps": max(args.steps, 1), "warmup": 1, "higher_is_better": True,
+            "dtype": "u8", "data": "synthetic (seeded genome and reads written to files)",
+            "config": {"workload": f"FASTA insert of {genome.size / 1e6:.0f} Mbp "
+                                   f"({fa_size / 1e6:.0f} MB, {width}-column lines), FASTQ query "
+                                   f"of {n_reads:,} x 150 bp reads ({fq_bytes / 1e9:.2f} GB)",
+                       "filter_bits": bits, "block_bytes": "256 MiB (SBF_FASTQ_BLOCK_BYTES)",
+                       "timing": "host wall clock around each file call, best of the steps"},
+            "graph": g, "stream": results["stream"], "host_parser": results["host"],
+            "graph_vs_stream_query": g["query_gb_per_s"] / results["stream"]["query_gb_per_s"],
+            "identical_across_paths": bool(same)}
+    print(json.dumps(line), flush=True)
+
+
 def _poisson_schedule(seed: int, rate: float, duration: float, pool_reads: int,
                       ins_pool: int, scale: float):
     """Arrival offsets (s), insert flags, reads per query, first read, insert
@@ -879,7 +973,7 @@ def main() -> None:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4", "c5", "fastx"])
     ap.add_argument("--duration", type=float, default=2.0, help="c5: seconds of arrivals")
     ap.add_argument("--server-inflight", type=int, default=0, help="c5: batches in flight")
     ap.add_argument("--server-batch-mb", type=int, default=0, help="c5: batch cap in MiB")
@@ -920,6 +1014,15 @@ def main() -> None:
                                              "batch) are inside the c4 line"}))
             return
         run_ragged(args, world, rank, local_rank)
+        return
+    if args.config == "fastx":
+        if args.impl == "reference" or rank != 0:
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "metric": FASTX_METRIC,
+                                  "unavailable": "the reference parses FASTA/FASTQ on the host; "
+                                                 "its parser is the host-parser leg of this line"}))
+            return
+        run_fastx_files(args)
         return
     if args.config == "c5":
         if args.impl == "reference" or rank != 0:
@@ -1256,6 +1359,7 @@ def main() -> None:
         line["served_dense_bits"] = run_form(["--config", "c5", "--duration", "2.0",
                                               "--server-dense", "--server-bits", "--no-serial"],
                                              summarize_served)
+        line["fastx_files"] = run_form(["--config", "fastx", "--steps", "2"], summarize_fastx)
         line["c1"] = run_form(["--config", "c1", "--steps", "20", "--warmup", "5"],
                               summarize_plain)
         line["c2"] = run_form(["--config", "c2", "--steps", "10", "--warmup", "3"],
@@ -1319,6 +1423,15 @@ def summarize_plain(d: dict) -> dict:
     return out
 
 
+def summarize_fastx(d: dict) -> dict:
+    keep = ("insert_gb_per_s", "query_gb_per_s", "insert_kmers_per_s", "query_kmers_per_s")
+    return {"metric": d["metric"], "workload": d["config"]["workload"],
+            "graph": {k: d["graph"][k] for k in keep},
+            "stream": {k: d["stream"][k] for k in keep},
+            "host_parser": {k: d["host_parser"][k] for k in keep},
+            "identical_across_paths": d["identical_across_paths"]}
+
+
 def compact_summary(line: dict) -> dict:
     """Headline numbers of the default run, G k-mers/s unless named."""
     def g(x):
@@ -1344,6 +1457,10 @@ def compact_summary(line: dict) -> dict:
                      "plain_per_record": g(rb.get("plain_per_record_kmers_per_s")),
                      "speedup_vs_plain": rb.get("speedup_vs_plain_per_record"),
                      "identical": rb.get("plain_hits_identical")}
+    fx = line.get("fastx_files") or {}
+    if "graph" in fx:
+        out["fastx_gb_s"] = {m: [round(fx[m]["insert_gb_per_s"], 2), round(fx[m]["query_gb_per_s"], 2)]
+                             for m in ("graph", "stream", "host_parser")}
     for key in ("served", "served_bits", "served_counts", "served_dense_bits"):
         sv = line.get(key) or {}
         if "latency_ms" in sv:

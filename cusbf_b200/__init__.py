@@ -265,6 +265,9 @@ _sig("sbf_server_wait", C.c_int, _vp, _u64, C.c_double, C.POINTER(ServerRequestI
 _sig("sbf_server_drain", C.c_int, _vp)
 _sig("sbf_server_get_stats", C.c_int, _vp, C.c_int, C.POINTER(ServerStats))
 _sig("sbf_contains_sequence_bits_async", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp)
+_sig("sbf_emit_runs_async", C.c_int, _vp, _vp, _u64, _vp, _vp, _u64, _vp, _vp)
+_sig("sbf_apply_runs_async", C.c_int, _vp, _vp, _vp, _u64, _u64, _u64, _vp)
+_sig("sbf_filter_synchronize", C.c_int, _vp, _vp)
 _sig("sbf_contains_sequence_bits", C.c_int, _vp, _vp, _u64, _vp, _u64, _vp)
 _sig("sbf_expand_result_bits", C.c_int, _vp, _u64, _vp, _u32)
 _sig("sbf_host_expand_threads", C.c_int)
@@ -696,6 +699,48 @@ def _persist_methods():
 
 
 _persist_methods()
+
+
+def _sharded_methods():
+    """Device steps of the sharded multi-rank insert (cusbf_b200.sharded)."""
+
+    def emit_runs(self, d_seq, stream=None):
+        """Run records of the windows of device bytes `d_seq`: (shards int32
+        CUDA tensor (R,), masks int64 CUDA tensor (R, 4), valid windows)."""
+        import torch
+
+        p, n = _dev_ptr(d_seq)
+        dev = d_seq.device
+        cap = max(self.kmer_count(n) // 4 + 4096, 1)
+        count = torch.zeros(2, dtype=torch.int64, device=dev)
+        while True:
+            shards = torch.empty(cap, dtype=torch.int32, device=dev)
+            masks = torch.empty((cap, 4), dtype=torch.int64, device=dev)
+            _check(_lib.sbf_emit_runs_async(self._h, p, n, shards.data_ptr(), masks.data_ptr(),
+                                            cap, count.data_ptr(), _stream(stream)))
+            got = count.tolist()
+            if got[0] <= cap:
+                return shards[:got[0]], masks[:got[0]], int(got[1])
+            cap = got[0]
+
+    def apply_runs(self, d_shards, d_masks, shard_lo: int, shard_hi: int, stream=None) -> None:
+        """ORs device run records (int32 shards (R,), int64 masks (R, 4)) whose
+        shards lie in [shard_lo, shard_hi) into this filter."""
+        s, _ = _dev_ptr(d_shards)
+        m, mn = _dev_ptr(d_masks)
+        _check(_lib.sbf_apply_runs_async(self._h, s, m, mn // 32, shard_lo, shard_hi,
+                                         _stream(stream)))
+
+    def synchronize(self, stream=None) -> None:
+        """Waits for `stream`; raises on a device-side error of this filter."""
+        _check(_lib.sbf_filter_synchronize(self._h, _stream(stream)))
+
+    Filter.emit_runs = emit_runs
+    Filter.apply_runs = apply_runs
+    Filter.synchronize = synchronize
+
+
+_sharded_methods()
 
 
 def _ragged_methods():

@@ -194,7 +194,9 @@ int sbf_filter::check_device_error(cudaStream_t st) const {
     if (h_err != kDevErrNone) {
         cudaMemsetAsync(d_err, 0, sizeof(int), st);
         cudaStreamSynchronize(st);
-        return set_error(SBF_ERR_CUDA, "device error %d (staging wait timed out)", h_err);
+        return set_error(SBF_ERR_CUDA, "device error %d (%s)", h_err,
+                         h_err == kDevErrRecordRange ? "run record outside this rank's shard range"
+                                                     : "staging wait timed out");
     }
     return SBF_OK;
 }

@@ -195,8 +195,9 @@ __device__ __forceinline__ void bulk_g2s(void* smem_dst, const void* gmem_src, u
 
 __device__ __forceinline__ void load_shard(const uint64_t* p, uint64_t& w0, uint64_t& w1,
                                            uint64_t& w2, uint64_t& w3) {
-    // One 32-byte sector per shard, read with a single 256-bit load.
-    asm volatile("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];"
+    // One 32-byte sector per shard, read with a single 256-bit load; an L2
+    // miss fills 64 bytes (.L2::64B) instead of 128.
+    asm volatile("ld.global.nc.L2::64B.v4.u64 {%0, %1, %2, %3}, [%4];"
                  : "=l"(w0), "=l"(w1), "=l"(w2), "=l"(w3)
                  : "l"(p));
 }

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstring>
 
 #include "../../include/sbf_b200.h"
@@ -37,6 +38,15 @@ namespace sbf {
 namespace {
 
 constexpr int kScanThreads = 256;
+
+// A count that is either the host's `n` or, in a block replayed as a CUDA
+// graph, read on the device from `dn` and clamped to the buffer capacity.
+__device__ __forceinline__ uint64_t dev_count(uint64_t n, const unsigned long long* dn,
+                                              uint64_t cap) {
+    if (!dn) return n;
+    const uint64_t v = *dn;
+    return v < cap ? v : cap;
+}
 constexpr uint64_t kTileBytes = uint64_t{kScanThreads} * 256;  // 256 bytes per thread
 
 __device__ __forceinline__ uint32_t newlines_in(const uint8_t* t, uint64_t a, uint64_t b) {
@@ -83,8 +93,10 @@ __global__ void tile_newlines_kernel(const uint8_t* t, uint64_t n, uint64_t* til
 }
 
 // In-place exclusive scan of up to a few hundred thousand counts (one CTA).
-__global__ void scan_counts_kernel(uint64_t* v, uint64_t n, uint64_t* total) {
+__global__ void scan_counts_kernel(uint64_t* v, uint64_t n, uint64_t* total,
+                                   const unsigned long long* dn = nullptr, uint64_t cap = 0) {
     __shared__ uint64_t part[1024];
+    n = dev_count(n, dn, cap);
     const uint64_t per = (n + 1023) / 1024;
     const uint64_t a = threadIdx.x * per;
     const uint64_t b = a + per < n ? a + per : n;
@@ -107,8 +119,14 @@ __global__ void scan_counts_kernel(uint64_t* v, uint64_t n, uint64_t* total) {
     if (threadIdx.x == 1023) *total = part[1023];
 }
 
+enum : unsigned int { kIrregular = 1u, kLineOverflow = 2u };
+static_assert(kIrregular == kBlockIrregular && kLineOverflow == kBlockLineOverflow,
+              "device flags are the block summary's");
+
+// Newline positions in order; positions at or beyond `cap` are not stored
+// and set kLineOverflow (the caller grows line_end and repeats the block).
 __global__ void newline_positions_kernel(const uint8_t* t, uint64_t n, const uint64_t* tile_off,
-                                         uint64_t* line_end) {
+                                         uint64_t* line_end, uint64_t cap, unsigned int* flags) {
     __shared__ uint32_t sh[kScanThreads];
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kTileBytes;
     const uint64_t a = base + static_cast<uint64_t>(threadIdx.x) * 256;
@@ -117,16 +135,25 @@ __global__ void newline_positions_kernel(const uint8_t* t, uint64_t n, const uin
     uint32_t total;
     const uint32_t before = block_exclusive_scan(c, sh, &total);
     uint64_t out = tile_off[blockIdx.x] + before;
+    bool over = false;
     for (uint64_t x = a; x < b; ++x)
-        if (t[x] == '\n') line_end[out++] = x;
+        if (t[x] == '\n') {
+            if (out < cap)
+                line_end[out] = x;
+            else
+                over = true;
+            ++out;
+        }
+    if (over) atomicOr(flags, kLineOverflow);
 }
-
-enum : unsigned int { kIrregular = 1u };
 
 // One thread per record: lines 4r .. 4r+3.
 __global__ void fastq_records_kernel(const uint8_t* t, const uint64_t* line_end, uint64_t n_rec,
                                      DevRange* seq, DevRange* hdr, unsigned int* flags,
-                                     unsigned long long* bases) {
+                                     unsigned long long* bases,
+                                     const unsigned long long* dn_lines = nullptr,
+                                     uint64_t cap = 0) {
+    if (dn_lines) n_rec = dev_count(0, dn_lines, cap) / 4;
     unsigned long long local = 0;
     for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n_rec;
          r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
@@ -168,7 +195,9 @@ __device__ __forceinline__ bool fasta_line(const uint8_t* t, const uint64_t* lin
 // FASTA, one thread per line: sequence bytes of the line (0 for headers and
 // '\r') and a header flag ('>' at the line start).
 __global__ void fasta_lines_kernel(const uint8_t* t, const uint64_t* line_end, uint64_t n,
-                                   uint64_t* len, uint64_t* hdr) {
+                                   uint64_t* len, uint64_t* hdr,
+                                   const unsigned long long* dn = nullptr, uint64_t cap = 0) {
+    n = dev_count(n, dn, cap);
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         uint64_t a, b;
@@ -181,7 +210,9 @@ __global__ void fasta_lines_kernel(const uint8_t* t, const uint64_t* line_end, u
 // One warp per line: copies sequence lines to their compacted offsets
 // (`off`: exclusive scan of the line lengths).
 __global__ void fasta_compact_kernel(const uint8_t* t, const uint64_t* line_end, uint64_t n,
-                                     const uint64_t* off, uint8_t* comp) {
+                                     const uint64_t* off, uint8_t* comp,
+                                     const unsigned long long* dn = nullptr, uint64_t cap = 0) {
+    n = dev_count(n, dn, cap);
     const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
     const uint32_t lane = threadIdx.x & 31;
@@ -198,7 +229,11 @@ __global__ void fasta_compact_kernel(const uint8_t* t, const uint64_t* line_end,
 __global__ void fasta_records_kernel(const uint8_t* t, const uint64_t* line_end, uint64_t n,
                                      const uint64_t* off, const uint64_t* hdr_scan,
                                      uint64_t n_rec, DevRange* seq, DevRange* hdr,
-                                     unsigned long long* last) {
+                                     unsigned long long* last,
+                                     const unsigned long long* dn = nullptr, uint64_t cap = 0,
+                                     const unsigned long long* dn_rec = nullptr) {
+    n = dev_count(n, dn, cap);
+    if (dn_rec) n_rec = *dn_rec;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         uint64_t a, b;
@@ -215,12 +250,68 @@ __global__ void fasta_records_kernel(const uint8_t* t, const uint64_t* line_end,
 }
 
 // Record lengths once every record start is known.
-__global__ void fasta_lengths_kernel(DevRange* seq, uint64_t n_rec, uint64_t total_seq) {
+__global__ void fasta_lengths_kernel(DevRange* seq, uint64_t n_rec, uint64_t total_seq,
+                                     const unsigned long long* dn_rec = nullptr,
+                                     const unsigned long long* d_total = nullptr) {
+    if (dn_rec) n_rec = *dn_rec;
+    if (d_total) total_seq = *d_total;
     for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < n_rec;
          r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint64_t end = r + 1 < n_rec ? seq[r + 1].offset : total_seq;
         seq[r].bytes = end - seq[r].offset;
     }
+}
+
+// Sizes of the ragged pass of a FASTQ block parsed on the device, and the
+// block summary.  ctl: [0] newlines, [1] flags, [2] sequence bytes.  A block
+// that is irregular, overflows line_end or holds no record gets n_tiles = 0.
+__global__ void fastq_sizes_kernel(const uint64_t* line_end, const unsigned long long* ctl,
+                                   uint64_t cap, int64_t phase, uint32_t k, DevSizes* sz,
+                                   BlockSummary* sum) {
+    const uint64_t n_lines = ctl[0];
+    const uint64_t flags = (ctl[1] & 0xFFFFFFFFull) | (n_lines > cap ? kLineOverflow : 0u);
+    const uint64_t n_rec = n_lines > cap ? 0 : n_lines / 4;
+    const bool ok = flags == 0 && n_rec > 0;
+    const uint64_t base_len = n_rec ? line_end[4 * n_rec - 1] + 1 : 0;
+    const uint64_t n_kmers = ok && base_len >= k ? base_len - k + 1 : 0;
+    sz->input_bytes = ok ? base_len : 0;
+    sz->n_kmers = n_kmers;
+    sz->n_tiles = n_kmers ? (n_kmers + static_cast<uint64_t>(phase) + kTileKmers - 1) / kTileKmers : 0;
+    sz->n_ranges = ok ? n_rec : 0;
+    sum->lines = n_lines;
+    sum->flags = flags;
+    sum->bases = ctl[2];
+    sum->consumed = base_len;
+    sum->records = n_rec;
+    sum->lines_used = 4 * n_rec;
+}
+
+// The same for a FASTA block.  ctl: [0] newlines, [1] flags, [3] compacted
+// sequence bytes, [4] headers (records), [5..7] the last header's line start,
+// sequence start and line.  Without `eof` the last record waits for the next
+// block; a block without a header is irregular.
+__global__ void fasta_sizes_kernel(const unsigned long long* ctl, uint64_t cap, uint64_t len,
+                                   int eof, int64_t phase, uint32_t k, DevSizes* sz,
+                                   BlockSummary* sum) {
+    const uint64_t n_lines = ctl[0];
+    const bool over = n_lines > cap;
+    const uint64_t n_rec = over ? 0 : ctl[4];
+    const uint64_t flags = (ctl[1] & 0xFFFFFFFFull) | (over ? kLineOverflow : 0u) |
+                           (!over && n_rec == 0 ? kIrregular : 0u);
+    const uint64_t use = n_rec == 0 ? 0 : (eof ? n_rec : n_rec - 1);
+    const uint64_t base_len = use == 0 ? 0 : (eof ? ctl[3] : ctl[6]);
+    const bool ok = flags == 0 && use > 0;
+    const uint64_t n_kmers = ok && base_len >= k ? base_len - k + 1 : 0;
+    sz->input_bytes = ok ? base_len : 0;
+    sz->n_kmers = n_kmers;
+    sz->n_tiles = n_kmers ? (n_kmers + static_cast<uint64_t>(phase) + kTileKmers - 1) / kTileKmers : 0;
+    sz->n_ranges = ok ? use : 0;
+    sum->lines = n_lines;
+    sum->flags = flags;
+    sum->bases = base_len;
+    sum->consumed = use == 0 ? 0 : (eof ? len : ctl[5]);
+    sum->records = use;
+    sum->lines_used = use == 0 ? 0 : (eof ? n_lines : ctl[7]);
 }
 
 template <class T>
@@ -258,7 +349,8 @@ int FastqDevice::scan_lines(sbf_filter* f, const uint8_t* h_text, uint64_t len, 
     if (n_lines == 0) return SBF_OK;
     if ((s = grow<uint64_t>(line_end, n_lines + 1)) != SBF_OK) return s;
     newline_positions_kernel<<<static_cast<unsigned>(tiles), kScanThreads, 0, st>>>(
-        d_text, len, d_tiles, static_cast<uint64_t*>(line_end.ptr));
+        d_text, len, d_tiles, static_cast<uint64_t*>(line_end.ptr), n_lines + 1,
+        reinterpret_cast<unsigned int*>(d_ctl + 1));
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "newline_positions_kernel");
     *n_lines_out = n_lines;
     return SBF_OK;
@@ -443,6 +535,167 @@ int FastqDevice::run(sbf_filter* f, bool query, const FastqBlock& b, cudaStream_
     return SBF_OK;
 }
 
+bool FastqDevice::graph_usable(const sbf_filter* f) {
+    // Graph kernel nodes take the kernels compiled into the library; the
+    // generic kernels do not read device-side sizes.
+    return f->ks && !f->ks->jit && f->ks != generic_kernels() && f->width == 1;
+}
+
+int FastqDevice::run_block_graph(sbf_filter* f, bool query, bool fasta, const uint8_t* h_text,
+                                 uint64_t len, bool eof, cudaStream_t st, BlockSummary* out) {
+    *out = BlockSummary{};
+    if (len == 0) return SBF_OK;
+    const uint64_t tiles = (len + kTileBytes - 1) / kTileBytes;
+    if (tiles > (uint64_t{1} << 20))
+        return set_error(SBF_ERR_INVALID_ARGUMENT, "FASTX block too large for the device parser");
+    // Every buffer is sized from `len` before capture (nothing allocates
+    // inside the graph): newlines up to line_cap, records up to line_cap,
+    // windows up to len.
+    line_cap = std::max<uint64_t>(line_cap, len / 32 + 1024);
+    const uint64_t max_kmers = f->kmers_of(len);
+    const uint64_t max_tiles = (max_kmers + 16 + kTileKmers - 1) / kTileKmers + 1;
+    int s;
+    if ((s = text.ensure(len + 64)) != SBF_OK || (s = grow<uint64_t>(tile_off, tiles + 2)) != SBF_OK ||
+        (s = ctl.ensure(128)) != SBF_OK || (s = grow<uint64_t>(line_end, line_cap + 1)) != SBF_OK ||
+        (s = grow<DevRange>(seq, line_cap)) != SBF_OK || (s = grow<DevRange>(hdr, line_cap)) != SBF_OK ||
+        (s = counts.ensure(64)) != SBF_OK || (s = g_sizes.ensure(sizeof(DevSizes))) != SBF_OK ||
+        (s = g_summary.ensure(sizeof(BlockSummary))) != SBF_OK || (s = g_queue.ensure(64)) != SBF_OK ||
+        (s = g_tile_rec.ensure(max_tiles * 4 + 64)) != SBF_OK ||
+        (s = h_summary.ensure(sizeof(BlockSummary))) != SBF_OK)
+        return s;
+    if (fasta && ((s = grow<uint64_t>(line_len, line_cap + 1)) != SBF_OK ||
+                  (s = grow<uint64_t>(line_hdr, line_cap + 1)) != SBF_OK ||
+                  (s = comp.ensure(len + 64)) != SBF_OK))
+        return s;
+    if (query && (s = this->out.ensure(max_kmers + 64)) != SBF_OK) return s;
+    auto* d_text = static_cast<uint8_t*>(text.ptr);
+    auto* d_tiles = static_cast<uint64_t*>(tile_off.ptr);
+    auto* d_ctl = static_cast<unsigned long long*>(ctl.ptr);
+    auto* d_le = static_cast<uint64_t*>(line_end.ptr);
+    auto* d_sizes = static_cast<DevSizes*>(g_sizes.ptr);
+    auto* d_sum = static_cast<BlockSummary*>(g_summary.ptr);
+    auto* d_counts = static_cast<unsigned long long*>(counts.ptr);
+    uint8_t* d_hits = query ? static_cast<uint8_t*>(this->out.ptr) : nullptr;
+    const uint8_t* d_base = fasta ? static_cast<const uint8_t*>(comp.ptr) : d_text;
+    const uint64_t cap = line_cap;
+    const unsigned fixed_grid = static_cast<unsigned>(f->sms) * 8;
+    // Ragged-pass parameters: the grid phase is host-known (pointer
+    // alignment), the sizes are the device's.
+    const int64_t phase = query ? static_cast<int64_t>(reinterpret_cast<uintptr_t>(d_hits) & 15u)
+                                : static_cast<int64_t>(reinterpret_cast<uintptr_t>(d_base) & 15u);
+    TileParams p{};
+    p.input = d_base;
+    p.input_bytes = len;
+    p.n_kmers = max_kmers;
+    p.sym_base = -phase;
+    p.words = f->d_words;
+    p.shard_mask = static_cast<uint32_t>(f->num_shards - 1);
+    p.out = d_hits;
+    p.n_tiles = max_tiles;
+    p.err = f->d_err;
+    p.ranges = static_cast<const DevRange*>(seq.ptr);
+    p.n_ranges = cap;
+    p.tile_rec = static_cast<const uint32_t*>(g_tile_rec.ptr);
+    p.queue = static_cast<unsigned int*>(g_queue.ptr);
+    p.counts = d_counts;
+    p.gen = f->gen;
+    p.sizes = d_sizes;
+    const int occ = f->occupancy[query ? 5 : 4];
+    const unsigned tile_grid = static_cast<unsigned>(std::max<uint64_t>(
+        std::min<uint64_t>(max_tiles, static_cast<uint64_t>(f->sms) * std::max(occ, 1)), 1));
+    const void* tile_fn = query ? f->ks->query_ragged : f->ks->insert_ragged;
+
+    cudaError_t e;
+    if (!capture_stream &&
+        (e = cudaStreamCreateWithFlags(&capture_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return cuda_fail(e, "cudaStreamCreateWithFlags");
+    const cudaStream_t launch_stream = st;
+    st = capture_stream;  // every call below is recorded into the graph
+    if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(e, "cudaStreamBeginCapture");
+    }
+    auto body = [&]() -> cudaError_t {
+        cudaError_t r;
+        if ((r = cudaMemcpyAsync(d_text, h_text, len, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+            (r = cudaMemsetAsync(d_ctl, 0, 128, st)) != cudaSuccess ||
+            (r = cudaMemsetAsync(d_counts, 0, 16, st)) != cudaSuccess)
+            return r;
+        tile_newlines_kernel<<<static_cast<unsigned>(tiles), kScanThreads, 0, st>>>(d_text, len, d_tiles);
+        scan_counts_kernel<<<1, 1024, 0, st>>>(d_tiles, tiles, reinterpret_cast<uint64_t*>(d_ctl));
+        newline_positions_kernel<<<static_cast<unsigned>(tiles), kScanThreads, 0, st>>>(
+            d_text, len, d_tiles, d_le, cap, reinterpret_cast<unsigned int*>(d_ctl + 1));
+        if (!fasta) {
+            fastq_records_kernel<<<fixed_grid, 256, 0, st>>>(
+                d_text, d_le, 0, static_cast<DevRange*>(seq.ptr), static_cast<DevRange*>(hdr.ptr),
+                reinterpret_cast<unsigned int*>(d_ctl + 1), d_ctl + 2, d_ctl, cap);
+            fastq_sizes_kernel<<<1, 1, 0, st>>>(d_le, d_ctl, cap, phase, f->k, d_sizes, d_sum);
+        } else {
+            auto* d_len = static_cast<uint64_t*>(line_len.ptr);
+            auto* d_hdrf = static_cast<uint64_t*>(line_hdr.ptr);
+            fasta_lines_kernel<<<fixed_grid, 256, 0, st>>>(d_text, d_le, 0, d_len, d_hdrf, d_ctl, cap);
+            scan_counts_kernel<<<1, 1024, 0, st>>>(d_len, 0, reinterpret_cast<uint64_t*>(d_ctl + 3),
+                                                   d_ctl, cap);
+            scan_counts_kernel<<<1, 1024, 0, st>>>(d_hdrf, 0, reinterpret_cast<uint64_t*>(d_ctl + 4),
+                                                   d_ctl, cap);
+            fasta_compact_kernel<<<fixed_grid, 256, 0, st>>>(d_text, d_le, 0, d_len,
+                                                             static_cast<uint8_t*>(comp.ptr), d_ctl, cap);
+            fasta_records_kernel<<<fixed_grid, 256, 0, st>>>(
+                d_text, d_le, 0, d_len, d_hdrf, 0, static_cast<DevRange*>(seq.ptr),
+                static_cast<DevRange*>(hdr.ptr), d_ctl + 5, d_ctl, cap, d_ctl + 4);
+            fasta_lengths_kernel<<<fixed_grid, 256, 0, st>>>(static_cast<DevRange*>(seq.ptr), 0, 0,
+                                                             d_ctl + 4, d_ctl + 3);
+            fasta_sizes_kernel<<<1, 1, 0, st>>>(d_ctl, cap, len, eof ? 1 : 0, phase, f->k, d_sizes,
+                                                d_sum);
+        }
+        if ((r = launch_tile_records_sized(p.ranges, d_sizes, p.sym_base, max_tiles,
+                                           const_cast<uint32_t*>(p.tile_rec), st)) != cudaSuccess ||
+            (r = cudaMemsetAsync(p.queue, 0, sizeof(unsigned int), st)) != cudaSuccess)
+            return r;
+        TileParams copy = p;
+        void* args[] = {&copy};
+        if ((r = cudaLaunchKernel(tile_fn, dim3(tile_grid), dim3(kThreads), args, f->ks->smem(query),
+                                  st)) != cudaSuccess)
+            return r;
+        if ((r = cudaMemcpyAsync(reinterpret_cast<uint8_t*>(h_summary.p) + offsetof(BlockSummary, valid),
+                                 d_counts, 16, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return r;
+        return cudaMemcpyAsync(h_summary.p, d_sum, offsetof(BlockSummary, valid),
+                               cudaMemcpyDeviceToHost, st);
+    };
+    const cudaError_t body_err = body();
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(st, &graph);
+    st = launch_stream;
+    if (body_err != cudaSuccess || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return cuda_fail(body_err != cudaSuccess ? body_err : e, "capturing the FASTX block graph");
+    }
+    // Same topology block after block: update the executable in place.
+    if (graph_exec) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(graph_exec, graph, &info) != cudaSuccess) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(graph_exec);
+            graph_exec = nullptr;
+        }
+    }
+    if (!graph_exec && (e = cudaGraphInstantiate(&graph_exec, graph, 0)) != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        graph_exec = nullptr;
+        return cuda_fail(e, "cudaGraphInstantiate");
+    }
+    cudaGraphDestroy(graph);
+    if ((e = cudaGraphLaunch(graph_exec, st)) != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+    f->launches += 2;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    if ((s = f->check_device_error(st)) != SBF_OK) return s;
+    *out = *static_cast<const BlockSummary*>(h_summary.p);
+    if (out->flags & kLineOverflow) line_cap = out->lines + 1;
+    return SBF_OK;
+}
+
 int PinnedBuf::ensure(size_t bytes) {
     if (bytes <= cap) return SBF_OK;
     if (p) cudaFreeHost(p);
@@ -473,6 +726,16 @@ void fastq_device_release(sbf_filter* f) {
 }
 
 void FastqDevice::release() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+    if (capture_stream) cudaStreamDestroy(capture_stream);
+    capture_stream = nullptr;
+    line_cap = 0;
+    g_sizes.release();
+    g_summary.release();
+    g_queue.release();
+    g_tile_rec.release();
+    h_summary.release();
     line_len.release();
     line_hdr.release();
     comp.release();

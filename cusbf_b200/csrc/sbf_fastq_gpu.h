@@ -32,10 +32,30 @@ struct FastqBlock {
     const DevRange* d_hdr = nullptr;  // header without '@' / '>' (offsets into the text)
 };
 
+// BlockSummary::flags bits.
+enum : uint64_t { kBlockIrregular = 1u, kBlockLineOverflow = 2u };
+
+// What one block replayed as a CUDA graph reports back (one download).
+struct BlockSummary {
+    uint64_t lines;       // newlines in the block
+    uint64_t flags;       // kIrregular / kLineOverflow bits
+    uint64_t bases;       // sequence bytes of the records processed
+    uint64_t consumed;    // text bytes of the records processed
+    uint64_t records;     // records processed
+    uint64_t lines_used;  // lines of the records processed
+    uint64_t valid, positive;
+};
+
 struct FastqDevice {
     DevBuf text, tile_off, line_end, seq, hdr, ctl, counts, out, rec_counts;
     DevBuf line_len, line_hdr, comp;  // FASTA line tables and compacted sequence
-    PinnedBuf h_hits, h_comp;
+    DevBuf g_sizes, g_summary, g_queue, g_tile_rec;  // graph replay
+    PinnedBuf h_hits, h_comp, h_summary;
+    cudaGraphExec_t graph_exec = nullptr;
+    // Blocks are captured on this stream (the caller's may be the legacy
+    // default stream, which cannot be captured) and launched on the caller's.
+    cudaStream_t capture_stream = nullptr;
+    uint64_t line_cap = 0;  // line_end entries the graph path may write
     // Filled by run() when record views are wanted.
     std::vector<DevRange> h_seq, h_hdr;
     std::vector<unsigned long long> h_valid, h_pos;
@@ -55,6 +75,15 @@ struct FastqDevice {
     // table, counts and hits are copied to the host (h_* members).
     int run(sbf_filter* f, bool query, const FastqBlock& b, cudaStream_t st, bool want_views,
             uint64_t* valid, uint64_t* positive);
+    // Upload, parse and insert / query one FASTQ (fasta = false) or FASTA
+    // block as one CUDA graph with a single synchronisation: the record count,
+    // sequence length and regularity are found and used on the device, and
+    // an irregular block or one whose newlines overflow line_end runs no
+    // insert or query (the caller retries or parses on the host).  Without
+    // per-record views only; needs kernels compiled into the library.
+    int run_block_graph(sbf_filter* f, bool query, bool fasta, const uint8_t* h_text,
+                        uint64_t len, bool eof, cudaStream_t st, BlockSummary* out);
+    static bool graph_usable(const sbf_filter* f);
     const uint8_t* hits_host() const { return static_cast<const uint8_t*>(h_hits.p); }
     // FASTA sequences for record views (filled by run() with want_views).
     const uint8_t* comp_host() const { return static_cast<const uint8_t*>(h_comp.p); }

@@ -349,6 +349,13 @@ bool device_fastq_enabled() {
     return !(v && std::strcmp(v, "host") == 0);
 }
 
+// Blocks without per-record views run as one CUDA graph each
+// (SBF_FASTX_GRAPH=0 runs them as stream launches).
+bool fastx_graph_enabled() {
+    const char* v = std::getenv("SBF_FASTX_GRAPH");
+    return !(v && std::strcmp(v, "0") == 0);
+}
+
 uint64_t fastq_block_bytes() {
     if (const char* v = std::getenv("SBF_FASTQ_BLOCK_BYTES")) {
         const long long b = std::strtoll(v, nullptr, 10);
@@ -416,6 +423,51 @@ int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const ch
             text[len] = '\n';  // the last line ends at end of input
             parse_len = len + 1;
         }
+        const bool views = query && consume;
+        if (!views && fastx_graph_enabled() && FastqDevice::graph_usable(f)) {
+            BlockSummary g;
+            s = dev.run_block_graph(f, query, !fastq, reinterpret_cast<const uint8_t*>(text),
+                                    parse_len, eof, st, &g);
+            if (s != SBF_OK) return s;
+            if (g.flags & kBlockLineOverflow) continue;  // line table grown: run the block again
+            if (fastq) {
+                // An insert of the records before a fallback is repeated by
+                // the host path, which ORs the same bits again.
+                if ((g.flags & kBlockIrregular) || g.records == 0 || (eof && g.consumed < parse_len))
+                    return fallback(len);
+            } else {
+                if (g.flags & kBlockIrregular) return fallback(len);
+                if (g.records == 0) {
+                    if (eof || cap >= kMaxBlockBytes) return fallback(len);
+                    PinnedBuf bigger;
+                    if ((s = bigger.ensure(2 * cap + 1)) != SBF_OK) return fallback(len);
+                    std::memcpy(bigger.p, text, len);
+                    buf.release();
+                    buf = bigger;
+                    bigger.p = nullptr;
+                    text = static_cast<char*>(buf.p);
+                    cap *= 2;
+                    continue;
+                }
+            }
+            if (query) {
+                qt.records_queried += g.records;
+                qt.queried_bases += g.bases;
+                qt.queried_kmers += g.valid;
+                qt.positive_kmers += g.positive;
+            } else {
+                it.records_indexed += g.records;
+                it.indexed_bases += g.bases;
+                it.inserted_kmers += g.valid;
+            }
+            index_base += g.records;
+            line_base += g.lines_used;
+            const uint64_t consumed = std::min<uint64_t>(g.consumed, len);
+            std::memmove(text, text + consumed, len - consumed);
+            len -= consumed;
+            if (eof && len == 0) break;
+            continue;
+        }
         FastqBlock b;
         if (fastq) {
             s = dev.parse(f, reinterpret_cast<const uint8_t*>(text), parse_len, st, &b);
@@ -440,7 +492,6 @@ int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const ch
             }
         }
         uint64_t valid = 0, positive = 0;
-        const bool views = query && consume;
         if ((s = dev.run(f, query, b, st, views, &valid, &positive)) != SBF_OK) return s;
         if (query) {
             qt.records_queried += b.records;

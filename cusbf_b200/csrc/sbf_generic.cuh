@@ -205,9 +205,8 @@ __global__ void __launch_bounds__(kThreads) generic_kernel(TileParams p) {
                 const uint32_t shard = eval_kmer(c, p.shard_mask, km, m);
                 if constexpr (kQuery) {
                     if (!in_run || shard != run_shard) {
-                        const uint64_t* src = p.words + static_cast<uint64_t>(shard) * 4;
-#pragma unroll
-                        for (int i = 0; i < 4; ++i) words[i] = __ldg(src + i);
+                        load_shard(p.words + static_cast<uint64_t>(shard) * 4, words[0], words[1],
+                                   words[2], words[3]);
                         run_shard = shard;
                         in_run = true;
                     }

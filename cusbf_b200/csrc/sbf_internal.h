@@ -38,6 +38,16 @@ struct GenericCfg {
     uint32_t alphabet;  // SBF_ALPHABET_*
 };
 
+// Sizes of a ragged launch that are known only on the device: a FASTX block
+// parsed on the GPU and replayed as one CUDA graph finds its record count and
+// sequence length on the device, so the graph's launches read them here.
+struct DevSizes {
+    uint64_t input_bytes;
+    uint64_t n_kmers;
+    uint64_t n_tiles;   // 0 skips the pass
+    uint64_t n_ranges;
+};
+
 // One launch of a tile kernel.  Grid position g of tile n is
 // g = n * kTileKmers + (0 .. kTileKmers-1); it holds window (k-mer)
 // i = g + sym_base, and symbol i is the first base of that window.
@@ -66,12 +76,17 @@ struct TileParams {
     unsigned long long* rec_pos;
     uint32_t rec_shift;
     GenericCfg gen;  // read by the generic kernels only
+    // Ragged tile kernels: when set, input_bytes, n_kmers, n_tiles and
+    // n_ranges are read from here at kernel start (n_tiles above is then the
+    // host's upper bound, used only for the launch shape).
+    const DevSizes* sizes;
 };
 
 // Device error codes written to TileParams::err.
 enum : int {
     kDevErrNone = 0,
     kDevErrStageTimeout = 1,  // a bulk-copy wait ran out of its time bound
+    kDevErrRecordRange = 2,   // sharded insert: a run record outside the rank's shards
 };
 
 // Function table for one compiled configuration <K,S,M,H> (k = s = m = h = 0
@@ -109,6 +124,11 @@ cudaError_t launch_pack_dense(const uint8_t* seq, uint64_t num_symbols, uint64_t
 // input byte of tile t (n_ranges when none).
 cudaError_t launch_tile_records(const DevRange* ranges, uint64_t n_ranges, int64_t sym_base,
                                 uint64_t n_tiles, uint32_t* tile_rec, cudaStream_t stream);
+// The same with the record and tile counts read from `sizes` on the device;
+// `max_tiles` bounds the launch.
+cudaError_t launch_tile_records_sized(const DevRange* ranges, const DevSizes* sizes,
+                                      int64_t sym_base, uint64_t max_tiles, uint32_t* tile_rec,
+                                      cudaStream_t stream);
 cudaError_t launch_popcount(const uint64_t* words, uint64_t n_words, unsigned long long* out,
                             cudaStream_t stream);
 // Kernels compiled at run time for a configuration that is not compiled into

@@ -29,6 +29,24 @@ __global__ void tile_records_kernel(const DevRange* ranges, uint64_t n, int64_t 
     tile_rec[t] = static_cast<uint32_t>(lo);
 }
 
+// tile_records_kernel with the record and tile counts read on the device.
+__global__ void tile_records_sized_kernel(const DevRange* ranges, const DevSizes* sizes,
+                                          int64_t sym_base, uint32_t* tile_rec) {
+    const uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= sizes->n_tiles) return;
+    const uint64_t n = sizes->n_ranges;
+    const int64_t s0 = static_cast<int64_t>(t) * kTileKmers + sym_base;
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (static_cast<int64_t>(ranges[mid].offset + ranges[mid].bytes) > s0)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    tile_rec[t] = static_cast<uint32_t>(lo);
+}
+
 // ---------------------------------------------------------------------------
 // Auxiliary kernels
 // ---------------------------------------------------------------------------
@@ -79,6 +97,15 @@ cudaError_t launch_tile_records(const DevRange* ranges, uint64_t n_ranges, int64
     if (n_tiles == 0) return cudaSuccess;
     tile_records_kernel<<<static_cast<unsigned>((n_tiles + 255) / 256), 256, 0, stream>>>(
         ranges, n_ranges, sym_base, n_tiles, tile_rec);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tile_records_sized(const DevRange* ranges, const DevSizes* sizes,
+                                      int64_t sym_base, uint64_t max_tiles, uint32_t* tile_rec,
+                                      cudaStream_t stream) {
+    if (max_tiles == 0) return cudaSuccess;
+    tile_records_sized_kernel<<<static_cast<unsigned>((max_tiles + 255) / 256), 256, 0, stream>>>(
+        ranges, sizes, sym_base, tile_rec);
     return cudaGetLastError();
 }
 

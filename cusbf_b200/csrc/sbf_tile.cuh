@@ -283,12 +283,12 @@ __device__ __forceinline__ void smer_masks(const uint32_t* c, int r, uint64_t m[
 
 // Insert: the mask of window j is T_j = OR of the one-hot masks of its F
 // s-mers; a super-k-mer run (consecutive valid windows with equal shard)
-// accumulates acc = OR T_j and is flushed with one red.or per shard word when
-// the next window leaves the run.
-template <class C>
+// accumulates acc = OR T_j and is handed to flush(shard, acc) when the next
+// window leaves the run (the insert kernel ORs it into the shard; the sharded
+// insert's emit kernel records it).
+template <class C, class Flush>
 __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
-                                             uint32_t shard_mask, uint64_t* words,
-                                             FlushRing& ring) {
+                                             uint32_t shard_mask, Flush&& flush) {
     constexpr int F = C::F;
     uint64_t acc[4] = {0, 0, 0, 0};
     uint32_t prev_shard = 0;
@@ -310,7 +310,7 @@ __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
             smer_masks<C>(c, j + 3, m3);
             const bool valid = (vmask >> j) & 1u;
             const bool cont = valid && prev_valid && shard == prev_shard;
-            if (prev_valid && !cont) flush_run(words, prev_shard, acc, ring);
+            if (prev_valid && !cont) flush(prev_shard, acc);
             const uint64_t keep = cont ? ~uint64_t{0} : uint64_t{0};
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
@@ -331,7 +331,7 @@ __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
             smer_masks<C>(c, j + F - 1, mring[(j + F - 1) % F]);
             const bool valid = (vmask >> j) & 1u;
             const bool cont = valid && prev_valid && shard == prev_shard;
-            if (prev_valid && !cont) flush_run(words, prev_shard, acc, ring);
+            if (prev_valid && !cont) flush(prev_shard, acc);
             const uint64_t keep = cont ? ~uint64_t{0} : uint64_t{0};
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
@@ -344,7 +344,7 @@ __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
             prev_valid = valid;
         });
     }
-    if (prev_valid) flush_run(words, prev_shard, acc, ring);
+    if (prev_valid) flush(prev_shard, acc);
 }
 
 // Query shard slots: the run heads of a strip fetch their 32-byte shards into
@@ -353,8 +353,12 @@ __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
 static_assert(kSlots * kThreads * 32 + kOverflow * kThreads * 4 == kQuerySlotBytes,
               "slot geometry");
 
+// Half of a shard into a slot.  The .L2::64B fetch size makes an L2 miss
+// fill 64 bytes instead of 128: a random 32-byte shard then costs about 64 B
+// of DRAM reads instead of about 120 (measured with random sector reads on
+// the B200), at the same speed.
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(smem_dst)),
+    asm volatile("cp.async.cg.shared.global.L2::64B [%0], [%1], 16;" ::"r"(smem_addr(smem_dst)),
                  "l"(gmem_src)
                  : "memory");
 }
@@ -366,7 +370,7 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 __device__ __forceinline__ void load_shard_now(const uint64_t* p, uint64_t w[4]) {
-    asm volatile("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];"
+    asm volatile("ld.global.nc.L2::64B.v4.u64 {%0, %1, %2, %3}, [%4];"
                  : "=l"(w[0]), "=l"(w[1]), "=l"(w[2]), "=l"(w[3])
                  : "l"(p));
 }
@@ -415,6 +419,19 @@ __device__ __forceinline__ void store_strip_bytes(uint32_t result, uint8_t* out,
                 out[i] = static_cast<uint8_t>((result >> j) & 1u);
         }
     }
+}
+
+// Loads shard slot words x[0..7] from shared address `addr` when `pred` is
+// non-zero and leaves them unchanged otherwise: a predicated load, so a run
+// head costs no branch in the per-window loop.
+__device__ __forceinline__ void lds_slot_if(uint32_t pred, uint32_t addr, uint32_t (&x)[8]) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %8, 0;\n\t"
+        "@p ld.shared.v4.u32 {%0, %1, %2, %3}, [%9];\n\t"
+        "@p ld.shared.v4.u32 {%4, %5, %6, %7}, [%9+16];\n\t}"
+        : "+r"(x[0]), "+r"(x[1]), "+r"(x[2]), "+r"(x[3]), "+r"(x[4]), "+r"(x[5]), "+r"(x[6]),
+          "+r"(x[7])
+        : "r"(pred), "r"(addr));
 }
 
 // Query of one strip without slots: each run head loads its shard when it is
@@ -528,7 +545,6 @@ __device__ __forceinline__ uint32_t query_strip(const uint32_t* c, uint32_t vmas
     __syncwarp();  // neighbours' slots are complete before any is borrowed
     uint64_t w[4] = {0, 0, 0, 0};
     uint32_t result = 0;
-    n = 0;
     // Bit addresses of the F positions of the current window, extracted once
     // per position as it enters the window.
     uint32_t ring[C::H == 4 ? F : 1][4];
@@ -539,6 +555,49 @@ __device__ __forceinline__ uint32_t query_strip(const uint32_t* c, uint32_t vmas
             for (int q = 0; q < 4; ++q) ring[o][q] = __byte_perm(bytes[o], 0u, 0x4440u + q);
         }
     }
+    // (Configurations with one s-mer per window or sixteen hashes keep the
+    // branching loop below: the predicated form spills registers there.)
+    constexpr bool kPredicated = F > 1 && C::H <= 8;
+    if (kPredicated && n <= kSlots) {
+        // Every head's shard is in a slot (the common case): each window
+        // does a predicated load of the next head's slot and advances the
+        // slot address when it is a head, so the loop has no per-head branch.
+        const uint64_t* sfirst = borrow ? slot0 + left_slot * kSlotStride - 4 : slot0;
+        uint32_t addr = smem_addr(sfirst);
+        const uint32_t base = smem_addr(slot0);
+        uint32_t x[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        uint32_t loaded = 0;
+#pragma unroll
+        for (int j = 0; j < kStrip; ++j) {
+            if constexpr (C::H == 4) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    ring[(j + F - 1) % F][q] = __byte_perm(bytes[j + F - 1], 0u, 0x4440u + q);
+            }
+            const uint32_t head = (heads >> j) & 1u;
+            lds_slot_if(head, addr, x);
+            loaded += head;
+            addr = head ? base + loaded * (kSlotStride * 8) : addr;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) w[q] = (static_cast<uint64_t>(x[2 * q + 1]) << 32) | x[2 * q];
+            uint32_t present = (vmask >> j) & 1u;
+#pragma unroll
+            for (int o = 0; o < F; ++o) {
+                if constexpr (C::H == 4) {
+                    const uint32_t* b = ring[(j + o) % F];
+                    present &= static_cast<uint32_t>(w[0] >> b[0]) & static_cast<uint32_t>(w[1] >> b[1]) &
+                               static_cast<uint32_t>(w[2] >> b[2]) & static_cast<uint32_t>(w[3] >> b[3]);
+                } else {
+                    present &= smer_present_h<C>(hs[j + o], w);
+                }
+            }
+            result |= (present & 1u) << j;
+        }
+        if (out) store_strip_bytes(result, out, first_kmer, n_kmers);
+        return result;
+    }
+    // More heads than slots: the later heads load their shards directly.
+    n = 0;
 #pragma unroll
     for (int j = 0; j < kStrip; ++j) {
         if constexpr (C::H == 4) {
@@ -731,6 +790,15 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
     __shared__ alignas(8) uint64_t bars[2];
 
     const int tid = threadIdx.x;
+    if constexpr (kRagged) {
+        if (p.sizes) {
+            const DevSizes z = *p.sizes;
+            p.input_bytes = z.input_bytes;
+            p.n_kmers = z.n_kmers;
+            p.n_tiles = z.n_tiles;
+            p.n_ranges = z.n_ranges;
+        }
+    }
     auto take = [&](uint32_t i, int slot) {
         uint64_t t;
         if constexpr (kRagged) {
@@ -826,7 +894,10 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
             if (p.out_bits && first_kmer < static_cast<int64_t>(p.n_kmers))
                 p.out_bits[first_kmer >> 5] = hits;
         } else {
-            if (vmask) insert_strip<C>(c, vmask, p.shard_mask, p.words, ring);
+            if (vmask)
+                insert_strip<C>(c, vmask, p.shard_mask, [&](uint32_t shard, const uint64_t* acc) {
+                    flush_run(p.words, shard, acc, ring);
+                });
         }
         if constexpr (kRagged) {
             if (p.rec_valid) tally_records(p, first_rec[it % 3], first_kmer, vmask, hits);

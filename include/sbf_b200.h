@@ -438,6 +438,37 @@ int sbf_ragged_autotune(sbf_filter_t* filter, int query, const char* h_seq, uint
 int sbf_ragged_tuning_lookup(const sbf_filter_t* filter, int query, uint64_t len, uint64_t n,
                              sbf_ragged_tuning* out);
 
+/* ---- Sharded multi-rank insert (no reference counterpart) --------------
+ *
+ * Replaces, when W ranks (one per GPU) split one input, the single-GPU insert
+ * (insert_sequence_kmers_kernel, detail/kernels.cuh:214-242, which ORs each
+ * super-k-mer run's word masks into its shard, filter_ref.cuh:94-108):
+ *   1. each rank emits the run records of its windows (sbf_emit_runs_async);
+ *   2. the caller routes every record to the rank owning its shard (shards
+ *      split into W contiguous ranges; cusbf_b200/sharded.py does this with
+ *      one torch.distributed all-to-all);
+ *   3. each rank ORs the records it owns into its shard range
+ *      (sbf_apply_runs_async), and an all-gather of the ranges gives every
+ *      rank the filter one GPU would build from the whole input.
+ * DNA configurations compiled into the library only. */
+
+/* Run records of the windows of device bytes d_seq[0, len): record i is
+ * d_shards[i] and the four word masks d_masks[4i, 4i+4) (16-byte aligned).
+ * d_count (device, 2 x uint64) receives the records emitted and the valid
+ * windows; records beyond `capacity` are counted but not stored, so a count
+ * above capacity means the call must be repeated with larger buffers. */
+int sbf_emit_runs_async(const sbf_filter_t* filter, const char* d_seq, uint64_t len,
+                        uint32_t* d_shards, uint64_t* d_masks, uint64_t capacity,
+                        uint64_t* d_count, sbf_stream_t stream);
+/* ORs n device records into the filter; every shard must lie in
+ * [shard_lo, shard_hi), else the device error word is set and the next
+ * sbf_filter_synchronize returns SBF_ERR_CUDA. */
+int sbf_apply_runs_async(sbf_filter_t* filter, const uint32_t* d_shards, const uint64_t* d_masks,
+                         uint64_t n, uint64_t shard_lo, uint64_t shard_hi, sbf_stream_t stream);
+/* Waits for `stream` and reports a device-side error of the filter's kernels
+ * (a staging wait that ran out, a misrouted run record) as SBF_ERR_CUDA. */
+int sbf_filter_synchronize(const sbf_filter_t* filter, sbf_stream_t stream);
+
 /* ---- Request server (no reference counterpart) ------------------------
  *
  * Keeps a filter resident and serves insert and query requests from any

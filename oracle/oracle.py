@@ -98,7 +98,7 @@ class Oracle:
         L = self.lib
         for name in ("sbf_oracle_insert", "sbf_oracle_contains", "sbf_oracle_pack_dense",
                      "sbf_oracle_insert_dense", "sbf_oracle_contains_dense",
-                     "sbf_oracle_window_shards", "sbf_oracle_count_runs"):
+                     "sbf_oracle_window_shards", "sbf_oracle_count_runs", "sbf_oracle_runs"):
             getattr(L, name).restype = C.c_int
         L.sbf_oracle_hash64.restype = C.c_uint64
         L.sbf_oracle_hash64.argtypes = [C.c_uint64]
@@ -162,6 +162,22 @@ class Oracle:
         self.lib.sbf_oracle_window_shards(C.byref(self.cfg), _ptr(b), C.c_uint64(b.size),
                                           C.c_uint64(n_shards), _ptr(shards), _ptr(valid))
         return shards[:n], valid[:n]
+
+    def runs(self, seq, n_shards) -> tuple[np.ndarray, np.ndarray]:
+        """Run records of ``seq``: (shards uint32[R], masks uint64[R, 4]); ORing
+        every record's masks into its shard of an empty filter gives the
+        filter that ``insert`` builds."""
+        b = _as_bytes(seq)
+        cap = max(windows(self.k, b.size, self.alphabet), 1)
+        shards = np.zeros(cap, dtype=np.uint32)
+        masks = np.zeros((cap, 4), dtype=np.uint64)
+        n = C.c_uint64(0)
+        rc = self.lib.sbf_oracle_runs(C.byref(self.cfg), _ptr(b), C.c_uint64(b.size),
+                                      C.c_uint64(n_shards), _ptr(shards), _ptr(masks),
+                                      C.c_uint64(cap), C.byref(n))
+        if rc != 0:
+            raise RuntimeError(f"sbf_oracle_runs failed ({rc})")
+        return shards[:n.value].copy(), masks[:n.value].copy()
 
     def count_runs(self, seq, n_shards) -> tuple[int, int]:
         """Super-k-mer runs R and valid windows of ``seq`` for a filter with

@@ -428,3 +428,44 @@ int sbf_oracle_count_runs(const sbf_oracle_config* cfg, const char* seq, uint64_
     if (valid_out) *valid_out = valid;
     return 0;
 }
+
+int sbf_oracle_runs(const sbf_oracle_config* cfg, const char* seq, uint64_t len,
+                    uint64_t num_shards, uint32_t* shard_out, uint64_t* masks_out,
+                    uint64_t capacity, uint64_t* n_out) {
+    /* The super-k-mer run records of a sequence: for every maximal stretch of
+     * consecutive valid windows with one shard, the shard and the OR of the
+     * windows' four word masks (what one insert of the stretch ORs into the
+     * shard; detail/kernels.cuh:107-172 merges windows the same way).  The
+     * OR of all records into an empty filter equals sbf_oracle_insert. */
+    cfg_t c;
+    if (make_cfg(cfg, &c) != 0) return -1;
+    uint64_t n_sym = 0;
+    uint8_t* sym = encode_all(&c, seq, len, &n_sym);
+    if (!sym) return -2;
+    const uint64_t n = windows_of(&c, n_sym);
+    uint64_t runs = 0, masks[4], acc[4] = {0, 0, 0, 0};
+    int prev_valid = 0, rc = 0;
+    uint32_t prev_shard = 0;
+    for (uint64_t i = 0; i <= n; ++i) {
+        uint32_t shard = 0;
+        const int v = i < n ? eval_window(&c, sym, i, num_shards, 0, &shard, masks) : 0;
+        const int cont = v && prev_valid && shard == prev_shard;
+        if (prev_valid && !cont) {
+            if (runs >= capacity) {
+                rc = -3;
+                break;
+            }
+            shard_out[runs] = prev_shard;
+            for (int w = 0; w < 4; ++w) masks_out[4 * runs + w] = acc[w];
+            ++runs;
+        }
+        if (v) {
+            for (int w = 0; w < 4; ++w) acc[w] = (cont ? acc[w] : 0) | masks[w];
+        }
+        prev_valid = v;
+        prev_shard = shard;
+    }
+    free(sym);
+    *n_out = runs;
+    return rc;
+}

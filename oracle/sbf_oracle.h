@@ -47,6 +47,9 @@ int sbf_oracle_window_shards(const sbf_oracle_config* cfg, const char* seq, uint
                              uint64_t num_shards, uint32_t* shards_out, uint8_t* valid_out);
 int sbf_oracle_count_runs(const sbf_oracle_config* cfg, const char* seq, uint64_t len,
                           uint64_t num_shards, uint64_t* runs_out, uint64_t* valid_out);
+int sbf_oracle_runs(const sbf_oracle_config* cfg, const char* seq, uint64_t len,
+                    uint64_t num_shards, uint32_t* shard_out, uint64_t* masks_out,
+                    uint64_t capacity, uint64_t* n_out);
 
 #ifdef __cplusplus
 }

@@ -26,6 +26,66 @@ static int failures = 0;
         }                                                                \
     } while (0)
 
+// A caller's own kernels over filter::ref(), as the reference's device view
+// allows (filter_ref.cuh:70-108): window i of a DNA sequence is packed
+// MSB-first (A0 C1 T2 G3), its minimizer selects the shard, and the window is
+// tested with sectorized_contains_packed_kmer or inserted with
+// apply_word_masks.
+__device__ uint32_t user_dna_code(char c) {
+    switch (c & 0xDF) {
+        case 'A': return 0;
+        case 'C': return 1;
+        case 'T': return 2;
+        case 'G': return 3;
+        default: return 0xFFu;
+    }
+}
+
+template <class Cfg>
+__device__ bool user_window(const char* seq, uint64_t i, uint64_t& packed, uint64_t& minhash) {
+    bool valid = true;
+    packed = 0;
+    for (int j = 0; j < Cfg::k; ++j) {
+        const uint32_t c = user_dna_code(seq[i + j]);
+        valid &= c != 0xFFu;
+        packed = (packed << 2) | (c & 3u);
+    }
+    minhash = ~uint64_t{0};
+    for (int o = 0; o + Cfg::m <= Cfg::k; ++o) {
+        const uint64_t mm = (packed >> (2 * (Cfg::k - o - Cfg::m))) & ((uint64_t{1} << (2 * Cfg::m)) - 1);
+        const uint64_t h = mm * 0x9E3779B97F4A7C15ULL;
+        minhash = h < minhash ? h : minhash;
+    }
+    return valid;
+}
+
+template <class Cfg>
+__global__ void user_query(cusbf::filter_ref<Cfg> ref, const char* seq, uint64_t n, uint8_t* out) {
+    const uint64_t i = blockIdx.x * uint64_t{blockDim.x} + threadIdx.x;
+    if (i >= n) return;
+    uint64_t packed, minhash;
+    const bool valid = user_window<Cfg>(seq, i, packed, minhash);
+    const auto& block = ref.blocks()[ref.shard_index(minhash)];
+    out[i] = valid && cusbf::filter_ref<Cfg>::sectorized_contains_packed_kmer(packed, block.words);
+}
+
+template <class Cfg>
+__global__ void user_insert(cusbf::filter_ref<Cfg> ref, const char* seq, uint64_t n) {
+    const uint64_t i = blockIdx.x * uint64_t{blockDim.x} + threadIdx.x;
+    if (i >= n) return;
+    uint64_t packed, minhash;
+    if (!user_window<Cfg>(seq, i, packed, minhash)) return;
+    uint64_t m[4] = {0, 0, 0, 0};
+    for (int o = 0; o + Cfg::s <= Cfg::k; ++o) {
+        uint64_t h = ((packed >> (2 * (Cfg::k - o - Cfg::s))) & ((uint64_t{1} << (2 * Cfg::s)) - 1)) *
+                     0x9e3779b97f4a7c15ULL;
+        h ^= h >> 33;
+        for (uint64_t j = 0; j < Cfg::hashCount; ++j)
+            m[j % 4] |= uint64_t{1} << cusbf::filter_block<Cfg>::sectorizedBitAddress(h, j);
+    }
+    ref.apply_word_masks(ref.blocks()[ref.shard_index(minhash)], m[0], m[1], m[2], m[3]);
+}
+
 static bool all_ones(const std::vector<uint8_t>& v) {
     for (uint8_t x : v)
         if (x != 1) return false;
@@ -152,6 +212,43 @@ int main() {
         CHECK(all_ones(CUSBF_UNWRAP(f.contains_sequence(seq))));
         CHECK(f.num_shards() == (1u << 12) && f.filter_bits() == (1u << 20));
         CHECK(f.ref().num_blocks() == f.num_shards());
+    }
+    {  // filter_ref device members from a caller's kernels (filter_ref.cuh:70-108)
+        cusbf::filter<K31> f(1 << 22), g(1 << 22);
+        std::string seq(40000, 'A');
+        uint64_t x = 0x9E3779B97F4A7C15ull;
+        for (size_t i = 0; i < seq.size(); ++i) {
+            x ^= x << 13;
+            x ^= x >> 7;
+            x ^= x << 17;
+            seq[i] = (i % 997 == 5) ? 'N' : "ACGTacgt"[x & 7];
+        }
+        const uint64_t n = seq.size() - K31::k + 1;
+        (void)CUSBF_UNWRAP(f.insert_sequence(seq.substr(0, 25000)));
+        const auto want = CUSBF_UNWRAP(f.contains_sequence(seq));
+        char* d = nullptr;
+        uint8_t* out = nullptr;
+        CUSBF_CUDA_CALL(cudaMalloc(&d, seq.size()));
+        CUSBF_CUDA_CALL(cudaMalloc(&out, n));
+        CUSBF_CUDA_CALL(cudaMemcpy(d, seq.data(), seq.size(), cudaMemcpyHostToDevice));
+        user_query<K31><<<(n + 255) / 256, 256>>>(f.ref(), d, n, out);
+        std::vector<uint8_t> got(n);
+        CUSBF_CUDA_CALL(cudaMemcpy(got.data(), out, n, cudaMemcpyDeviceToHost));
+        CHECK(got == want);
+        // Inserting the first 25000 bytes through apply_word_masks gives the
+        // engine's shard words.
+        user_insert<K31><<<(25000 - K31::k + 1 + 255) / 256, 256>>>(g.ref(), d, 25000 - K31::k + 1);
+        CUSBF_CUDA_CALL(cudaDeviceSynchronize());
+        const uint64_t words = f.ref().num_blocks() * 4;
+        std::vector<uint64_t> wf(words), wg(words);
+        CUSBF_CUDA_CALL(cudaMemcpy(wf.data(), f.ref().blocks(), words * 8, cudaMemcpyDeviceToHost));
+        CUSBF_CUDA_CALL(cudaMemcpy(wg.data(), g.ref().blocks(), words * 8, cudaMemcpyDeviceToHost));
+        CHECK(wf == wg);
+        uint64_t set = 0;
+        for (uint64_t w : wf) set += w != 0;
+        CHECK(set > 0);
+        cudaFree(d);
+        cudaFree(out);
     }
     {  // other alphabets and configurations run on the generic kernels
         using P = cusbf::Config<5, 4, 3, 4, 256, cusbf::ProteinAlphabet>;
