@@ -673,21 +673,22 @@ int FastqDevice::run_block_graph(sbf_filter* f, bool query, bool fasta, const ui
         return cuda_fail(body_err != cudaSuccess ? body_err : e, "capturing the FASTX block graph");
     }
     // Same topology block after block: update the executable in place.
-    if (graph_exec) {
+    cudaGraphExec_t& exec = graph_exec[(fasta ? 2 : 0) + (query ? 1 : 0)];
+    if (exec) {
         cudaGraphExecUpdateResultInfo info{};
-        if (cudaGraphExecUpdate(graph_exec, graph, &info) != cudaSuccess) {
+        if (cudaGraphExecUpdate(exec, graph, &info) != cudaSuccess) {
             cudaGetLastError();
-            cudaGraphExecDestroy(graph_exec);
-            graph_exec = nullptr;
+            cudaGraphExecDestroy(exec);
+            exec = nullptr;
         }
     }
-    if (!graph_exec && (e = cudaGraphInstantiate(&graph_exec, graph, 0)) != cudaSuccess) {
+    if (!exec && (e = cudaGraphInstantiate(&exec, graph, 0)) != cudaSuccess) {
         cudaGraphDestroy(graph);
-        graph_exec = nullptr;
+        exec = nullptr;
         return cuda_fail(e, "cudaGraphInstantiate");
     }
     cudaGraphDestroy(graph);
-    if ((e = cudaGraphLaunch(graph_exec, st)) != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+    if ((e = cudaGraphLaunch(exec, st)) != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
     f->launches += 2;
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
     if ((s = f->check_device_error(st)) != SBF_OK) return s;
@@ -726,8 +727,10 @@ void fastq_device_release(sbf_filter* f) {
 }
 
 void FastqDevice::release() {
-    if (graph_exec) cudaGraphExecDestroy(graph_exec);
-    graph_exec = nullptr;
+    for (cudaGraphExec_t& g : graph_exec) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
     if (capture_stream) cudaStreamDestroy(capture_stream);
     capture_stream = nullptr;
     line_cap = 0;

@@ -51,7 +51,9 @@ struct FastqDevice {
     DevBuf line_len, line_hdr, comp;  // FASTA line tables and compacted sequence
     DevBuf g_sizes, g_summary, g_queue, g_tile_rec;  // graph replay
     PinnedBuf h_hits, h_comp, h_summary;
-    cudaGraphExec_t graph_exec = nullptr;
+    // One executable per (FASTA?, query?): blocks of one kind update theirs in
+    // place; a different kind never forces a re-instantiation.
+    cudaGraphExec_t graph_exec[4] = {nullptr, nullptr, nullptr, nullptr};
     // Blocks are captured on this stream (the caller's may be the legacy
     // default stream, which cannot be captured) and launched on the caller's.
     cudaStream_t capture_stream = nullptr;
