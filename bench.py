@@ -649,6 +649,86 @@ SERVED_METRIC = ("served k-mers/s and p50/p99/p999 latency, Poisson 20k req/s (l
                  "1-100k x 150 bp reads, 5% inserts of 1-10 Mbp) on the resident 100 Mbp filter")
 
 
+SHARDED_METRIC = ("k-mers/s of one 3.1 Gbp genome inserted over N GPUs by the sharded insert "
+                  "(emit runs, all-to-all to shard owners, OR, all-gather to replicas)")
+
+
+def run_sharded(args, world: int, rank: int, local_rank: int) -> None:
+    """Strong scaling of the insert: every rank holds the same genome; each
+    step clears the filter and runs cusbf_b200.sharded.sharded_insert (each
+    rank emits the runs of 1/N of the windows, records go to the owners of
+    their shards, owners OR them in, an all-gather restores the whole filter
+    on every rank).  The step time and the per-phase times are the max over
+    ranks.  After timing, rank 0's filter is compared word for word with a
+    single-GPU insert, which is also timed."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import cusbf_b200 as sbf
+    from cusbf_b200 import sharded
+
+    spec = workload_spec("c3", args.scale)
+    joined, _, n_ins_valid = build_host_genome(spec, seed=args.seed)
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    os.environ.setdefault("MASTER_PORT", "29517")
+    dist.init_process_group("nccl", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120), device_id=dev)
+    bits = int(round(spec["bits_per_kmer"] * n_ins_valid))
+    f = sbf.Filter(bits, k=K, s=S, m=M, hashes=H)
+    d_genome = torch.from_numpy(joined).to(dev)
+    times, phases = [], {}
+    for i in range(args.warmup + args.steps):
+        f.clear()
+        torch.cuda.synchronize(dev)
+        dist.barrier()
+        a, b = _ev(torch), _ev(torch)
+        a.record()
+        sharded.sharded_insert(f, d_genome, timings=phases if i >= args.warmup else None)
+        b.record()
+        torch.cuda.synchronize(dev)
+        if i >= args.warmup:
+            times.append(a.elapsed_time(b))
+    names = ("emit", "route", "apply", "gather")
+    got = max_over_ranks([float(np.mean(times))] + [phases.get(n, 0.0) / args.steps
+                                                     for n in names], dist, dev)
+    ms, phase_ms = got[0], dict(zip(names, got[1:]))
+    same = single_ms = None
+    if rank == 0:
+        g = sbf.Filter(bits, k=K, s=S, m=M, hashes=H)
+        st = []
+        for i in range(1 + args.steps):
+            g.clear()
+            a, b = _ev(torch), _ev(torch)
+            a.record()
+            g.insert_sequence_async(d_genome)
+            b.record()
+            torch.cuda.synchronize(dev)
+            if i:
+                st.append(a.elapsed_time(b))
+        single_ms = float(np.mean(st))
+        same = bool(torch.equal(f.words(), g.words()))
+        g.close()
+    dist.barrier()
+    if rank == 0:
+        print(json.dumps({
+            "metric": SHARDED_METRIC, "value": n_ins_valid / (ms / 1e3), "unit": "k-mers/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded stand-in with the configuration's shapes; no public genome)",
+            "config": {"workload": f"{spec['name']}: {spec['genome_bp'] / 1e9:.3g} Gbp in "
+                                   f"{spec['n_records']} records, one insert over all ranks",
+                       "filter_bits": f.filter_bits(), "insert_kmers": n_ins_valid,
+                       "parallelism": f"sharded insert x{world} (strong)"},
+            "phase_ms": phase_ms, "single_gpu_insert_ms": single_ms,
+            "identical_to_single_gpu_insert": same}), flush=True)
+    f.close()
+    dist.destroy_process_group()
+
+
 FASTX_METRIC = ("GB/s of FASTA insert and FASTQ query from files, parsed on the GPU, each block "
                 "replayed as one CUDA graph vs stream launches vs the host parser")
 
@@ -973,7 +1053,8 @@ def main() -> None:
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="c3", choices=["c1", "c2", "c3", "c4", "c5", "fastx"])
+    ap.add_argument("--config", default="c3",
+                    choices=["c1", "c2", "c3", "c4", "c5", "fastx", "sharded"])
     ap.add_argument("--duration", type=float, default=2.0, help="c5: seconds of arrivals")
     ap.add_argument("--server-inflight", type=int, default=0, help="c5: batches in flight")
     ap.add_argument("--server-batch-mb", type=int, default=0, help="c5: batch cap in MiB")
@@ -1014,6 +1095,14 @@ def main() -> None:
                                              "batch) are inside the c4 line"}))
             return
         run_ragged(args, world, rank, local_rank)
+        return
+    if args.config == "sharded":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "metric": SHARDED_METRIC,
+                                  "unavailable": "the reference has no multi-GPU insert"}))
+            return
+        run_sharded(args, world, rank, local_rank)
         return
     if args.config == "fastx":
         if args.impl == "reference" or rank != 0:

@@ -35,6 +35,27 @@ __device__ __forceinline__ void flush_run(uint64_t* words, uint32_t shard, const
     ++ring.count;
 }
 
+// flush_run as predicated instructions: the insert kernels call it for every
+// window with `pred` set where a run ends, so no lane of a warp branches (some
+// lane ends a run on almost every window).
+__device__ __forceinline__ void flush_run_if(uint32_t pred, uint64_t* words, uint32_t shard,
+                                             const uint64_t a[4], FlushRing& ring) {
+    static_assert(kFlushSlots == 8, "wait_group.read immediate below assumes 8 slots");
+    uint64_t* slot = ring.slot0 + (ring.count & (kFlushSlots - 1)) * (kThreads * 4);
+    const uint64_t* g = words + static_cast<uint64_t>(shard) * 4;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %0, 0;\n\t"
+        "@p cp.async.bulk.wait_group.read 7;\n\t"
+        "@p st.shared.v2.u64 [%1], {%2, %3};\n\t"
+        "@p st.shared.v2.u64 [%1+16], {%4, %5};\n\t"
+        "@p fence.proxy.async.shared::cta;\n\t"
+        "@p cp.reduce.async.bulk.global.shared::cta.bulk_group.or.b64 [%6], [%1], 32;\n\t"
+        "@p cp.async.bulk.commit_group;\n\t}" ::"r"(pred),
+        "r"(smem_addr(slot)), "l"(a[0]), "l"(a[1]), "l"(a[2]), "l"(a[3]), "l"(g)
+        : "memory");
+    ring.count += pred;
+}
+
 __device__ __forceinline__ void flush_ring_drain() {
     // Every bulk reduction issued by this thread has completed (its global
     // writes performed and its shared-memory slot read).

@@ -84,7 +84,9 @@ __global__ void __launch_bounds__(kThreads, 2) emit_kernel(TileParams p, RunLog 
         const uint32_t vmask = strip_valid<C>(iv, first_kmer, p.n_kmers);
         n_valid += __popc(vmask);
         if (vmask)
-            insert_strip<C>(c, vmask, p.shard_mask, [&](uint32_t shard, const uint64_t* acc) {
+            insert_strip<C>(c, vmask, p.shard_mask, [&](uint32_t end, uint32_t shard,
+                                                        const uint64_t* acc) {
+                if (!end) return;
                 const unsigned int i = atomicAdd(&cta_n, 1u);
                 if (i < static_cast<unsigned int>(kLogRecords)) {
                     s_shards[i] = shard;
@@ -108,10 +110,16 @@ __global__ void __launch_bounds__(kThreads, 2) emit_kernel(TileParams p, RunLog 
     if ((tid & 31) == 0 && n_valid) atomicAdd(log.count + 1, n_valid);
 }
 
-// ORs records whose shards lie in [lo, hi) into the filter; a record outside
-// the range sets the error word (the records were routed to the wrong rank).
-__global__ void apply_runs_kernel(const uint32_t* shards, const uint64_t* masks, uint64_t n,
-                                  uint64_t* words, uint64_t lo, uint64_t hi, int* err) {
+// ORs records whose shards lie in [lo, hi) into the filter, each with one
+// 32-byte bulk OR-reduction from the thread's shared-memory ring (one L2
+// operation per record, as the insert kernel flushes its runs); a record
+// outside the range sets the error word (it was routed to the wrong rank).
+__global__ void __launch_bounds__(kThreads) apply_runs_kernel(const uint32_t* shards,
+                                                              const uint64_t* masks, uint64_t n,
+                                                              uint64_t* words, uint64_t lo,
+                                                              uint64_t hi, int* err) {
+    extern __shared__ __align__(16) uint64_t ring_mem[];
+    FlushRing ring{ring_mem + 4 * threadIdx.x, 0u};
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint64_t sh = shards[i];
@@ -121,12 +129,10 @@ __global__ void apply_runs_kernel(const uint32_t* shards, const uint64_t* masks,
         }
         const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(masks + 4 * i);
         const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(masks + 4 * i + 2);
-        uint64_t* w = words + 4 * sh;
-        if (a.x) red_or(w + 0, a.x);
-        if (a.y) red_or(w + 1, a.y);
-        if (b.x) red_or(w + 2, b.x);
-        if (b.y) red_or(w + 3, b.y);
+        const uint64_t m[4] = {a.x, a.y, b.x, b.y};
+        flush_run(words, static_cast<uint32_t>(sh), m, ring);
     }
+    flush_ring_drain();
 }
 
 using EmitFn = void (*)(TileParams, RunLog);
@@ -221,10 +227,19 @@ extern "C" int sbf_apply_runs_async(sbf_filter_t* f, const uint32_t* d_shards,
     if ((reinterpret_cast<uintptr_t>(d_masks) & 15u) != 0)
         return set_error(SBF_ERR_INVALID_ARGUMENT, "mask buffer must be 16-byte aligned");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, static_cast<uint64_t>(f->sms) * 16);
-    apply_runs_kernel<<<static_cast<unsigned>(blocks), 256, 0, st>>>(d_shards, d_masks, n,
-                                                                     f->d_words, shard_lo,
-                                                                     shard_hi, f->d_err);
+    static int ring_set[64] = {};
+    cudaError_t e0;
+    if (f->device >= 0 && f->device < 64 && !ring_set[f->device]) {
+        if ((e0 = cudaFuncSetAttribute(reinterpret_cast<const void*>(&apply_runs_kernel),
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kInsertSlotBytes)) != cudaSuccess)
+            return cuda_fail(e0, "cudaFuncSetAttribute(apply_runs_kernel)");
+        ring_set[f->device] = 1;
+    }
+    const uint64_t blocks = std::min<uint64_t>((n + kThreads - 1) / kThreads,
+                                               static_cast<uint64_t>(f->sms) * 2);
+    apply_runs_kernel<<<static_cast<unsigned>(blocks), kThreads, kInsertSlotBytes, st>>>(
+        d_shards, d_masks, n, f->d_words, shard_lo, shard_hi, f->d_err);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "apply_runs_kernel");
     return SBF_OK;

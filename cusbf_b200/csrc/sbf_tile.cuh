@@ -283,9 +283,11 @@ __device__ __forceinline__ void smer_masks(const uint32_t* c, int r, uint64_t m[
 
 // Insert: the mask of window j is T_j = OR of the one-hot masks of its F
 // s-mers; a super-k-mer run (consecutive valid windows with equal shard)
-// accumulates acc = OR T_j and is handed to flush(shard, acc) when the next
-// window leaves the run (the insert kernel ORs it into the shard; the sharded
-// insert's emit kernel records it).
+// accumulates acc = OR T_j and is handed to flush(end, shard, acc) with end
+// non-zero when the next window leaves the run (the insert kernel ORs it
+// into the shard; the sharded insert's emit kernel records it).  With four
+// s-mers per window, flush is called on every window with `end` as its
+// predicate, so the per-run work needs no branch.
 template <class C, class Flush>
 __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
                                              uint32_t shard_mask, Flush&& flush) {
@@ -310,7 +312,7 @@ __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
             smer_masks<C>(c, j + 3, m3);
             const bool valid = (vmask >> j) & 1u;
             const bool cont = valid && prev_valid && shard == prev_shard;
-            if (prev_valid && !cont) flush(prev_shard, acc);
+            flush((prev_valid && !cont) ? 1u : 0u, prev_shard, acc);
             const uint64_t keep = cont ? ~uint64_t{0} : uint64_t{0};
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
@@ -331,7 +333,7 @@ __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
             smer_masks<C>(c, j + F - 1, mring[(j + F - 1) % F]);
             const bool valid = (vmask >> j) & 1u;
             const bool cont = valid && prev_valid && shard == prev_shard;
-            if (prev_valid && !cont) flush(prev_shard, acc);
+            if (prev_valid && !cont) flush(1u, prev_shard, acc);
             const uint64_t keep = cont ? ~uint64_t{0} : uint64_t{0};
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
@@ -344,7 +346,7 @@ __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
             prev_valid = valid;
         });
     }
-    if (prev_valid) flush(prev_shard, acc);
+    if (prev_valid) flush(1u, prev_shard, acc);
 }
 
 // Query shard slots: the run heads of a strip fetch their 32-byte shards into
@@ -895,9 +897,10 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
                 p.out_bits[first_kmer >> 5] = hits;
         } else {
             if (vmask)
-                insert_strip<C>(c, vmask, p.shard_mask, [&](uint32_t shard, const uint64_t* acc) {
-                    flush_run(p.words, shard, acc, ring);
-                });
+                insert_strip<C>(c, vmask, p.shard_mask,
+                                [&](uint32_t end, uint32_t shard, const uint64_t* acc) {
+                                    flush_run_if(end, p.words, shard, acc, ring);
+                                });
         }
         if constexpr (kRagged) {
             if (p.rec_valid) tally_records(p, first_rec[it % 3], first_kmer, vmask, hits);

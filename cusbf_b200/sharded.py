@@ -103,31 +103,54 @@ def gather_shards(words, num_shards: int, group, torch, dist) -> None:
     words.copy_(torch.cat(gathered)[:num_shards * 4])
 
 
-def sharded_insert(filt, d_seq, group=None, gather: bool = True, stream=None) -> int:
+def sharded_insert(filt, d_seq, group=None, gather: bool = True, stream=None,
+                   timings: dict | None = None) -> int:
     """Inserts device bytes `d_seq` into `filt` on every rank of `group`
     (each rank passes the same input and a filter of the same size on its own
     GPU): rank r emits the runs of its windows, the records are routed to the
     owners of their shards and ORed there, and with `gather` every rank ends
-    with the whole filter.  Returns the valid k-mers this rank emitted."""
+    with the whole filter.  Returns the valid k-mers this rank emitted.  With
+    `timings`, the device milliseconds of the emit, route, apply and gather
+    phases are added to it under those keys."""
     import torch
     import torch.distributed as dist
 
     from . import Filter  # noqa: F401  (the library is loaded by the package)
+
+    ev = []
+
+    def mark():
+        if timings is not None:
+            e = torch.cuda.Event(enable_timing=True)
+            e.record()
+            ev.append(e)
 
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
     k = filt.config.k
     b0, b1 = byte_slice(d_seq.numel(), k, world, rank)
     num_shards = filt.num_shards()
+    mark()
     shards, masks, valid = filt.emit_runs(d_seq[b0:b1], stream=stream)
-    records = pack_records(shards, masks, torch)
-    mine = route_records(records, num_shards, group, torch, dist)
+    mark()
     per = shards_per_owner(num_shards, world)
-    filt.apply_runs(mine[:, 0].to(torch.int32).contiguous(), mine[:, 1:].contiguous(),
-                    rank * per, min((rank + 1) * per, num_shards), stream=stream)
-    if gather:
+    if world == 1:
+        mine_sh, mine_m = shards, masks  # every shard is this rank's
+    else:
+        mine = route_records(pack_records(shards, masks, torch), num_shards, group, torch, dist)
+        mine_sh, mine_m = mine[:, 0].to(torch.int32).contiguous(), mine[:, 1:].contiguous()
+    mark()
+    filt.apply_runs(mine_sh, mine_m, rank * per, min((rank + 1) * per, num_shards),
+                    stream=stream)
+    mark()
+    if gather and world > 1:
         torch.cuda.current_stream().synchronize()
         gather_shards(filt.words().view(torch.int64), num_shards, group, torch, dist)
+    mark()
+    if timings is not None:
+        torch.cuda.synchronize()
+        for name, x, y in zip(("emit", "route", "apply", "gather"), ev, ev[1:]):
+            timings[name] = timings.get(name, 0.0) + x.elapsed_time(y)
     return valid
 
 

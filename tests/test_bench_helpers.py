@@ -1,0 +1,51 @@
+"""bench.py helpers shared by the main arm and the reference arm: the CPU
+sample both arms time is one deterministic function of the workload, and the
+host-side query counts equal a direct count over the query bytes the main arm
+builds on the device."""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def test_cpu_sample_is_deterministic_and_bounded():
+    import bench
+
+    spec = bench.workload_spec("c3", 0.01)
+    joined, _, _ = bench.build_host_genome(spec, seed=42)
+    a_ins, a_q = bench.cpu_sample(spec, joined, 42)
+    b_ins, b_q = bench.cpu_sample(spec, joined, 42)
+    assert np.array_equal(a_ins, b_ins) and np.array_equal(a_q, b_q)
+    assert a_ins.size == min(joined.size, bench.CPU_SAMPLE_BP)
+    assert a_q.size == bench.CPU_SAMPLE_READS * (spec["read_len"] + 1) - 1
+    # Reads are joined by one separator each.
+    rl = spec["read_len"]
+    assert (a_q[rl::rl + 1] == ord("N")).all()
+
+
+def test_query_counts_match_the_query_layout():
+    import bench
+
+    spec = bench.workload_spec("c3", 0.001)
+    n_q_valid, n_q_windows = bench.query_counts(spec, np.zeros(0, np.uint8))
+    rl, n = spec["read_len"], spec["n_reads"]
+    q = np.full((n, rl + 1), ord("N"), np.uint8)
+    q[:, :rl] = ord("A")
+    q = q.reshape(-1)[:-1]
+    assert n_q_windows == q.size - bench.K + 1
+    assert n_q_valid == bench.valid_windows(q)
+
+
+def test_plain_config_is_the_same_for_both_arms():
+    import bench
+
+    spec = bench.workload_spec("c3", 1.0)
+    a = bench.plain_config(spec, 1, 1 << 36, 3099999280, 12000000000, 15099999969)
+    b = bench.plain_config(spec, 1, 1 << 36, 3099999280, 12000000000, 15099999969)
+    assert a == b
+    assert a["workload"].startswith("plain-large: 3.1 Gbp in 24 records")
+    assert a["filter_bits"] == 1 << 36
