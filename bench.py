@@ -73,7 +73,7 @@ def workload_spec(name: str, scale: float) -> dict:
                     bits_per_kmer=85.7, n_reads=0, read_len=150, positive_frac=0.5,
                     sub_rate=0.0, fresh_query_bp=int(2e6 * scale),
                     l2="L2-resident by design: 32 MiB filter and 2-4 MB inputs stay in L2 "
-                       "between steps (no flush); judged against L2 bandwidth")
+                       "between steps (no flush); its roofline is the L2 bandwidth")
     raise SystemExit(f"unknown config {name}")
 
 

@@ -87,3 +87,25 @@ def test_graph_grows_the_line_table(sbf, cuda, monkeypatch):
     h = _run(sbf, monkeypatch, "host", 0, data, genome, True)
     assert g[0] == h[0]
     np.testing.assert_array_equal(g[1], h[1])
+
+
+@pytest.mark.parametrize("query", [True, False])
+def test_large_plain_file_device_equals_host_parser(sbf, cuda, monkeypatch, tmp_path, query):
+    """A 40 MB uncompressed FASTQ file: the device parser reads its blocks
+    with parallel pread() slices (files above 8 MiB), the host parser in 4 MiB
+    chunks; reports and filter words must agree."""
+    rng = np.random.default_rng(99)
+    genome = random_dna(rng, 500_000)
+    path = tmp_path / "reads.fq"
+    path.write_bytes(_fastq(rng, 150_000, 100, 400))
+    assert path.stat().st_size > 5 * (8 << 20)
+    out = {}
+    for mode in ("graph", "host"):
+        monkeypatch.setenv("SBF_FASTX_PARSER", "host" if mode == "host" else "device")
+        monkeypatch.setenv("SBF_FASTQ_BLOCK_BYTES", str(16 << 20))
+        f = sbf.Filter(1 << 22, **K31)
+        f.insert_sequence(genome)
+        rep = f.query_fastx_file(str(path)) if query else f.insert_fastx_file(str(path))
+        out[mode] = (rep.as_dict(), f.words_host())
+    assert out["graph"][0] == out["host"][0]
+    np.testing.assert_array_equal(out["graph"][1], out["host"][1])
