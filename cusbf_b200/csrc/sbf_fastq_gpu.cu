@@ -545,6 +545,22 @@ int FastqDevice::run_block_graph(sbf_filter* f, bool query, bool fasta, const ui
                                  uint64_t len, bool eof, cudaStream_t st, BlockSummary* out) {
     *out = BlockSummary{};
     if (len == 0) return SBF_OK;
+    const int s = launch_block_graph(f, query, fasta, h_text, len, eof, st);
+    return s != SBF_OK ? s : finish_block_graph(f, st, out);
+}
+
+int FastqDevice::finish_block_graph(sbf_filter* f, cudaStream_t st, BlockSummary* out) {
+    cudaError_t e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    const int s = f->check_device_error(st);
+    if (s != SBF_OK) return s;
+    *out = *static_cast<const BlockSummary*>(h_summary.p);
+    if (out->flags & kLineOverflow) line_cap = out->lines + 1;
+    return SBF_OK;
+}
+
+int FastqDevice::launch_block_graph(sbf_filter* f, bool query, bool fasta, const uint8_t* h_text,
+                                    uint64_t len, bool eof, cudaStream_t st) {
     const uint64_t tiles = (len + kTileBytes - 1) / kTileBytes;
     if (tiles > (uint64_t{1} << 20))
         return set_error(SBF_ERR_INVALID_ARGUMENT, "FASTX block too large for the device parser");
@@ -690,10 +706,6 @@ int FastqDevice::run_block_graph(sbf_filter* f, bool query, bool fasta, const ui
     cudaGraphDestroy(graph);
     if ((e = cudaGraphLaunch(exec, st)) != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
     f->launches += 2;
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
-    if ((s = f->check_device_error(st)) != SBF_OK) return s;
-    *out = *static_cast<const BlockSummary*>(h_summary.p);
-    if (out->flags & kLineOverflow) line_cap = out->lines + 1;
     return SBF_OK;
 }
 
@@ -720,6 +732,7 @@ void PinnedBuf::release() {
 
 void fastq_device_release(sbf_filter* f) {
     f->fastq_block.release();
+    f->fastq_ahead.release();
     if (!f->fastq) return;
     f->fastq->release();
     delete f->fastq;

@@ -85,6 +85,12 @@ struct FastqDevice {
     // per-record views only; needs kernels compiled into the library.
     int run_block_graph(sbf_filter* f, bool query, bool fasta, const uint8_t* h_text,
                         uint64_t len, bool eof, cudaStream_t st, BlockSummary* out);
+    // The same in two halves: launch returns once the graph is queued (the
+    // host text must stay untouched until finish), finish waits for it and
+    // fills the summary.
+    int launch_block_graph(sbf_filter* f, bool query, bool fasta, const uint8_t* h_text,
+                           uint64_t len, bool eof, cudaStream_t st);
+    int finish_block_graph(sbf_filter* f, cudaStream_t st, BlockSummary* out);
     static bool graph_usable(const sbf_filter* f);
     const uint8_t* hits_host() const { return static_cast<const uint8_t*>(h_hits.p); }
     // FASTA sequences for record views (filled by run() with want_views).

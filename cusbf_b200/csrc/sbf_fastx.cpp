@@ -360,6 +360,18 @@ bool fastx_graph_enabled() {
     return !(v && std::strcmp(v, "0") == 0);
 }
 
+// FASTQ blocks on the graph path read the next block while the device
+// works on the current one (SBF_FASTQ_READ_AHEAD=0 reads them in turn).
+bool fastq_read_ahead_enabled() {
+    const char* v = std::getenv("SBF_FASTQ_READ_AHEAD");
+    return !(v && std::strcmp(v, "0") == 0);
+}
+
+// Room in front of each FASTQ block buffer for the previous block's
+// unconsumed tail (less than one record); a longer tail hands the rest of
+// the input to the host parser.
+constexpr uint64_t kTailRoom = uint64_t{32} << 20;
+
 uint64_t fastq_block_bytes() {
     if (const char* v = std::getenv("SBF_FASTQ_BLOCK_BYTES")) {
         const long long b = std::strtoll(v, nullptr, 10);
@@ -397,7 +409,7 @@ int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const ch
     uint64_t cap = fastq_block_bytes();
     const uint64_t kMaxBlockBytes = uint64_t{8} << 30;  // FASTA records up to this size
     PinnedBuf& buf = f->fastq_block;
-    int s = buf.ensure(cap + 1);
+    int s = buf.ensure(kTailRoom + cap + 1);
     if (s != SBF_OK) return s;
     auto* text = static_cast<char*>(buf.p);
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
@@ -428,6 +440,85 @@ int run_fastx(sbf_filter* f, bool query, sbf_read_fn read, void* ruser, const ch
             parse_len = len + 1;
         }
         const bool views = query && consume;
+        if (fastq && !views && fastx_graph_enabled() && fastq_read_ahead_enabled() &&
+            FastqDevice::graph_usable(f)) {
+            // The block runs as one graph while the next block is read into
+            // the other pinned buffer, behind kTailRoom bytes that then take
+            // this block's unconsumed tail, so the next block is contiguous.
+            BlockSummary g;
+            s = dev.launch_block_graph(f, query, false, reinterpret_cast<const uint8_t*>(text),
+                                       parse_len, eof, st);
+            if (s != SBF_OK) return s;
+            char* ahead = nullptr;
+            uint64_t nb = 0;
+            bool eof2 = eof;
+            int rs = SBF_OK;
+            if (!eof) {
+                const char* a0 = static_cast<const char*>(f->fastq_block.p);
+                const bool in_block = text >= a0 && text < a0 + f->fastq_block.cap;
+                PinnedBuf& other = in_block ? f->fastq_ahead : f->fastq_block;
+                rs = other.ensure(kTailRoom + cap + 1);
+                if (rs == SBF_OK) ahead = static_cast<char*>(other.p) + kTailRoom;
+                while (rs == SBF_OK && !eof2 && nb < cap) {
+                    const int64_t n = read(ruser, ahead + nb, cap - nb);
+                    if (n < 0)
+                        rs = set_error(SBF_ERR_IO, "Failed to read FASTA/FASTQ input from %s",
+                                       source ? source : "<stream>");
+                    else if (n == 0)
+                        eof2 = true;
+                    else
+                        nb += static_cast<uint64_t>(n);
+                }
+            }
+            if ((s = dev.finish_block_graph(f, st, &g)) != SBF_OK) return s;
+            if (rs != SBF_OK) return rs;
+            while (g.flags & kBlockLineOverflow) {  // line table grown: run the block again
+                s = dev.run_block_graph(f, query, false, reinterpret_cast<const uint8_t*>(text),
+                                        parse_len, eof, st, &g);
+                if (s != SBF_OK) return s;
+            }
+            // The host parser takes over from `from` with the read-ahead bytes
+            // in front of the rest of the input.
+            auto fallback_from = [&](uint64_t from) -> int {
+                std::string pre(text + from, len - from);
+                if (nb) pre.append(ahead, nb);
+                PrefixReader pr{pre.data(), pre.size(), 0, read, ruser};
+                return finish(run_fastx_host(f, query, &PrefixReader::read, &pr, source,
+                                             fill_fraction, stream, it, qt, consume, cuser,
+                                             line_base, index_base));
+            };
+            // An insert of the records before a fallback is repeated by the
+            // host path, which ORs the same bits again.
+            if ((g.flags & kBlockIrregular) || g.records == 0 || (eof && g.consumed < parse_len))
+                return fallback_from(0);
+            if (query) {
+                qt.records_queried += g.records;
+                qt.queried_bases += g.bases;
+                qt.queried_kmers += g.valid;
+                qt.positive_kmers += g.positive;
+            } else {
+                it.records_indexed += g.records;
+                it.indexed_bases += g.bases;
+                it.inserted_kmers += g.valid;
+            }
+            index_base += g.records;
+            line_base += g.lines_used;
+            const uint64_t consumed = std::min<uint64_t>(g.consumed, len);
+            const uint64_t tail = len - consumed;
+            if (eof) {
+                std::memmove(text, text + consumed, tail);
+                len = tail;
+                if (len == 0) break;
+                continue;
+            }
+            if (tail > kTailRoom) return fallback_from(consumed);
+            std::memcpy(ahead - tail, text + consumed, tail);
+            text = ahead - tail;
+            len = tail + nb;
+            eof = eof2;
+            if (eof && len == 0) break;
+            continue;
+        }
         if (!views && fastx_graph_enabled() && FastqDevice::graph_usable(f)) {
             BlockSummary g;
             s = dev.run_block_graph(f, query, !fastq, reinterpret_cast<const uint8_t*>(text),

@@ -86,6 +86,9 @@ struct sbf_filter {
     // and the pinned block of input text it parses.
     sbf::FastqDevice* fastq = nullptr;
     sbf::PinnedBuf fastq_block;
+    // The second block buffer of FASTQ input read ahead while the device
+    // processes the current block.
+    sbf::PinnedBuf fastq_ahead;
 
     // Record-batch staging (sbf_records.cu).
     sbf::DevBuf rb_dense, rb_norm, rb_meta, rb_hits, rb_stats;
