@@ -1,6 +1,7 @@
 """Benchmark of the Super Bloom engine: k-mers/s insert + query at k=31.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--config c3|c2|c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W]
+                    [--config c3|c2|c1|c4|c5|fastx|sharded|configs]
                     [--impl ours|reference] [--scale S]
 
 Workload (default `c3`, the configuration the metric is quoted on): a seeded
@@ -823,6 +824,129 @@ def run_fastx_files(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+CONFIGS_METRIC = ("windows/s of insert and query for other filter configurations (1 GiB "
+                  "device-resident inputs, 2^34-bit filter)")
+# (name, configuration id of the reference build in oracle/_ref, engine
+# configuration, input letters)
+OTHER_CONFIGS = (
+    ("k31_s28_m21_h4", 7, dict(k=31, s=28, m=21, hashes=4), b"ACGT"),
+    ("k25_s22_m13_h4", 8, dict(k=25, s=22, m=13, hashes=4), b"ACGT"),
+    ("k21_s19_m11_h4", 6, dict(k=21, s=19, m=11, hashes=4), b"ACGT"),
+    ("k31_s28_m16_h8", 4, dict(k=31, s=28, m=16, hashes=8), b"ACGT"),
+    ("k31_s28_m16_h16", 5, dict(k=31, s=28, m=16, hashes=16), b"ACGT"),
+    ("protein_k12_s10_m6_h4", 9, dict(k=12, s=10, m=6, hashes=4, alphabet=2),
+     b"ACDEFGHIKLMNPQRSTVWY"),
+)
+
+
+def other_config_inputs(torch, dev, letters: bytes, n: int, seed: int):
+    """Insert input: n uniform letters; query input: the insert input's first
+    half followed by n - n/2 fresh letters (about half the windows present)."""
+    g = torch.Generator(device=dev).manual_seed(seed)
+    lut = torch.tensor(list(letters), dtype=torch.uint8, device=dev)
+    ins = lut[torch.randint(0, len(letters), (n,), device=dev, generator=g, dtype=torch.int32)]
+    qry = ins.clone()
+    h = n // 2
+    qry[h:] = lut[torch.randint(0, len(letters), (n - h,), device=dev, generator=g,
+                                dtype=torch.int32)]
+    return ins, qry
+
+
+def run_other_configs(args) -> None:
+    """Insert and query of 1 GiB device inputs for each of OTHER_CONFIGS,
+    timed with CUDA events on the launching stream (inputs are 8x L2, so no
+    flush is needed).  The main arm runs the engine; --impl reference runs the
+    unmodified reference GPU path (oracle/_ref) on the same seeded inputs."""
+    import torch
+
+    reference = args.impl == "reference"
+    if reference:
+        from oracle.oracle import RefGpu
+
+        if not RefGpu.available():
+            print(json.dumps({"impl": "reference", "metric": CONFIGS_METRIC,
+                              "unavailable": "oracle/_ref/libsbf_refgpu.so was not built"}))
+            return
+    else:
+        import cusbf_b200 as sbf
+    dev = torch.device("cuda", 0)
+    n = max(int((1 << 30) * args.scale), 1 << 20)
+    bits = max(int((1 << 34) * args.scale), 1 << 24)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    steps, warmup = max(args.steps, 1), max(args.warmup, 3)
+    clocks = ClockSampler(0)
+    clocks.start()
+    results = {}
+    total_windows, total_ms = 0, 0.0
+    for name, cfg_id, cfg, letters in OTHER_CONFIGS:
+        ins, qry = other_config_inputs(torch, dev, letters, n, args.seed + cfg_id)
+        n_out = n - cfg["k"] + 1
+        out = torch.empty(n_out, dtype=torch.uint8, device=dev)
+        if reference:
+            filt = RefGpu(bits, cfg_id)
+            clear = lambda: filt.clear(sp)  # noqa: E731
+            insert = lambda: filt.insert_async(ins.data_ptr(), n, sp)  # noqa: E731
+            query = lambda: filt.contains_async(qry.data_ptr(), n, out.data_ptr(),  # noqa: E731
+                                                n_out, sp)
+        else:
+            filt = sbf.Filter(bits, **cfg)
+            clear = lambda: filt.clear(stream)  # noqa: E731
+            insert = lambda: filt.insert_sequence_async(ins, stream)  # noqa: E731
+            query = lambda: filt.contains_sequence_async(qry, out, stream)  # noqa: E731
+        ins_ms, q_ms = [], []
+        for i in range(warmup + steps):
+            clear()
+            a, b, c = _ev(torch), _ev(torch), _ev(torch)
+            a.record(stream)
+            insert()
+            b.record(stream)
+            query()
+            c.record(stream)
+            torch.cuda.synchronize(dev)
+            if i >= warmup:
+                ins_ms.append(a.elapsed_time(b))
+                q_ms.append(b.elapsed_time(c))
+        i_ms, qm = float(np.mean(ins_ms)), float(np.mean(q_ms))
+        results[name] = {"insert_windows_per_s": n_out / (i_ms / 1e3), "insert_ms": i_ms,
+                         "query_windows_per_s": n_out / (qm / 1e3), "query_ms": qm,
+                         "positive_windows": int(torch.count_nonzero(out))}
+        if not reference:
+            results[name]["kernel_path"] = ("compiled in", "compiled at run time",
+                                            "generic")[filt.kernel_path()]
+        total_windows += 2 * n_out
+        total_ms += i_ms + qm
+        filt.close()
+        del ins, qry, out
+        torch.cuda.empty_cache()
+    clock_info = clocks.stop()
+    line = {"metric": CONFIGS_METRIC, "value": total_windows / (total_ms / 1e3),
+            "unit": "windows/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
+            "ms_per_step": total_ms, "higher_is_better": True, "dtype": "u8",
+            "data": "synthetic (seeded uniform letters generated on the device)",
+            "config": {"workload": f"{n} letters inserted and {n} queried per configuration",
+                       "filter_bits": bits, "l2": "inputs are 8x L2; no flush"},
+            "configs": results, "clocks": clock_info}
+    if reference:
+        line["impl"] = "reference"
+        line["path"] = ("reference cuSBF filter<Config<...>> insert_sequence_async + "
+                        "contains_sequence_async, device-resident inputs, CUDA events")
+    print(json.dumps(line), flush=True)
+
+
+def summarize_configs(d: dict) -> dict:
+    if "configs" not in d:
+        return d
+    return {"metric": d["metric"], "workload": d["config"]["workload"],
+            "filter_bits": d["config"]["filter_bits"],
+            "g_windows_per_s": {name: [round(r["insert_windows_per_s"] / 1e9, 2),
+                                       round(r["query_windows_per_s"] / 1e9, 2)]
+                                for name, r in d["configs"].items()},
+            "kernel_path": {name: r.get("kernel_path") for name, r in d["configs"].items()},
+            "positive_windows": {name: r["positive_windows"] for name, r in d["configs"].items()},
+            "clocks": d.get("clocks")}
+
+
 def _poisson_schedule(seed: int, rate: float, duration: float, pool_reads: int,
                       ins_pool: int, scale: float):
     """Arrival offsets (s), insert flags, reads per query, first read, insert
@@ -1054,7 +1178,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default="c3",
-                    choices=["c1", "c2", "c3", "c4", "c5", "fastx", "sharded"])
+                    choices=["c1", "c2", "c3", "c4", "c5", "fastx", "sharded", "configs"])
     ap.add_argument("--duration", type=float, default=2.0, help="c5: seconds of arrivals")
     ap.add_argument("--server-inflight", type=int, default=0, help="c5: batches in flight")
     ap.add_argument("--server-batch-mb", type=int, default=0, help="c5: batch cap in MiB")
@@ -1112,6 +1236,10 @@ def main() -> None:
                                                  "its parser is the host-parser leg of this line"}))
             return
         run_fastx_files(args)
+        return
+    if args.config == "configs":
+        if rank == 0:
+            run_other_configs(args)
         return
     if args.config == "c5":
         if args.impl == "reference" or rank != 0:
@@ -1453,6 +1581,8 @@ def main() -> None:
                               summarize_plain)
         line["c2"] = run_form(["--config", "c2", "--steps", "10", "--warmup", "3"],
                               summarize_plain)
+        line["other_configs"] = run_form(["--config", "configs", "--steps", "5", "--warmup", "3"],
+                                         summarize_configs)
         # Last, so that it stays in the tail of the line: the headline figures
         # of every configuration in a few hundred bytes.
         line["summary"] = compact_summary(line)
@@ -1546,6 +1676,9 @@ def compact_summary(line: dict) -> dict:
                      "plain_per_record": g(rb.get("plain_per_record_kmers_per_s")),
                      "speedup_vs_plain": rb.get("speedup_vs_plain_per_record"),
                      "identical": rb.get("plain_hits_identical")}
+    oc = line.get("other_configs") or {}
+    if "g_windows_per_s" in oc:
+        out["other_configs_gwin_s"] = oc["g_windows_per_s"]
     fx = line.get("fastx_files") or {}
     if "graph" in fx:
         out["fastx_gb_s"] = {m: [round(fx[m]["insert_gb_per_s"], 2), round(fx[m]["query_gb_per_s"], 2)]
@@ -1601,6 +1734,10 @@ def run_reference_arm(args, spec, world) -> None:
     }
     if not args.no_reference_gpu:
         line["reference_gpu"] = reference_gpu_run(args, spec, joined, n_ins_valid)
+        if world == 1 and args.config == "c3" and args.scale == 1.0 and not args.no_forms:
+            line["reference_gpu_other_configs"] = run_form(
+                ["--config", "configs", "--impl", "reference", "--steps", "5", "--warmup", "3"],
+                summarize_configs)
     print(json.dumps(line), flush=True)
 
 

@@ -49,3 +49,21 @@ def test_plain_config_is_the_same_for_both_arms():
     assert a == b
     assert a["workload"].startswith("plain-large: 3.1 Gbp in 24 records")
     assert a["filter_bits"] == 1 << 36
+
+
+def test_other_config_inputs_share_the_insert_half():
+    """Both arms of `--config configs` build their inputs with this function:
+    the query repeats the insert input's first half, the rest is fresh, and
+    only the configuration's letters occur."""
+    import torch
+
+    import bench
+
+    for name, cfg_id, cfg, letters in bench.OTHER_CONFIGS:
+        a_ins, a_q = bench.other_config_inputs(torch, torch.device("cpu"), letters, 10_001, 5)
+        b_ins, b_q = bench.other_config_inputs(torch, torch.device("cpu"), letters, 10_001, 5)
+        assert torch.equal(a_ins, b_ins) and torch.equal(a_q, b_q)
+        assert torch.equal(a_q[:5000], a_ins[:5000])
+        assert not torch.equal(a_q[5000:], a_ins[5000:])
+        assert set(a_ins.unique().tolist()) | set(a_q.unique().tolist()) <= set(letters)
+        assert cfg["k"] <= 31 and cfg_id in range(10), name
