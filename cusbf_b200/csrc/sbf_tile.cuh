@@ -215,25 +215,28 @@ __device__ __forceinline__ uint32_t min64_lo(uint64_t a, uint64_t b) {
 }
 
 // Calls fn(j, shard) for the strip's windows j = 0..kStrip-1 in order.
-// For 16 m-mers per window the minimum is a Gil-Werman sliding minimum over
-// blocks of 16 positions: window j of block b is min(suffix_b[j],
-// prefix_{b+1}[j-1]), about three 64-bit comparisons per window.
+// For 2 <= W <= 16 m-mers per window the minimum is a Gil-Werman sliding
+// minimum over blocks of W positions: window b0 + r of the block starting at
+// b0 is min(suffix_b0[r], prefix_{b0+W}[r-1]), about three 64-bit
+// comparisons per window whatever W is (instead of W - 1).
 template <class C, class Fn>
 __device__ __forceinline__ void for_each_shard(const uint32_t* c, uint32_t shard_mask, Fn&& fn) {
     constexpr int W = C::W;
-    if constexpr (W == 16) {
+    if constexpr (W >= 2 && W <= 16) {
 #pragma unroll
-        for (int b = 0; b < kStrip / 16; ++b) {
-            uint64_t suf[16];
-            suf[15] = mh_at<C>(c, 16 * b + 15);
+        for (int b0 = 0; b0 < kStrip; b0 += W) {
+            uint64_t suf[W];
+            suf[W - 1] = mh_at<C>(c, b0 + W - 1);
 #pragma unroll
-            for (int r = 14; r >= 0; --r) suf[r] = min64(mh_at<C>(c, 16 * b + r), suf[r + 1]);
-            fn(16 * b, static_cast<uint32_t>(suf[0]) & shard_mask);
+            for (int r = W - 2; r >= 0; --r) suf[r] = min64(mh_at<C>(c, b0 + r), suf[r + 1]);
+            fn(b0, static_cast<uint32_t>(suf[0]) & shard_mask);
             uint64_t pre = ~uint64_t{0};
 #pragma unroll
-            for (int j = 1; j < 16; ++j) {
-                pre = min64(pre, mh_at<C>(c, 16 * b + 15 + j));
-                fn(16 * b + j, min64_lo(suf[j], pre) & shard_mask);
+            for (int r = 1; r < W; ++r) {
+                if (b0 + r < kStrip) {
+                    pre = min64(pre, mh_at<C>(c, b0 + W - 1 + r));
+                    fn(b0 + r, min64_lo(suf[r], pre) & shard_mask);
+                }
             }
         }
     } else {
