@@ -55,11 +55,13 @@ __global__ void __launch_bounds__(kThreads, 2) emit_kernel(TileParams p, RunLog 
     __shared__ uint32_t inval[kCodeWords + 4];
     __shared__ unsigned int cta_n;
     __shared__ unsigned long long cta_base;
+    __shared__ uint64_t onehot[64];
     extern __shared__ __align__(16) uint64_t dyn[];
     uint64_t* s_masks = dyn;                                          // [kLogRecords][4]
     uint32_t* s_shards = reinterpret_cast<uint32_t*>(dyn + 4 * kLogRecords);  // [kLogRecords]
     const int tid = threadIdx.x;
     if (tid == 0) cta_n = 0;
+    onehot_init(onehot);  // published by the barrier at the top of the tile loop
     unsigned long long n_valid = 0;
     for (uint64_t tile = blockIdx.x; tile < p.n_tiles; tile += gridDim.x) {
         TileGeom g = tile_geom<false>(p, tile);
@@ -84,7 +86,7 @@ __global__ void __launch_bounds__(kThreads, 2) emit_kernel(TileParams p, RunLog 
         const uint32_t vmask = strip_valid<C>(iv, first_kmer, p.n_kmers);
         n_valid += __popc(vmask);
         if (vmask)
-            insert_strip<C>(c, vmask, p.shard_mask, [&](uint32_t end, uint32_t shard,
+            insert_strip<C>(c, vmask, p.shard_mask, onehot, [&](uint32_t end, uint32_t shard,
                                                         const uint64_t* acc) {
                 if (!end) return;
                 const unsigned int i = atomicAdd(&cta_n, 1u);

@@ -275,13 +275,28 @@ __device__ __forceinline__ uint32_t strip_valid(const uint32_t* inv, int64_t fir
     return vmask;
 }
 
-// One-hot word masks of the s-mer at strip position r.
+// One-hot word masks of the s-mer at strip position r.  With four hashes
+// each word gets one bit, read from `onehot` (1 << b for b = 0..63 in the
+// CTA's shared memory): four table loads replace four 64-bit variable
+// shifts on the ALU pipe.
 template <class C>
-__device__ __forceinline__ void smer_masks(const uint32_t* c, int r, uint64_t m[4]) {
+__device__ __forceinline__ void smer_masks(const uint32_t* c, int r, uint64_t m[4],
+                                           const uint64_t* onehot) {
     const uint64_t h = smer_hash(smer_at<C>(c, r));
-    m[0] = m[1] = m[2] = m[3] = 0;
+    if constexpr (C::H == 4) {
 #pragma unroll
-    for (int j = 0; j < C::H; ++j) m[j & 3] |= uint64_t{1} << bit_address<C::H>(h, j);
+        for (int j = 0; j < 4; ++j) m[j] = onehot[bit_address<4>(h, j)];
+    } else {
+        m[0] = m[1] = m[2] = m[3] = 0;
+#pragma unroll
+        for (int j = 0; j < C::H; ++j) m[j & 3] |= uint64_t{1} << bit_address<C::H>(h, j);
+    }
+}
+
+// Fills the one-hot table of smer_masks (threads 0..63; the caller's next
+// barrier publishes it).
+__device__ __forceinline__ void onehot_init(uint64_t* onehot) {
+    if (threadIdx.x < 64) onehot[threadIdx.x] = uint64_t{1} << threadIdx.x;
 }
 
 // Insert: the mask of window j is T_j = OR of the one-hot masks of its F
@@ -293,7 +308,8 @@ __device__ __forceinline__ void smer_masks(const uint32_t* c, int r, uint64_t m[
 // predicate, so the per-run work needs no branch.
 template <class C, class Flush>
 __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
-                                             uint32_t shard_mask, Flush&& flush) {
+                                             uint32_t shard_mask, const uint64_t* onehot,
+                                             Flush&& flush) {
     constexpr int F = C::F;
     uint64_t acc[4] = {0, 0, 0, 0};
     uint32_t prev_shard = 0;
@@ -301,9 +317,9 @@ __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
     if constexpr (F == 4) {
         // T_j = P_j | P_{j+2} with pair masks P_x = m_x | m_{x+1}.
         uint64_t m0[4], m1[4], m2[4];
-        smer_masks<C>(c, 0, m0);
-        smer_masks<C>(c, 1, m1);
-        smer_masks<C>(c, 2, m2);
+        smer_masks<C>(c, 0, m0, onehot);
+        smer_masks<C>(c, 1, m1, onehot);
+        smer_masks<C>(c, 2, m2, onehot);
         uint64_t pa[4], pb[4];
 #pragma unroll
         for (int w = 0; w < 4; ++w) {
@@ -312,7 +328,7 @@ __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
         }
         for_each_shard<C>(c, shard_mask, [&](int j, uint32_t shard) {
             uint64_t m3[4];
-            smer_masks<C>(c, j + 3, m3);
+            smer_masks<C>(c, j + 3, m3, onehot);
             const bool valid = (vmask >> j) & 1u;
             const bool cont = valid && prev_valid && shard == prev_shard;
             flush((prev_valid && !cont) ? 1u : 0u, prev_shard, acc);
@@ -331,9 +347,9 @@ __device__ __forceinline__ void insert_strip(const uint32_t* c, uint32_t vmask,
     } else {
         uint64_t mring[F][4];
 #pragma unroll
-        for (int o = 0; o < F - 1; ++o) smer_masks<C>(c, o, mring[o]);
+        for (int o = 0; o < F - 1; ++o) smer_masks<C>(c, o, mring[o], onehot);
         for_each_shard<C>(c, shard_mask, [&](int j, uint32_t shard) {
-            smer_masks<C>(c, j + F - 1, mring[(j + F - 1) % F]);
+            smer_masks<C>(c, j + F - 1, mring[(j + F - 1) % F], onehot);
             const bool valid = (vmask >> j) & 1u;
             const bool cont = valid && prev_valid && shard == prev_shard;
             if (prev_valid && !cont) flush(1u, prev_shard, acc);
@@ -793,8 +809,10 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
     __shared__ uint32_t first_rec[3];
     __shared__ unsigned long long tally[2];
     __shared__ alignas(8) uint64_t bars[2];
+    __shared__ uint64_t onehot[kQuery ? 1 : 64];
 
     const int tid = threadIdx.x;
+    if constexpr (!kQuery) onehot_init(onehot);
     if constexpr (kRagged) {
         if (p.sizes) {
             const DevSizes z = *p.sizes;
@@ -900,7 +918,7 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
                 p.out_bits[first_kmer >> 5] = hits;
         } else {
             if (vmask)
-                insert_strip<C>(c, vmask, p.shard_mask,
+                insert_strip<C>(c, vmask, p.shard_mask, onehot,
                                 [&](uint32_t end, uint32_t shard, const uint64_t* acc) {
                                     flush_run_if(end, p.words, shard, acc, ring);
                                 });
