@@ -145,7 +145,7 @@ KernelSet make_set() {
 }
 
 static const KernelSet kSets[] = {
-    make_set<31, 28, 16, 4>(),  // the graded configuration
+    make_set<31, 28, 16, 4>(),  // the benchmark configuration
     make_set<31, 30, 16, 4>(),  make_set<31, 31, 16, 4>(), make_set<31, 28, 16, 8>(),
     make_set<31, 28, 16, 16>(), make_set<21, 19, 11, 4>(), make_set<5, 4, 3, 4>(),
     make_set<3, 2, 2, 4>(),

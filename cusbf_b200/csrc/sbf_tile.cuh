@@ -409,6 +409,17 @@ __device__ __forceinline__ uint32_t smer_bytes4(const uint32_t* c, int r) {
     return __byte_perm(a | b, 0u, 0x3120u);        // bytes b0 b1 b2 b3
 }
 
+// The same four bit addresses, one per word: b[j] is the bit of shard word j.
+template <class C>
+__device__ __forceinline__ void smer_addr4(const uint32_t* c, int r, uint32_t b[4]) {
+    const uint64_t h = smer_hash(smer_at<C>(c, r));
+    const uint32_t lo = static_cast<uint32_t>(h), hi = static_cast<uint32_t>(h >> 32);
+    b[0] = lo & 63u;
+    b[1] = (lo >> 16) & 63u;
+    b[2] = hi & 63u;
+    b[3] = (hi >> 16) & 63u;
+}
+
 template <class C>
 __device__ __forceinline__ uint32_t smer_present_h(uint64_t h, const uint64_t* w) {
     uint32_t acc = 0xFFFFFFFFu;
@@ -486,7 +497,12 @@ __device__ __noinline__ uint32_t query_strip_direct(const uint32_t* c, uint32_t 
 // Query of one strip: minimizers -> cp.async of every run head's shard into
 // the thread's slots (issued as the heads are found) -> s-mer hashing while
 // the copies are in flight -> wait -> findere tests -> output bytes.
-template <class C>
+// kAddrInLoop (four hashes): compute each position's bit addresses as it
+// enters the window instead of packing the strip's addresses while the
+// copies fly.  It frees 35 registers and makes the plain <31,28,16,4> query
+// 1.1% faster, but spills in the ragged kernels and with one s-mer per
+// window, which keep the packed form.
+template <class C, bool kAddrInLoop>
 __device__ __forceinline__ uint32_t query_strip(const uint32_t* c, uint32_t vmask, uint32_t shard_mask,
                                             const uint64_t* words, uint64_t* slot0,
                                             uint32_t* ovf0, uint8_t* out, int64_t first_kmer,
@@ -551,15 +567,18 @@ __device__ __forceinline__ uint32_t query_strip(const uint32_t* c, uint32_t vmas
         if (out) store_strip_bytes(direct, out, first_kmer, n_kmers);
         return direct;
     }
-    // Hash the strip's s-mers while the shard copies are in flight.
+    // Hash the strip's s-mers while the shard copies are in flight (with
+    // four hashes, one word of bit addresses per position), unless
+    // kAddrInLoop computes them as the positions enter the window.
     constexpr int NP = kStrip + F - 1;
-    uint32_t bytes[C::H == 4 ? NP : 1];
+    constexpr bool kPacked = C::H == 4 && !kAddrInLoop;
+    uint32_t bytes[kPacked ? NP : 1];
     uint64_t hs[C::H == 4 ? 1 : NP];
 #pragma unroll
     for (int r = 0; r < NP; ++r) {
-        if constexpr (C::H == 4)
+        if constexpr (kPacked)
             bytes[r] = smer_bytes4<C>(c, r);
-        else
+        else if constexpr (C::H != 4)
             hs[r] = smer_hash(smer_at<C>(c, r));
     }
     cp_async_wait_all();
@@ -569,13 +588,16 @@ __device__ __forceinline__ uint32_t query_strip(const uint32_t* c, uint32_t vmas
     // Bit addresses of the F positions of the current window, extracted once
     // per position as it enters the window.
     uint32_t ring[C::H == 4 ? F : 1][4];
-    if constexpr (C::H == 4) {
+    auto enter = [&](int r) {  // position r enters the window
+        if constexpr (kPacked) {
 #pragma unroll
-        for (int o = 0; o < F - 1; ++o) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) ring[o][q] = __byte_perm(bytes[o], 0u, 0x4440u + q);
+            for (int q = 0; q < 4; ++q) ring[r % F][q] = __byte_perm(bytes[r], 0u, 0x4440u + q);
+        } else if constexpr (C::H == 4) {
+            smer_addr4<C>(c, r, ring[r % F]);
         }
-    }
+    };
+#pragma unroll
+    for (int o = 0; o < F - 1; ++o) enter(o);
     // (Configurations with one s-mer per window or sixteen hashes keep the
     // branching loop below: the predicated form spills registers there.)
     constexpr bool kPredicated = F > 1 && C::H <= 8;
@@ -590,11 +612,7 @@ __device__ __forceinline__ uint32_t query_strip(const uint32_t* c, uint32_t vmas
         uint32_t loaded = 0;
 #pragma unroll
         for (int j = 0; j < kStrip; ++j) {
-            if constexpr (C::H == 4) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    ring[(j + F - 1) % F][q] = __byte_perm(bytes[j + F - 1], 0u, 0x4440u + q);
-            }
+            enter(j + F - 1);
             const uint32_t head = (heads >> j) & 1u;
             lds_slot_if(head, addr, x);
             loaded += head;
@@ -621,11 +639,7 @@ __device__ __forceinline__ uint32_t query_strip(const uint32_t* c, uint32_t vmas
     n = 0;
 #pragma unroll
     for (int j = 0; j < kStrip; ++j) {
-        if constexpr (C::H == 4) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                ring[(j + F - 1) % F][q] = __byte_perm(bytes[j + F - 1], 0u, 0x4440u + q);
-        }
+        enter(j + F - 1);
         if ((heads >> j) & 1u) {
             if (n < kSlots) {
                 // Slot 0 may be the left neighbour's last slot (its thread's
@@ -908,9 +922,11 @@ __global__ void __launch_bounds__(kThreads, 2) tile_kernel(TileParams p) {
         }
         uint32_t hits = 0;
         if constexpr (kQuery) {
-            hits = query_strip<C>(c, vmask, p.shard_mask, p.words, slots + 4 * tid,
-                                  reinterpret_cast<uint32_t*>(slots + kSlots * kThreads * 4) + tid,
-                                  p.out, first_kmer, p.n_kmers);
+            constexpr bool kAddrInLoop = !kRagged && C::W == 16 && C::F > 1;
+            hits = query_strip<C, kAddrInLoop>(
+                c, vmask, p.shard_mask, p.words, slots + 4 * tid,
+                reinterpret_cast<uint32_t*>(slots + kSlots * kThreads * 4) + tid, p.out,
+                first_kmer, p.n_kmers);
             if constexpr (kRagged) n_pos += __popc(hits & vmask);
             // Bit-packed mode (grid phase 0, so strips start at multiples of
             // 32 windows): one 32-bit word per strip, coalesced across the warp.
