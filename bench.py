@@ -1,7 +1,7 @@
 """Benchmark of the Super Bloom engine: k-mers/s insert + query at k=31.
 
     python bench.py [--gpus N] [--steps K] [--warmup W]
-                    [--config c3|c2|c1|c4|c5|fastx|sharded|configs]
+                    [--config c3|c2|c1|c4|c5|fastx|sharded|configs|fpr]
                     [--impl ours|reference] [--scale S]
 
 Workload (default `c3`, the configuration the metric is quoted on): a seeded
@@ -934,6 +934,103 @@ def run_other_configs(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+FPR_METRIC = ("false-positive rate of uniform random 31-mers against the 100 Mbp genome of the "
+              "small plain workload, s = 28 / 30 / 31 at 21.4 / 85.7 / 342.6 bits per k-mer")
+# (s, configuration id of the reference build in oracle/_ref)
+FPR_S = ((28, 0), (30, 10), (31, 11))
+# Filter sizes: the workload's 21.4 bits per k-mer, and 4x and 16x that.
+FPR_SIZE_FACTORS = (1, 4, 16)
+# The reference's published table (README.md:59-63, a real genome), percent.
+FPR_PUBLISHED = {28: (0.848, 0.091, 0.0095), 30: (0.951, 0.107, 0.0114),
+                 31: (1.593, 0.210, 0.0264)}
+
+
+def run_fpr(args) -> None:
+    """False-positive rates in the form of the reference's sweep
+    (benchmarks/fpr_fastx_sweep.cu): the genome of the small plain workload
+    inserted into filters of 1x, 4x and 16x its 21.4 bits per k-mer, then 1e9
+    uniform random 31-mers queried (records of 2^28 windows generated on the
+    device from one seed, the same for every filter); FPR = positive windows /
+    queried windows.  The main arm runs the engine, --impl reference the
+    unmodified reference GPU path on the same inputs."""
+    import torch
+
+    reference = args.impl == "reference"
+    if reference:
+        from oracle.oracle import RefGpu
+
+        if not RefGpu.available():
+            print(json.dumps({"impl": "reference", "metric": FPR_METRIC,
+                              "unavailable": "oracle/_ref/libsbf_refgpu.so was not built"}))
+            return
+    else:
+        import cusbf_b200 as sbf
+    spec = workload_spec("c2", args.scale)
+    joined, _, n_ins_valid = build_host_genome(spec, seed=args.seed)
+    dev = torch.device("cuda", 0)
+    d_genome = torch.from_numpy(joined).to(dev)
+    del joined
+    base_bits = int(round(spec["bits_per_kmer"] * n_ins_valid))
+    n_query = max(int(1e9 * args.scale), 1 << 20)
+    chunk = 1 << 28
+    lut = torch.tensor(list(b"ACGT"), dtype=torch.uint8, device=dev)
+    out = torch.empty(min(chunk, n_query), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    rows = []
+    t0 = time.perf_counter()
+    for s, ref_id in FPR_S:
+        for i, factor in enumerate(FPR_SIZE_FACTORS):
+            requested = base_bits * factor
+            if reference:
+                filt = RefGpu(requested, ref_id)
+                filt.insert_async(d_genome.data_ptr(), d_genome.numel(), stream.cuda_stream)
+                filter_bits = filt.num_shards() * 256
+            else:
+                filt = sbf.Filter(requested, k=31, s=s, m=16, hashes=4)
+                filt.insert_sequence_async(d_genome, stream)
+                filter_bits = filt.filter_bits()
+            gen = torch.Generator(device=dev).manual_seed(1337)
+            positives = 0
+            for off in range(0, n_query, chunk):
+                w = min(chunk, n_query - off)
+                q = lut[torch.randint(0, 4, (w + 30,), device=dev, generator=gen,
+                                      dtype=torch.int32)]
+                if reference:
+                    filt.contains_async(q.data_ptr(), q.numel(), out.data_ptr(), w,
+                                        stream.cuda_stream)
+                else:
+                    filt.contains_sequence_async(q, out[:w], stream)
+                positives += int(torch.count_nonzero(out[:w]))
+                del q
+            filt.close()
+            rows.append({"s": s, "requested_bits": requested, "filter_bits": filter_bits,
+                         "bits_per_kmer": filter_bits / n_ins_valid, "positives": positives,
+                         "queried": n_query, "fpr_pct": 100.0 * positives / n_query,
+                         "published_pct": FPR_PUBLISHED[s][i]})
+    torch.cuda.synchronize(dev)
+    line = {"metric": FPR_METRIC, "value": rows[0]["fpr_pct"], "unit": "%",
+            "higher_is_better": False, "n_gpus": 1,
+            "data": "synthetic (seeded genome with repeats and N runs; uniform random queries "
+                    "generated on the device); the published table is on a real genome",
+            "config": {"workload": f"{n_ins_valid:,} k-mers inserted, {n_query:,} random "
+                                   f"31-mers queried per filter", "k": 31, "m": 16, "hashes": 4},
+            "fpr": rows, "seconds": time.perf_counter() - t0}
+    if reference:
+        line["impl"] = "reference"
+    print(json.dumps(line), flush=True)
+
+
+def summarize_fpr(d: dict) -> dict:
+    if "fpr" not in d:
+        return d
+    return {"metric": d["metric"], "workload": d["config"]["workload"],
+            "fpr_pct": {f"s{r['s']}@{r['bits_per_kmer']:.1f}": round(r["fpr_pct"], 4)
+                        for r in d["fpr"]},
+            "published_pct": {f"s{r['s']}@{r['bits_per_kmer']:.1f}": r["published_pct"]
+                              for r in d["fpr"]},
+            "positives": [r["positives"] for r in d["fpr"]]}
+
+
 def summarize_configs(d: dict) -> dict:
     if "configs" not in d:
         return d
@@ -1178,7 +1275,8 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default="c3",
-                    choices=["c1", "c2", "c3", "c4", "c5", "fastx", "sharded", "configs"])
+                    choices=["c1", "c2", "c3", "c4", "c5", "fastx", "sharded", "configs",
+                             "fpr"])
     ap.add_argument("--duration", type=float, default=2.0, help="c5: seconds of arrivals")
     ap.add_argument("--server-inflight", type=int, default=0, help="c5: batches in flight")
     ap.add_argument("--server-batch-mb", type=int, default=0, help="c5: batch cap in MiB")
@@ -1240,6 +1338,10 @@ def main() -> None:
     if args.config == "configs":
         if rank == 0:
             run_other_configs(args)
+        return
+    if args.config == "fpr":
+        if rank == 0:
+            run_fpr(args)
         return
     if args.config == "c5":
         if args.impl == "reference" or rank != 0:
@@ -1583,6 +1685,7 @@ def main() -> None:
                               summarize_plain)
         line["other_configs"] = run_form(["--config", "configs", "--steps", "5", "--warmup", "3"],
                                          summarize_configs)
+        line["fpr"] = run_form(["--config", "fpr"], summarize_fpr)
         # Last, so that it stays in the tail of the line: the headline figures
         # of every configuration in a few hundred bytes.
         line["summary"] = compact_summary(line)
@@ -1676,6 +1779,9 @@ def compact_summary(line: dict) -> dict:
                      "plain_per_record": g(rb.get("plain_per_record_kmers_per_s")),
                      "speedup_vs_plain": rb.get("speedup_vs_plain_per_record"),
                      "identical": rb.get("plain_hits_identical")}
+    fp = line.get("fpr") or {}
+    if "fpr_pct" in fp:
+        out["fpr_pct"] = fp["fpr_pct"]
     oc = line.get("other_configs") or {}
     if "g_windows_per_s" in oc:
         out["other_configs_gwin_s"] = oc["g_windows_per_s"]
@@ -1738,6 +1844,8 @@ def run_reference_arm(args, spec, world) -> None:
             line["reference_gpu_other_configs"] = run_form(
                 ["--config", "configs", "--impl", "reference", "--steps", "5", "--warmup", "3"],
                 summarize_configs)
+            line["reference_gpu_fpr"] = run_form(["--config", "fpr", "--impl", "reference"],
+                                                 summarize_fpr)
     print(json.dumps(line), flush=True)
 
 

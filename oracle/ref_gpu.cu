@@ -21,6 +21,8 @@ using C21 = cusbf::Config<21, 19, 11, 4>;
 using C31M21 = cusbf::Config<31, 28, 21, 4>;                       // 7
 using C25 = cusbf::Config<25, 22, 13, 4>;                          // 8
 using CP12 = cusbf::Config<12, 10, 6, 4, 256, cusbf::ProteinAlphabet>;  // 9
+using C31S30 = cusbf::Config<31, 30, 16, 4>;                       // 10
+using C31S31 = cusbf::Config<31, 31, 16, 4>;                       // 11
 
 struct Handle {
     int cfg;
@@ -53,10 +55,13 @@ SBF_REF_SHARDS(Shards21, C21)
 SBF_REF_SHARDS(Shards31M21, C31M21)
 SBF_REF_SHARDS(Shards25, C25)
 SBF_REF_SHARDS(ShardsP12, CP12)
+SBF_REF_SHARDS(Shards31S30, C31S30)
+SBF_REF_SHARDS(Shards31S31, C31S31)
 
 // Configuration ids: 0-6 as in oracle/oracle.py REF_CONFIGS; 7-9 extra
 // configurations (a long minimizer, one with no specialised engine kernel,
-// and a protein alphabet).
+// and a protein alphabet); 10-11 the s = 30 and s = 31 columns of the
+// reference's false-positive sweep (benchmarks/fpr_fastx_sweep.cu).
 template <typename Fn>
 int with(Handle* h, Fn&& fn) {
     if (!h) return -1;
@@ -69,6 +74,8 @@ int with(Handle* h, Fn&& fn) {
         case 7: return fn(*static_cast<cusbf::filter<C31M21>*>(h->f));
         case 8: return fn(*static_cast<cusbf::filter<C25>*>(h->f));
         case 9: return fn(*static_cast<cusbf::filter<CP12>*>(h->f));
+        case 10: return fn(*static_cast<cusbf::filter<C31S30>*>(h->f));
+        case 11: return fn(*static_cast<cusbf::filter<C31S31>*>(h->f));
         default: return -1;
     }
 }
@@ -87,6 +94,8 @@ void* sbf_refgpu_create(int cfg, uint64_t bits) {
             case 7: return new Handle{7, new cusbf::filter<C31M21>(bits)};
             case 8: return new Handle{8, new cusbf::filter<C25>(bits)};
             case 9: return new Handle{9, new cusbf::filter<CP12>(bits)};
+            case 10: return new Handle{10, new cusbf::filter<C31S30>(bits)};
+            case 11: return new Handle{11, new cusbf::filter<C31S31>(bits)};
             default: break;
         }
     } catch (...) {

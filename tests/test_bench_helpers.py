@@ -67,3 +67,21 @@ def test_other_config_inputs_share_the_insert_half():
         assert not torch.equal(a_q[5000:], a_ins[5000:])
         assert set(a_ins.unique().tolist()) | set(a_q.unique().tolist()) <= set(letters)
         assert cfg["k"] <= 31 and cfg_id in range(10), name
+
+
+def test_fpr_form_tables():
+    """The FPR form sweeps s = 28, 30, 31 at three filter sizes, each beside
+    the reference's published rate for that cell, and its summary keeps one
+    entry per cell."""
+    import bench
+
+    assert [s for s, _ in bench.FPR_S] == [28, 30, 31]
+    for s, _ in bench.FPR_S:
+        assert len(bench.FPR_PUBLISHED[s]) == len(bench.FPR_SIZE_FACTORS)
+    rows = [{"s": s, "bits_per_kmer": 21.47 * f, "fpr_pct": 0.5, "published_pct": p,
+             "positives": 5} for s, _ in bench.FPR_S
+            for f, p in zip(bench.FPR_SIZE_FACTORS, bench.FPR_PUBLISHED[s])]
+    d = {"metric": bench.FPR_METRIC, "config": {"workload": "w"}, "fpr": rows}
+    out = bench.summarize_fpr(d)
+    assert len(out["fpr_pct"]) == len(out["published_pct"]) == 9
+    assert bench.summarize_fpr({"unavailable": "x"}) == {"unavailable": "x"}

@@ -102,10 +102,13 @@ def test_large_single_launch(sbf, cuda, refgpu):
                                         (1, dict(k=5, s=4, m=3, hashes=4)),
                                         (7, dict(k=31, s=28, m=21, hashes=4)),
                                         (8, dict(k=25, s=22, m=13, hashes=4)),
-                                        (9, dict(k=12, s=10, m=6, hashes=4, alphabet=2))])
+                                        (9, dict(k=12, s=10, m=6, hashes=4, alphabet=2)),
+                                        (10, dict(k=31, s=30, m=16, hashes=4)),
+                                        (11, dict(k=31, s=31, m=16, hashes=4))])
 def test_other_configs(sbf, cuda, refgpu, cfg_id, cfg):
-    """Specialised (4, 5, 6, 1, 7) and generic (8, and the protein alphabet 9)
-    engine kernels against the reference GPU path for that configuration."""
+    """Specialised (4, 5, 6, 1, 7, 10, 11) and generic (8, and the protein
+    alphabet 9) engine kernels against the reference GPU path for that
+    configuration."""
     torch = cuda
     rng = np.random.default_rng(cfg_id)
     if cfg.get("alphabet") == 2:
