@@ -415,13 +415,22 @@ extern "C" int sbf_filter_create(uint32_t k, uint32_t s, uint32_t m, uint32_t ha
         f->ks = ks;
         const void* fns[6] = {ks->insert_bytes, ks->query_bytes, ks->insert_dense,
                               ks->query_dense, ks->insert_ragged, ks->query_ragged};
-        // Run-time compiled kernels have their attributes set when loaded;
-        // their occupancy is the set's (two CTAs per SM for the tile
-        // kernels, as their shared memory allows).
+        // Run-time compiled kernels have their attributes set when loaded.
+        // Their occupancy is the loaded kernel's own (registers and shared
+        // memory): a persistent grid larger than what fits the SMs at once
+        // runs its last CTAs as a second wave.  When the handle does not
+        // answer, the set's assumption (two CTAs per SM for the tile
+        // kernels, as their shared memory allows) stands.
         for (int i = 0; i < 6 && ks->jit; ++i) {
             const int dyn = ks->smem((i & 1) != 0);
-            f->occupancy[i] = dyn ? std::min(ks->jit_occupancy, (227 << 10) / dyn)
-                                  : ks->jit_occupancy;
+            int occ = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fns[i], kThreads, dyn) !=
+                    cudaSuccess ||
+                occ < 1) {
+                cudaGetLastError();
+                occ = dyn ? std::min(ks->jit_occupancy, (227 << 10) / dyn) : ks->jit_occupancy;
+            }
+            f->occupancy[i] = occ;
         }
         for (int i = 0; i < 6 && rc == SBF_OK && !ks->jit; ++i) {
             // Query kernels: shard slots; insert kernels: flush staging ring.
