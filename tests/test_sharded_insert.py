@@ -65,7 +65,7 @@ def _rank_main(rank, world, port, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("world", [2, 3, 4])
 def test_gloo_ranks_build_the_single_insert_filter(oracle_mod, world):
     import torch.multiprocessing as mp
 
