@@ -716,8 +716,12 @@ def _sharded_methods():
         while True:
             shards = torch.empty(cap, dtype=torch.int32, device=dev)
             masks = torch.empty((cap, 4), dtype=torch.int64, device=dev)
+            # The count buffer is written on torch's current stream and read
+            # back after the launch on `stream`, which may be another one.
+            torch.cuda.current_stream(dev).synchronize()
             _check(_lib.sbf_emit_runs_async(self._h, p, n, shards.data_ptr(), masks.data_ptr(),
                                             cap, count.data_ptr(), _stream(stream)))
+            self.synchronize(stream)
             got = count.tolist()
             if got[0] <= cap:
                 return shards[:got[0]], masks[:got[0]], int(got[1])

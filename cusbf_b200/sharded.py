@@ -140,11 +140,14 @@ def sharded_insert(filt, d_seq, group=None, gather: bool = True, stream=None,
         mine = route_records(pack_records(shards, masks, torch), num_shards, group, torch, dist)
         mine_sh, mine_m = mine[:, 0].to(torch.int32).contiguous(), mine[:, 1:].contiguous()
     mark()
+    # The records come from torch ops on the current stream; the OR runs on
+    # `stream`, and the gather reads the words on the current stream again.
+    torch.cuda.current_stream().synchronize()
     filt.apply_runs(mine_sh, mine_m, rank * per, min((rank + 1) * per, num_shards),
                     stream=stream)
+    filt.synchronize(stream)
     mark()
     if gather and world > 1:
-        torch.cuda.current_stream().synchronize()
         gather_shards(filt.words().view(torch.int64), num_shards, group, torch, dist)
     mark()
     if timings is not None:
