@@ -10,7 +10,8 @@ the reference headers by oracle/Makefile and driven window by window
 
 Outputs:
   * k31_small.npz   -- full word arrays and query bytes for small inputs
-                       (k=31,s=28,m=16,h=4 and the other compiled configs).
+                       (k=31,s=28,m=16,h=4, the other compiled configs, and
+                       the protein and DNA-triplet alphabets).
   * digests.json    -- SHA-256 digests of the word arrays and query bytes of
                        the plain-method small workload (2 Mbp, 85.7 bits per
                        k-mer, + a fresh 2 Mbp query record) and of a 20 Mbp
@@ -40,6 +41,12 @@ SMALL_CASES = [
     ("k21", 21, 19, 11, 4, 1 << 15, 10_000, 46, b"ACGTN"),
     ("k5", 5, 4, 3, 4, 1 << 12, 2_000, 47, b"ACGT"),
 ]
+# Protein and DNA-triplet alphabets (alphabet id, as in the C ABI):
+# (name, k, s, m, h, bits, insert_len, seed, letters, alphabet)
+ALPHABET_CASES = [
+    ("prot5", 5, 4, 3, 4, 1 << 12, 3_000, 48, b"ACDEFGHIKLMNPQRSTVWYacdefXB*", 2),
+    ("trip3", 3, 2, 2, 4, 1 << 12, 6_000, 49, b"ACGTACGTACGTacgtN", 1),
+]
 
 
 def seq_of(rng, n, alphabet):
@@ -63,11 +70,12 @@ def plain_small_inputs():
 
 def main() -> None:
     arrays = {}
-    for name, k, s, m, h, bits, n, seed, alpha in SMALL_CASES:
+    cases = [c + (0,) for c in SMALL_CASES] + ALPHABET_CASES
+    for name, k, s, m, h, bits, n, seed, alpha, alphabet in cases:
         rng = np.random.default_rng(seed)
         ins = seq_of(rng, n, alpha)
         qry = np.concatenate([ins[: n // 2], seq_of(rng, n, alpha)])
-        r = RefCpu(k, s, m, h, 0)
+        r = RefCpu(k, s, m, h, alphabet)
         w = np.zeros(num_shards(bits) * 4, dtype=np.uint64)
         r.insert(w, ins)
         hits = r.contains(w, qry)
@@ -76,6 +84,7 @@ def main() -> None:
         arrays[f"{name}__words"] = w
         arrays[f"{name}__hits"] = hits
         arrays[f"{name}__cfg"] = np.array([k, s, m, h, bits], dtype=np.uint64)
+        arrays[f"{name}__alphabet"] = np.array([alphabet], dtype=np.uint64)
     np.savez_compressed(os.path.join(HERE, "k31_small.npz"), **arrays)
 
     digests = {}

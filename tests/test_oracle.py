@@ -101,11 +101,15 @@ def test_shard_count(oracle_mod):
     assert ns(int(85.7 * 1_999_970)) == 1 << 20
 
 
-@pytest.mark.parametrize("name", ["k31_uniform", "k31_invalid", "k31_h8", "k31_h16", "k21", "k5"])
+@pytest.mark.parametrize("name", ["k31_uniform", "k31_invalid", "k31_h8", "k31_h16", "k21", "k5",
+                                  "prot5", "trip3"])
 def test_golden_vectors(oracle_mod, name):
+    """Fixtures from the reference's own arithmetic (oracle/_ref), including
+    the protein and DNA-triplet alphabets."""
     z = np.load(os.path.join(GOLDEN, "k31_small.npz"))
     k, s, m, h, bits = (int(x) for x in z[f"{name}__cfg"])
-    o = _o(oracle_mod, k, s, m, h)
+    alphabet = int(z[f"{name}__alphabet"][0])
+    o = _o(oracle_mod, k, s, m, h, alphabet)
     w = o.new_words(bits)
     o.insert(w, z[f"{name}__insert"])
     np.testing.assert_array_equal(w, z[f"{name}__words"])
