@@ -20,16 +20,18 @@
 //   * Each of the 256 threads owns a strip of 32 consecutive windows.  Every
 //     m-mer and s-mer of the strip is a funnel shift of the code words,
 //     every position is hashed once, and the per-window minimizer is a
-//     Gil-Werman sliding minimum (about 3 comparisons per window instead of
-//     the reference's 16 multiplies).
+//     Gil-Werman sliding minimum over blocks of W positions (about 3
+//     comparisons per window for any W <= 16, where the reference hashes
+//     and compares all W m-mers of every window).
 //   * Insert merges consecutive windows that select the same shard (a
 //     super-k-mer run) in registers and flushes each run with one 32-byte
 //     bulk OR-reduction (cp.reduce.async.bulk .or.b64) from a per-thread
 //     shared-memory ring: one L2 sector operation per run.
 //   * Query copies each run head's 32-byte shard into per-thread shared
-//     slots with cp.async while the strip's s-mers are hashed, borrows the
-//     left neighbour's staged shard when a run crosses the strip boundary,
-//     and tests the findere rule (all k-s+1 s-mers present) per window.
+//     slots with cp.async as the heads are found, borrows the left
+//     neighbour's staged shard when a run crosses the strip boundary, and
+//     tests the findere rule (all k-s+1 s-mers present) per window.
+//   * Insert word masks come from a shared one-hot table (1 << b).
 //   * Ragged launches take tiles from a device work-queue counter and drop
 //     windows that cross a record boundary or touch a byte outside every
 //     record (marked per tile in shared memory).
