@@ -85,3 +85,22 @@ def test_fpr_form_tables():
     out = bench.summarize_fpr(d)
     assert len(out["fpr_pct"]) == len(out["published_pct"]) == 9
     assert bench.summarize_fpr({"unavailable": "x"}) == {"unavailable": "x"}
+
+
+def test_reference_forms_report_unavailable_without_the_build(monkeypatch, capsys):
+    """Without oracle/_ref/libsbf_refgpu.so the reference arm's configuration
+    and false-positive forms print one `unavailable` line and touch no GPU."""
+    import argparse
+    import json
+
+    import bench
+    from oracle import oracle
+
+    monkeypatch.setattr(oracle.RefGpu, "available", staticmethod(lambda: False))
+    args = argparse.Namespace(impl="reference", scale=1.0, seed=42, steps=1, warmup=3)
+    for run, metric in ((bench.run_other_configs, bench.CONFIGS_METRIC),
+                        (bench.run_fpr, bench.FPR_METRIC)):
+        run(args)
+        line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+        assert line["impl"] == "reference" and line["metric"] == metric
+        assert "unavailable" in line
